@@ -1,0 +1,181 @@
+/*
+ * rvf_b200.h -- C ABI of librvf_b200.so, the B200 backend for
+ * RadiativeViewFactor.jl's element-pair view-factor assembly.
+ *
+ * The library replaces the GPU path behind compute_view_factors(mesh; ...)
+ * (src/Assembly.jl:64-96): everything below the GPU hook _GPU_HOOK_REF
+ * (src/Assembly.jl:241-252) -- compute_view_factors_gpu (src/GPUAssembly.jl:32-105),
+ * the pair kernel (src/GPUKernels.jl:226-323), the flat BVH and its traversal
+ * (src/GPUBVH.jl:99-285), the Monte Carlo kernel (src/GPUMCKernels.jl:146-328)
+ * and, as a device path the reference lacks, the Duffy integrals
+ * (src/DuffyKernel.jl:452-487).
+ *
+ * Conventions
+ *   - Every entry point returns an int status (RVF_OK == 0, negative on error)
+ *     and never aborts or throws; rvf_last_error() gives the message of the
+ *     last failure on the calling thread.
+ *   - Matrices are column-major like Julia's (element (i,j) of an N x N matrix
+ *     at i + j*N, 0-based); F[i,j] is the view factor from element i to j.
+ *   - Node ids inside the node tables are 1-based, exactly as
+ *     build_gpu_arrays (src/GPUKernels.jl:336-412) produces them.
+ *   - One session drives one GPU.  Calls on one session are serialised by an
+ *     internal mutex; results are written before rvf_solve returns
+ *     (synchronous, like KernelAbstractions.synchronize at src/GPUKernels.jl:498).
+ */
+#ifndef RVF_B200_H
+#define RVF_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define RVF_ABI_VERSION 1
+
+/* status codes */
+#define RVF_OK 0
+#define RVF_EINVAL (-1)       /* malformed argument / mesh (bad node id, zero-area element, ...) */
+#define RVF_ENOMEM (-2)       /* device or pinned host allocation failed */
+#define RVF_EBUDGET (-3)      /* request exceeds the session's HBM budget */
+#define RVF_ECUDA (-4)        /* CUDA runtime error */
+#define RVF_ETIMEDOUT (-5)    /* a bounded device wait gave up, or rvf_wait timed out */
+#define RVF_ECANCELED (-6)    /* request cancelled */
+#define RVF_EUNSUPPORTED (-7) /* option combination not implemented */
+#define RVF_ENODEV (-8)       /* no usable sm_100 device */
+#define RVF_EBUSY (-9)        /* result not ready yet (rvf_poll) */
+#define RVF_ECLOSED (-10)     /* serving queue closed */
+
+/* element family codes: src/GPUKernels.jl:344 (0..3), extended with curves */
+#define RVF_QUAD8 0
+#define RVF_TRI6 1
+#define RVF_QUAD4 2
+#define RVF_TRI3 3
+#define RVF_LINE3 4
+#define RVF_LINE2 5
+
+#define RVF_METHOD_QUADRATURE 0
+#define RVF_METHOD_MONTE_CARLO 1
+
+#define RVF_PREC_FP64 0  /* everything in FP64 (the plain path) */
+#define RVF_PREC_MIXED 1 /* FP32 far field and traversal, FP64 where stability needs it */
+
+typedef struct rvf_session rvf_session;
+typedef struct rvf_mesh rvf_mesh;
+typedef struct rvf_request rvf_request;
+
+typedef struct {
+  int32_t device;             /* CUDA ordinal (default 0) */
+  uint64_t hbm_budget_bytes;  /* 0 = 90% of the device's free memory at creation */
+  int32_t n_host_threads;     /* host staging threads (0 = hardware concurrency) */
+  int32_t reserved[8];
+} rvf_session_opts;
+
+/* Mesh, laid out as build_gpu_arrays (src/GPUKernels.jl:336-412) flattens
+ * MeshData, plus the merged obstruction soup of build_flat_bvh_from_mesh
+ * (src/GPUBVH.jl:146-174) and the sorted group tags of _aggregate
+ * (src/Results.jl:59).  The library copies everything it needs; the caller
+ * keeps ownership of these buffers. */
+typedef struct {
+  int32_t mesh_dim;             /* 2 = surface mesh (3-D view factors), 1 = curve mesh (2-D, per unit depth) */
+  int64_t n_nodes;
+  const double* coords;         /* 3 x n_nodes, column-major */
+  int64_t n_elems;
+  const int8_t* elem_family;    /* RVF_QUAD8 ... RVF_LINE2 */
+  const int32_t* elem_node_idx; /* 1-based column of the element in its family's node table */
+  const int32_t* elem_group;    /* physical group tag */
+  const int32_t* nodes[6];      /* per family: k x n_family[f] column-major, 1-based node ids (k = 8,6,4,3,3,2) */
+  int64_t n_family[6];
+  int64_t n_obs;                /* obstruction primitives (0 = no obstruction) */
+  int32_t obs_nv;               /* 3 = triangle soup, 2 = segment soup */
+  const double* obs_soup;       /* soup[c + 3*(v + obs_nv*t)], the layout of src/MeshIO.jl:648-685 */
+  const int32_t* obs_group;     /* group tag per primitive, pre-permutation */
+  int32_t n_groups;             /* number of sorted group tags (F_group is n_groups^2) */
+  const int32_t* group_tags;    /* sorted ascending */
+} rvf_mesh_desc;
+
+typedef struct {
+  int32_t nquad;              /* Gauss points per direction / Dunavant selector (src/GPUKernels.jl:388-393) */
+  int32_t method;             /* RVF_METHOD_* */
+  int32_t use_duffy;          /* Sauter-Schwab integrals for Quad8 pairs sharing corners */
+  int32_t n_samples;          /* Monte Carlo samples per pair */
+  uint64_t seed;              /* Monte Carlo seed (the reference draws rand(UInt64), src/GPUAssembly.jl:72) */
+  int32_t precision;          /* RVF_PREC_* */
+  int32_t occlusion;          /* 1: cast shadow rays against the mesh's obstruction soup */
+  int32_t geometric_soup;     /* 0: read soup triangles as the reference does (parity); 1: true vertices */
+  int32_t mc_exclude_groups;  /* MC: 0 passes group tags 0/0 like src/GPUMCKernels.jl:164; 1 skips src/dst groups */
+  double near_field_factor;   /* mixed: centroid distance < factor * max diameter runs in FP64 (default 2) */
+  uint8_t* ray_log;           /* debug: host buffer of n_elems^2 * ray_log_pm^2 bytes, or NULL */
+  int32_t ray_log_pm;         /* stride of the ray log (>= points per element) */
+  int32_t reserved[8];
+} rvf_options;
+
+typedef struct {
+  double ms_upload;       /* host->device of the mesh description */
+  double ms_prep;         /* quadrature tables, areas, BVH upload */
+  double ms_pairs;        /* pair integration (+ occlusion) */
+  double ms_duffy;        /* singular pairs */
+  double ms_reduce;       /* group aggregation and row sums */
+  double ms_download;     /* device->host of the results */
+  double ms_total;
+  int64_t n_pairs;        /* unordered element pairs integrated */
+  int64_t n_point_pairs;  /* quadrature / sample point pairs evaluated */
+  int64_t n_rays;         /* shadow rays cast */
+  int64_t n_rays_fp64;    /* rays traced in FP64 (all of them in FP64 mode; re-tests in mixed mode) */
+  int64_t n_pairs_fp64;   /* mixed mode: pairs integrated in FP64 (near field / grazing) */
+  int64_t n_duffy_pairs;  /* vertex- or edge-sharing Quad8 pairs */
+  double max_row_sum_dev; /* max_i |sum_j F_ij - 1| */
+  int64_t reserved[8];
+} rvf_stats;
+
+const char* rvf_version(void);
+int rvf_abi_version(void);
+int rvf_last_error(char* buf, size_t n);
+void rvf_default_options(rvf_options* o);
+
+/* session: replaces the CUDABackend / CuArray registration of
+ * ext/RadiativeViewFactorCUDAExt.jl:11-12 (device selection, Float64). */
+int rvf_session_create(const rvf_session_opts* opts, rvf_session** out);
+int rvf_session_destroy(rvf_session* s);
+int rvf_device_info(rvf_session* s, int* sm_count, uint64_t* hbm_total, uint64_t* hbm_free);
+
+/* mesh upload: build_gpu_arrays (src/GPUKernels.jl:336-412) +
+ * build_flat_bvh_from_mesh (src/GPUBVH.jl:146-174). */
+int rvf_mesh_upload(rvf_session* s, const rvf_mesh_desc* d, rvf_mesh** out);
+int rvf_mesh_release(rvf_session* s, rvf_mesh* m);
+int rvf_mesh_n_elems(const rvf_mesh* m, int64_t* n);
+
+/* Solve: compute_view_factors_gpu (src/GPUAssembly.jl:32-105).
+ * F_elem (N*N), A_elem (N), F_group (G*G), A_group (G), row_sums (N) are
+ * caller-owned host buffers or NULL.  The element matrix also stays on the
+ * device until the next solve on this mesh (rvf_result_copy). */
+int rvf_solve(rvf_session* s, rvf_mesh* m, const rvf_options* o, double* F_elem, double* A_elem,
+              double* F_group, double* A_group, double* row_sums, rvf_stats* st);
+int rvf_result_copy(rvf_session* s, rvf_mesh* m, double* F_elem, double* A_elem);
+/* Device address of the element matrix of the last solve (column-major N*N). */
+int rvf_result_device(rvf_mesh* m, const double** F_dev, const double** A_dev);
+
+/* pinned host memory for result buffers (faster device->host copies) */
+int rvf_host_alloc(size_t bytes, void** p);
+int rvf_host_free(void* p);
+
+/* quadrature rule tables used by the device (for cross-checks) */
+int rvf_quadrature_rule(int32_t family, int32_t nquad, double* pts, double* wts, int32_t* n_pts);
+
+/* Measured FMA throughput of the device (fp64 = 1: FP64, 0: FP32) in TFLOP/s:
+ * the denominator of the pair kernels' roofline (they are FMA-pipe bound). */
+int rvf_fma_peak(int32_t device, int32_t fp64, double* tflops);
+
+/* Host-side BVH build of rvf_mesh_upload (build_bvh, src/BVH.jl:71-148, plus
+ * the miss links of src/GPUBVH.jl:69-82), exported for cross-checks; needs no
+ * GPU.  Call with lo == NULL to get the node count in *n_nodes; then lo/hi
+ * (3*M), meta (5*M: left,right,tri_start,tri_count,miss, 1-based as
+ * src/GPUBVH.jl:48-55) and tri_idx (n_prims, 1-based) are filled. */
+int rvf_bvh_build_host(const double* soup, int32_t nv, int64_t n_prims, double* lo, double* hi, int32_t* meta,
+                       int32_t* tri_idx, int64_t* n_nodes);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,26 @@
+"""B200 backend for RadiativeViewFactor.jl's element-pair view-factor assembly.
+
+The package mirrors the reference's user-facing API for the GPU path
+(compute_view_factors, register_gpu_hook, ViewFactorResult, check_reciprocity,
+check_closure, aggregate_by_group; src/RadiativeViewFactor.jl:33-46) over the
+C ABI of lib/librvf_b200.so (include/rvf_b200.h).  The directory name is not a
+Python identifier; import it through importlib, e.g.
+
+    spec = importlib.util.spec_from_file_location(
+        "rvf_b200", "radiativeviewfactor.jl_b200/__init__.py",
+        submodule_search_locations=["radiativeviewfactor.jl_b200"])
+"""
+from . import meshes
+from ._abi import PinnedArray, RVFError, Session, DeviceMesh, load_library
+from .assembly import (B200Backend, CPU, compute_view_factors, compute_view_factors_b200, make_options,
+                       mesh_desc_arrays, register_gpu_hook)
+from .mesh import FAMILY_CODES, MeshData, SurfaceElement, build_group_obs_soups, flatten, merged_obstruction
+from .results import (ViewFactorResult, aggregate_by_group, check_closure, check_reciprocity,
+                      reciprocity_error)
+
+__all__ = [
+    "B200Backend", "CPU", "DeviceMesh", "FAMILY_CODES", "MeshData", "PinnedArray", "RVFError", "Session",
+    "SurfaceElement", "ViewFactorResult", "aggregate_by_group", "build_group_obs_soups", "check_closure",
+    "check_reciprocity", "compute_view_factors", "compute_view_factors_b200", "flatten", "load_library",
+    "make_options", "merged_obstruction", "mesh_desc_arrays", "meshes", "reciprocity_error", "register_gpu_hook",
+]

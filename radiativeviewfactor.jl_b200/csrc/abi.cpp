@@ -1,0 +1,290 @@
+// abi.cpp -- the C ABI of librvf_b200 (include/rvf_b200.h).
+//
+// compute_view_factors_gpu (src/GPUAssembly.jl:32-105) restated as a
+// host driver: upload (build_gpu_arrays, src/GPUKernels.jl:336-412), BVH
+// (build_flat_bvh_from_mesh, src/GPUBVH.jl:146-174), pair kernel, F = raw/A,
+// aggregation (src/Results.jl:56-82) and the copies back to the host.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "../../include/rvf_b200.h"
+#include "kernels.h"
+#include "rvf_internal.h"
+
+namespace rvf {
+
+thread_local std::string g_last_error;
+
+int set_err(int code, const char* fmt, ...) {
+  char buf[1024];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  g_last_error = buf;
+  return code;
+}
+
+int cuda_err(cudaError_t e, const char* what) {
+  return set_err(RVF_ECUDA, "%s: %s (%s)", what, cudaGetErrorName(e), cudaGetErrorString(e));
+}
+
+// ---------------------------------------------------------------------------
+// device buffers with budget accounting
+// ---------------------------------------------------------------------------
+int DevBuf::alloc(Session* s, size_t n) {
+  free_();
+  if (n == 0) return RVF_OK;
+  if (s->used + n > s->budget)
+    return set_err(RVF_EBUDGET, "HBM budget exceeded: need %zu more bytes, %zu of %zu in use", n, s->used,
+                   s->budget);
+  cudaError_t e = cudaMalloc(&ptr, n);
+  if (e != cudaSuccess) {
+    ptr = nullptr;
+    cudaGetLastError();
+    return set_err(RVF_ENOMEM, "cudaMalloc(%zu) failed: %s", n, cudaGetErrorString(e));
+  }
+  bytes = n;
+  owner = s;
+  s->used += n;
+  return RVF_OK;
+}
+void DevBuf::free_() {
+  if (ptr) {
+    cudaFree(ptr);
+    if (owner) owner->used -= bytes;
+  }
+  ptr = nullptr;
+  bytes = 0;
+  owner = nullptr;
+}
+
+int upload(Session* s, DevBuf& b, const void* src, size_t n) {
+  int rc = b.alloc(s, n);
+  if (rc) return rc;
+  if (n == 0) return RVF_OK;
+  cudaError_t e = cudaMemcpyAsync(b.ptr, src, n, cudaMemcpyHostToDevice, s->stream);
+  return e == cudaSuccess ? RVF_OK : cuda_err(e, "cudaMemcpyAsync H2D");
+}
+
+// ---------------------------------------------------------------------------
+// mesh upload
+// ---------------------------------------------------------------------------
+static const int kFamNodes[6] = {8, 6, 4, 3, 3, 2};
+
+int mesh_upload(Session* s, const rvf_mesh_desc* d, rvf_mesh** out) {
+  if (!d || !out) return set_err(RVF_EINVAL, "null argument");
+  if (d->mesh_dim != 1 && d->mesh_dim != 2) return set_err(RVF_EINVAL, "mesh_dim must be 1 or 2, got %d", d->mesh_dim);
+  if (d->n_elems < 0 || d->n_nodes < 0) return set_err(RVF_EINVAL, "negative sizes");
+  if (d->n_elems > 0 && (!d->coords || !d->elem_family || !d->elem_node_idx || !d->elem_group))
+    return set_err(RVF_EINVAL, "missing mesh arrays");
+  auto m = std::make_unique<rvf_mesh>();
+  m->s = s;
+  m->dim = d->mesh_dim;
+  m->N = d->n_elems;
+  m->Nn = d->n_nodes;
+  const int64_t N = m->N;
+  // padded, 0-based node table (element-major)
+  m->h_enodes.assign((size_t)N * 8, 0);
+  m->h_fam.assign(d->elem_family, d->elem_family + N);
+  m->h_group.assign(d->elem_group, d->elem_group + N);
+  for (int64_t e = 0; e < N; ++e) {
+    int f = d->elem_family[e];
+    if (f < 0 || f > 5) return set_err(RVF_EINVAL, "element %lld: unknown family code %d", (long long)e + 1, f);
+    if ((d->mesh_dim == 2) != (f <= 3))
+      return set_err(RVF_EINVAL, "element %lld: family %d does not match mesh_dim %d", (long long)e + 1, f,
+                     d->mesh_dim);
+    int64_t col = d->elem_node_idx[e];
+    if (col < 1 || col > d->n_family[f] || !d->nodes[f])
+      return set_err(RVF_EINVAL, "element %lld: elem_node_idx %lld outside the family table", (long long)e + 1,
+                     (long long)col);
+    int k = kFamNodes[f];
+    for (int a = 0; a < k; ++a) {
+      int32_t nid = d->nodes[f][(col - 1) * k + a];
+      if (nid < 1 || nid > d->n_nodes)
+        return set_err(RVF_EINVAL, "element %lld: node id %d outside 1..%lld", (long long)e + 1, nid,
+                       (long long)d->n_nodes);
+      m->h_enodes[(size_t)e * 8 + a] = nid - 1;
+    }
+  }
+  // groups: sorted tags (src/Results.jl:59) -> member lists in element order
+  std::vector<int32_t> tags;
+  if (d->n_groups > 0 && d->group_tags) tags.assign(d->group_tags, d->group_tags + d->n_groups);
+  else {
+    tags = m->h_group;
+    std::sort(tags.begin(), tags.end());
+    tags.erase(std::unique(tags.begin(), tags.end()), tags.end());
+  }
+  for (size_t k = 1; k < tags.size(); ++k)
+    if (!(tags[k - 1] < tags[k])) return set_err(RVF_EINVAL, "group_tags must be sorted ascending and distinct");
+  m->G = (int)tags.size();
+  m->h_tags = tags;
+  m->h_member_off.assign(m->G + 1, 0);
+  std::vector<std::vector<int32_t>> mem(m->G);
+  for (int64_t e = 0; e < N; ++e) {
+    auto it = std::lower_bound(tags.begin(), tags.end(), m->h_group[e]);
+    if (it != tags.end() && *it == m->h_group[e]) mem[it - tags.begin()].push_back((int32_t)e);
+  }
+  for (int g = 0; g < m->G; ++g) {
+    m->h_member_off[g + 1] = m->h_member_off[g] + (int64_t)mem[g].size();
+    m->h_members.insert(m->h_members.end(), mem[g].begin(), mem[g].end());
+  }
+
+  int rc;
+  if ((rc = upload(s, m->coords, d->coords, sizeof(double) * 3 * d->n_nodes))) return rc;
+  if ((rc = upload(s, m->enodes, m->h_enodes.data(), sizeof(int32_t) * 8 * N))) return rc;
+  if ((rc = upload(s, m->fam, m->h_fam.data(), N))) return rc;
+  if ((rc = upload(s, m->group, m->h_group.data(), sizeof(int32_t) * N))) return rc;
+  if ((rc = upload(s, m->member_off, m->h_member_off.data(), sizeof(int64_t) * (m->G + 1)))) return rc;
+  if ((rc = upload(s, m->members, m->h_members.data(), sizeof(int32_t) * m->h_members.size()))) return rc;
+
+  // obstruction BVH (exact tree of src/BVH.jl over the merged soup)
+  if (d->n_obs > 0) {
+    if (!d->obs_soup || !d->obs_group) return set_err(RVF_EINVAL, "obstruction soup arrays missing");
+    const int nv = d->obs_nv;
+    if ((d->mesh_dim == 2 && nv != 3) || (d->mesh_dim == 1 && nv != 2))
+      return set_err(RVF_EINVAL, "obs_nv %d does not match mesh_dim %d", nv, d->mesh_dim);
+    m->h_soup.assign(d->obs_soup, d->obs_soup + (size_t)3 * nv * d->n_obs);
+    m->h_obs_group.assign(d->obs_group, d->obs_group + d->n_obs);
+    for (double v : m->h_soup)
+      if (!std::isfinite(v)) return set_err(RVF_EINVAL, "obstruction soup holds a non-finite coordinate");
+    HostBVH b = build_bvh(m->h_soup.data(), nv, d->n_obs);
+    const int M = (int)b.nodes.size();
+    std::vector<NodeD> nodes(M);
+    for (int k = 0; k < M; ++k) {
+      const HostBVH::Node& h = b.nodes[k];
+      NodeD& n = nodes[k];
+      for (int c = 0; c < 3; ++c) { n.lo[c] = h.lo[c]; n.hi[c] = h.hi[c]; }
+      if (h.left != 0 && h.left != k + 2) return set_err(RVF_EINVAL, "internal: BVH is not in pre-order");
+      n.a = h.tri_count > 0 ? (int32_t)(h.tri_start - 1) : 0;
+      n.b = (int32_t)h.tri_count;
+      n.miss = h.miss == 0 ? M : (int32_t)(h.miss - 1);
+      n.pad = 0;
+    }
+    m->n_nodes = M;
+    m->h_nodes = nodes;
+    if ((rc = upload(s, m->nodes, nodes.data(), sizeof(NodeD) * M))) return rc;
+    const int64_t T = d->n_obs;
+    if (nv == 3) {
+      std::vector<TriD> tref(T), tgeo(T);
+      for (int64_t k = 0; k < T; ++k) {
+        int64_t t = b.tri_idx[k] - 1;
+        const double* sp = m->h_soup.data() + 9 * t;
+        double rv[3][3], gv[3][3];
+        for (int a = 0; a < 3; ++a)
+          for (int c = 0; c < 3; ++c) {
+            rv[a][c] = sp[a + 3 * c];  // bvh_tris[a, c, t]: the reference's read (src/GPUBVH.jl:243-245)
+            gv[a][c] = sp[c + 3 * a];  // true vertex a
+          }
+        for (int pass = 0; pass < 2; ++pass) {
+          double(*v)[3] = pass == 0 ? rv : gv;
+          TriD& o = pass == 0 ? tref[k] : tgeo[k];
+          for (int c = 0; c < 3; ++c) {
+            o.v0[c] = v[0][c];
+            o.e1[c] = v[1][c] - v[0][c];
+            o.e2[c] = v[2][c] - v[0][c];
+          }
+          o.group = m->h_obs_group[t];
+          o.pad = 0;
+        }
+      }
+      if ((rc = upload(s, m->tris_ref, tref.data(), sizeof(TriD) * T))) return rc;
+      if ((rc = upload(s, m->tris_geo, tgeo.data(), sizeof(TriD) * T))) return rc;
+    } else {
+      std::vector<SegD> segs(T);
+      for (int64_t k = 0; k < T; ++k) {
+        int64_t t = b.tri_idx[k] - 1;
+        const double* sp = m->h_soup.data() + 6 * t;
+        segs[k] = SegD{sp[0], sp[1], sp[3], sp[4], m->h_obs_group[t], 0, 0, 0};
+      }
+      if ((rc = upload(s, m->segs, segs.data(), sizeof(SegD) * T))) return rc;
+    }
+    m->n_obs = T;
+  }
+  cudaError_t e = cudaStreamSynchronize(s->stream);
+  if (e != cudaSuccess) return cuda_err(e, "mesh upload");
+  *out = m.release();
+  return RVF_OK;
+}
+
+// ---------------------------------------------------------------------------
+// quadrature tables for one nquad
+// ---------------------------------------------------------------------------
+int ensure_tables(Session* s, rvf_mesh* m, int nquad, Tables** out) {
+  auto it = m->tables.find(nquad);
+  if (it != m->tables.end()) { *out = it->second.get(); return RVF_OK; }
+  Rule q = gl2d(nquad), t = tri_rule(nquad), l = line_rule(nquad);
+  bool has_q = false, has_t = false, has_l = false;
+  for (int8_t f : m->h_fam) {
+    if (f == 0 || f == 2) has_q = true;
+    else if (f == 1 || f == 3) has_t = true;
+    else has_l = true;
+  }
+  int pmax = std::max({has_q ? q.size() : 0, has_t ? t.size() : 0, has_l ? l.size() : 0, 1});
+  if (pmax > kMaxPts)
+    return set_err(RVF_EUNSUPPORTED, "nquad=%d gives %d points per element; at most %d are supported", nquad, pmax,
+                   kMaxPts);
+  auto T = std::make_unique<Tables>();
+  T->nquad = nquad;
+  T->pmax = pmax;
+  const int64_t N = m->N;
+  const int64_t nT = (N + kTile - 1) / kTile;
+  int rc;
+  std::vector<double> rules;
+  auto push = [&](const std::vector<double>& v) { rules.insert(rules.end(), v.begin(), v.end()); };
+  push(q.xi); push(q.eta); push(q.w); push(t.xi); push(t.eta); push(t.w); push(l.xi); push(l.w);
+  if ((rc = upload(s, T->rules, rules.data(), sizeof(double) * rules.size()))) return rc;
+  if ((rc = T->tab.alloc(s, sizeof(double) * nT * kComp * pmax * kTile))) return rc;
+  if ((rc = T->area.alloc(s, sizeof(double) * std::max<int64_t>(N, 1)))) return rc;
+  if ((rc = T->np.alloc(s, std::max<int64_t>(N, 1)))) return rc;
+  if ((rc = T->flat.alloc(s, std::max<int64_t>(N, 1)))) return rc;
+  if ((rc = T->nrm.alloc(s, sizeof(double) * 3 * std::max<int64_t>(N, 1)))) return rc;
+  if ((rc = T->cen.alloc(s, sizeof(double) * 3 * std::max<int64_t>(N, 1)))) return rc;
+  if ((rc = T->diam.alloc(s, sizeof(double) * std::max<int64_t>(N, 1)))) return rc;
+  cudaMemsetAsync(T->tab.ptr, 0, T->tab.bytes, s->stream);
+  cudaMemsetAsync(s->err.ptr, 0, sizeof(int), s->stream);
+  PrepArgs a{};
+  a.N = N;
+  a.pmax = pmax;
+  a.coords = (const double*)m->coords.ptr;
+  a.enodes = (const int32_t*)m->enodes.ptr;
+  a.fam = (const int8_t*)m->fam.ptr;
+  const double* r = (const double*)T->rules.ptr;
+  a.qx = r; r += q.size(); a.qe = r; r += q.size(); a.qw = r; r += q.size();
+  a.tx = r; r += t.size(); a.te = r; r += t.size(); a.tw = r; r += t.size();
+  a.lx = r; r += l.size(); a.lw = r;
+  a.nquadpts = q.size(); a.ntripts = t.size(); a.nline = l.size();
+  a.tab = (double*)T->tab.ptr;
+  a.area = (double*)T->area.ptr;
+  a.np = (int8_t*)T->np.ptr;
+  a.flat = (uint8_t*)T->flat.ptr;
+  a.nrm = (double*)T->nrm.ptr;
+  a.cen = (double*)T->cen.ptr;
+  a.diam = (double*)T->diam.ptr;
+  a.err = (int*)s->err.ptr;
+  cudaError_t e = launch_prep(a, s->stream);
+  if (e != cudaSuccess) return cuda_err(e, "prep kernel launch");
+  int herr = 0;
+  e = cudaMemcpyAsync(&herr, s->err.ptr, sizeof(int), cudaMemcpyDeviceToHost, s->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+  if (e != cudaSuccess) return cuda_err(e, "prep kernel");
+  if (herr & kErrBadInput)
+    return set_err(RVF_EINVAL, "mesh holds a degenerate element (zero or non-finite area element at a quadrature point)");
+  if (N == 1) cudaMemsetAsync(T->area.ptr, 0, sizeof(double), s->stream);  // no pair writes area_out
+  *out = T.get();
+  m->tables[nquad] = std::move(T);
+  return RVF_OK;
+}
+
+}  // namespace rvf

@@ -1,0 +1,78 @@
+// kernels.h -- launch arguments and launchers of the librvf_b200 kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "rvf_host.h"
+
+namespace rvf {
+
+struct PrepArgs {
+  int64_t N;
+  int pmax;
+  const double* coords;   // 3 x n_nodes
+  const int32_t* enodes;  // N x 8, 0-based node ids
+  const int8_t* fam;
+  // rules (device pointers)
+  const double *qx, *qe, *qw, *tx, *te, *tw, *lx, *lw;
+  int nquadpts, ntripts, nline;
+  // outputs
+  double* tab;     // tiles x kComp x pmax x 32
+  double* area;
+  int8_t* np;
+  uint8_t* flat;
+  double* nrm;     // 3N
+  double* cen;     // 3N
+  double* diam;    // N
+  int* err;
+};
+
+struct PairArgs {
+  int64_t N;
+  int64_t nT;       // tiles per side
+  int64_t n_tiles;  // nT (nT + 1) / 2
+  int pmax;
+  bool dim3;
+  const double* tab;
+  const int8_t* np;
+  const double* area;
+  const uint8_t* flat;
+  const double* nrm;
+  const int32_t* group;
+  double* F;        // N x N column-major
+  // occlusion (n_nodes == 0: none)
+  const NodeD* nodes;
+  int n_nodes;
+  bool nodes_in_smem;
+  const TriD* tris;
+  const SegD* segs;
+  unsigned long long* tile_counter;
+  unsigned long long* counters;  // [point pairs, rays, node visits, primitive tests]
+  int* err;
+  uint8_t* ray_log;              // device, or null
+  int log_pm;
+};
+
+struct RedArgs {
+  int64_t N;
+  int G;
+  int n_chunks;
+  const double* F;
+  const double* area;
+  const int64_t* member_off;  // G+1
+  const int32_t* members;     // element ids grouped by group (ascending within a group)
+  double* part;               // n_chunks x G x N
+  double* rowgroup;           // G x N
+  double* rowsum;             // N
+  double* Fgroup;             // G x G column-major
+  double* Agroup;             // G
+};
+
+cudaError_t launch_prep(const PrepArgs& a, cudaStream_t st);
+size_t pair_smem_bytes(int pmax, int n_nodes_smem);
+cudaError_t launch_pairs_fp64(const PairArgs& a, int sm_count, cudaStream_t st);
+cudaError_t launch_reduce(const RedArgs& a, cudaStream_t st);
+
+}  // namespace rvf

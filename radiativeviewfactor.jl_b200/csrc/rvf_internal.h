@@ -1,0 +1,96 @@
+// rvf_internal.h -- session / mesh state behind the C ABI.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdint>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <set>
+#include <string>
+#include <vector>
+
+#include "../../include/rvf_b200.h"
+#include "rvf_host.h"
+
+struct rvf_session;
+
+namespace rvf {
+
+using Session = ::rvf_session;
+
+int set_err(int code, const char* fmt, ...);
+int cuda_err(cudaError_t e, const char* what);
+extern thread_local std::string g_last_error;
+
+// Device allocation charged against the session's HBM budget.
+struct DevBuf {
+  void* ptr = nullptr;
+  size_t bytes = 0;
+  Session* owner = nullptr;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  ~DevBuf() { free_(); }
+  int alloc(Session* s, size_t n);
+  void free_();
+  template <typename T>
+  T* as() const { return reinterpret_cast<T*>(ptr); }
+};
+
+int upload(Session* s, DevBuf& b, const void* src, size_t n);
+
+struct Tables {
+  int nquad = 0, pmax = 0;
+  DevBuf rules, tab, area, np, flat, nrm, cen, diam;
+};
+
+}  // namespace rvf
+
+struct rvf_session {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  size_t budget = 0, used = 0;
+  int sm_count = 0;
+  size_t smem_optin = 0;
+  std::mutex mu;
+  rvf::DevBuf err;           // int
+  rvf::DevBuf tile_counter;  // u64
+  rvf::DevBuf counters;      // u64 x 8
+  std::set<rvf_mesh*> meshes;
+  cudaEvent_t ev[8] = {};
+};
+
+struct rvf_mesh {
+  rvf_session* s = nullptr;
+  int dim = 2;
+  int64_t N = 0, Nn = 0;
+  // host copies
+  std::vector<int32_t> h_enodes;  // N x 8, 0-based
+  std::vector<int8_t> h_fam;
+  std::vector<int32_t> h_group;
+  std::vector<int32_t> h_tags;
+  std::vector<int64_t> h_member_off;
+  std::vector<int32_t> h_members;
+  std::vector<double> h_soup;
+  std::vector<int32_t> h_obs_group;
+  std::vector<rvf::NodeD> h_nodes;
+  int G = 0;
+  // device
+  rvf::DevBuf coords, enodes, fam, group, member_off, members;
+  rvf::DevBuf nodes, tris_ref, tris_geo, segs;
+  int n_nodes = 0;
+  int64_t n_obs = 0;
+  std::map<int, std::unique_ptr<rvf::Tables>> tables;
+  // results of the last solve
+  rvf::DevBuf F, part, rowgroup, rowsum, Fgroup, Agroup;
+  int result_nquad = -1;
+  bool has_result = false;
+};
+
+namespace rvf {
+int mesh_upload(Session* s, const rvf_mesh_desc* d, rvf_mesh** out);
+int ensure_tables(Session* s, rvf_mesh* m, int nquad, Tables** out);
+}  // namespace rvf

@@ -1,0 +1,405 @@
+// solve.cpp -- extern "C" entry points of librvf_b200 (include/rvf_b200.h).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <vector>
+
+#include "../../include/rvf_b200.h"
+#include "kernels.h"
+#include "rvf_internal.h"
+
+using namespace rvf;
+
+namespace {
+
+struct EvTimer {
+  cudaStream_t st;
+  cudaEvent_t a = nullptr, b = nullptr;
+  explicit EvTimer(cudaStream_t s) : st(s) {
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    cudaEventRecord(a, st);
+  }
+  double stop() {
+    cudaEventRecord(b, st);
+    cudaEventSynchronize(b);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, a, b);
+    return ms;
+  }
+  ~EvTimer() {
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+  }
+};
+
+int read_err(Session* s) {
+  int herr = 0;
+  cudaError_t e = cudaMemcpyAsync(&herr, s->err.ptr, sizeof(int), cudaMemcpyDeviceToHost, s->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+  if (e != cudaSuccess) return cuda_err(e, "kernel execution");
+  if (herr & kErrWaitTimeout) return set_err(RVF_ETIMEDOUT, "a bounded device wait gave up (shared-memory copy did not complete)");
+  if (herr & kErrBadInput) return set_err(RVF_EINVAL, "kernel reported invalid input");
+  return RVF_OK;
+}
+
+int validate_options(const rvf_mesh* m, const rvf_options* o) {
+  if (o->nquad < 1) return set_err(RVF_EINVAL, "nquad must be >= 1, got %d", o->nquad);
+  if (o->method != RVF_METHOD_QUADRATURE && o->method != RVF_METHOD_MONTE_CARLO)
+    return set_err(RVF_EINVAL, "unknown method %d", o->method);
+  if (o->precision != RVF_PREC_FP64 && o->precision != RVF_PREC_MIXED)
+    return set_err(RVF_EINVAL, "unknown precision %d", o->precision);
+  if (o->method == RVF_METHOD_MONTE_CARLO && o->use_duffy)
+    return set_err(RVF_EINVAL, "use_duffy and monte_carlo cannot both be true.");  // src/Assembly.jl:79-80
+  if (o->method == RVF_METHOD_MONTE_CARLO && o->n_samples < 1)
+    return set_err(RVF_EINVAL, "n_samples must be >= 1");
+  if (o->ray_log && o->ray_log_pm < 1) return set_err(RVF_EINVAL, "ray_log needs ray_log_pm >= 1");
+  (void)m;
+  return RVF_OK;
+}
+
+int run_reduce(Session* s, rvf_mesh* m, Tables* T) {
+  const int64_t N = m->N;
+  if (N == 0 || m->G == 0) return RVF_OK;
+  int n_chunks = (int)std::min<int64_t>(256, std::max<int64_t>(1, (1 << 20) / std::max<int64_t>(N, 1)));
+  int rc;
+  if (m->part.bytes < sizeof(double) * n_chunks * m->G * N)
+    if ((rc = m->part.alloc(s, sizeof(double) * n_chunks * m->G * N))) return rc;
+  if (m->rowgroup.bytes < sizeof(double) * m->G * N)
+    if ((rc = m->rowgroup.alloc(s, sizeof(double) * m->G * N))) return rc;
+  if (m->rowsum.bytes < sizeof(double) * N)
+    if ((rc = m->rowsum.alloc(s, sizeof(double) * N))) return rc;
+  if (m->Fgroup.bytes < sizeof(double) * m->G * m->G)
+    if ((rc = m->Fgroup.alloc(s, sizeof(double) * m->G * m->G))) return rc;
+  if (m->Agroup.bytes < sizeof(double) * m->G)
+    if ((rc = m->Agroup.alloc(s, sizeof(double) * m->G))) return rc;
+  RedArgs r{};
+  r.N = N;
+  r.G = m->G;
+  r.n_chunks = n_chunks;
+  r.F = m->F.as<double>();
+  r.area = T->area.as<double>();
+  r.member_off = m->member_off.as<int64_t>();
+  r.members = m->members.as<int32_t>();
+  r.part = m->part.as<double>();
+  r.rowgroup = m->rowgroup.as<double>();
+  r.rowsum = m->rowsum.as<double>();
+  r.Fgroup = m->Fgroup.as<double>();
+  r.Agroup = m->Agroup.as<double>();
+  cudaError_t e = launch_reduce(r, s->stream);
+  return e == cudaSuccess ? RVF_OK : cuda_err(e, "reduction kernels");
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* rvf_version(void) { return "rvf_b200 0.1.0 (sm_100a)"; }
+int rvf_abi_version(void) { return RVF_ABI_VERSION; }
+
+int rvf_last_error(char* buf, size_t n) {
+  if (!buf || n == 0) return (int)g_last_error.size();
+  size_t k = std::min(n - 1, g_last_error.size());
+  std::memcpy(buf, g_last_error.data(), k);
+  buf[k] = 0;
+  return (int)g_last_error.size();
+}
+
+void rvf_default_options(rvf_options* o) {
+  if (!o) return;
+  std::memset(o, 0, sizeof(*o));
+  o->nquad = 4;  // src/Assembly.jl:65
+  o->method = RVF_METHOD_QUADRATURE;
+  o->n_samples = 10000;  // src/Assembly.jl:70
+  o->seed = 0;
+  o->precision = RVF_PREC_FP64;
+  o->occlusion = 1;
+  o->near_field_factor = 2.0;
+}
+
+int rvf_session_create(const rvf_session_opts* opts, rvf_session** out) {
+  if (!out) return set_err(RVF_EINVAL, "null out");
+  *out = nullptr;
+  int dev = opts ? opts->device : 0;
+  int n = 0;
+  cudaError_t e = cudaGetDeviceCount(&n);
+  if (e != cudaSuccess || n == 0) {
+    cudaGetLastError();
+    return set_err(RVF_ENODEV, "no CUDA device available (%s)", cudaGetErrorString(e));
+  }
+  if (dev < 0 || dev >= n) return set_err(RVF_ENODEV, "device %d out of range (%d devices)", dev, n);
+  cudaDeviceProp p;
+  if ((e = cudaGetDeviceProperties(&p, dev)) != cudaSuccess) return cuda_err(e, "cudaGetDeviceProperties");
+  if (p.major < 10) return set_err(RVF_ENODEV, "device %d is sm_%d%d; this library is built for sm_100a", dev, p.major, p.minor);
+  if ((e = cudaSetDevice(dev)) != cudaSuccess) return cuda_err(e, "cudaSetDevice");
+  auto s = std::make_unique<rvf_session>();
+  s->device = dev;
+  s->sm_count = p.multiProcessorCount;
+  s->smem_optin = p.sharedMemPerBlockOptin;
+  if ((e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking)) != cudaSuccess)
+    return cuda_err(e, "cudaStreamCreate");
+  size_t fr = 0, tot = 0;
+  cudaMemGetInfo(&fr, &tot);
+  s->budget = (opts && opts->hbm_budget_bytes) ? opts->hbm_budget_bytes : (size_t)(0.9 * (double)fr);
+  int rc;
+  if ((rc = s->err.alloc(s.get(), 256))) return rc;
+  if ((rc = s->tile_counter.alloc(s.get(), 256))) return rc;
+  if ((rc = s->counters.alloc(s.get(), 256))) return rc;
+  *out = s.release();
+  return RVF_OK;
+}
+
+int rvf_session_destroy(rvf_session* s) {
+  if (!s) return RVF_OK;
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    cudaSetDevice(s->device);
+    cudaStreamSynchronize(s->stream);
+    for (rvf_mesh* m : s->meshes) delete m;
+    s->meshes.clear();
+    s->err.free_();
+    s->tile_counter.free_();
+    s->counters.free_();
+    cudaStreamDestroy(s->stream);
+  }
+  delete s;
+  return RVF_OK;
+}
+
+int rvf_device_info(rvf_session* s, int* sm_count, uint64_t* hbm_total, uint64_t* hbm_free) {
+  if (!s) return set_err(RVF_EINVAL, "null session");
+  cudaSetDevice(s->device);
+  size_t fr = 0, tot = 0;
+  cudaMemGetInfo(&fr, &tot);
+  if (sm_count) *sm_count = s->sm_count;
+  if (hbm_total) *hbm_total = tot;
+  if (hbm_free) *hbm_free = fr;
+  return RVF_OK;
+}
+
+int rvf_mesh_upload(rvf_session* s, const rvf_mesh_desc* d, rvf_mesh** out) {
+  if (!s) return set_err(RVF_EINVAL, "null session");
+  std::lock_guard<std::mutex> lk(s->mu);
+  cudaSetDevice(s->device);
+  int rc = mesh_upload(s, d, out);
+  if (rc == RVF_OK) s->meshes.insert(*out);
+  return rc;
+}
+
+int rvf_mesh_release(rvf_session* s, rvf_mesh* m) {
+  if (!s || !m) return set_err(RVF_EINVAL, "null argument");
+  std::lock_guard<std::mutex> lk(s->mu);
+  if (!s->meshes.count(m)) return set_err(RVF_EINVAL, "mesh does not belong to this session");
+  cudaSetDevice(s->device);
+  cudaStreamSynchronize(s->stream);
+  s->meshes.erase(m);
+  delete m;
+  return RVF_OK;
+}
+
+int rvf_mesh_n_elems(const rvf_mesh* m, int64_t* n) {
+  if (!m || !n) return set_err(RVF_EINVAL, "null argument");
+  *n = m->N;
+  return RVF_OK;
+}
+
+int rvf_solve(rvf_session* s, rvf_mesh* m, const rvf_options* o, double* F_elem, double* A_elem, double* F_group,
+              double* A_group, double* row_sums, rvf_stats* st) {
+  if (!s || !m || !o) return set_err(RVF_EINVAL, "null argument");
+  std::lock_guard<std::mutex> lk(s->mu);
+  if (!s->meshes.count(m)) return set_err(RVF_EINVAL, "mesh does not belong to this session");
+  cudaSetDevice(s->device);
+  int rc = validate_options(m, o);
+  if (rc) return rc;
+  if (o->method == RVF_METHOD_MONTE_CARLO) return set_err(RVF_EUNSUPPORTED, "Monte Carlo is not available in this build");
+  if (o->use_duffy) return set_err(RVF_EUNSUPPORTED, "use_duffy is not available in this build");
+  if (o->precision == RVF_PREC_MIXED) return set_err(RVF_EUNSUPPORTED, "mixed precision is not available in this build");
+  rvf_stats S{};
+  int64_t n_kernels = 0;  // kernels of this library launched by this call
+  EvTimer total(s->stream);
+  const int64_t N = m->N;
+  Tables* T = nullptr;
+  {
+    EvTimer t(s->stream);
+    const bool fresh = m->tables.find(o->nquad) == m->tables.end();
+    if ((rc = ensure_tables(s, m, o->nquad, &T))) return rc;
+    if (fresh && N > 0) n_kernels += 1;
+    S.ms_prep = t.stop();
+  }
+  if (m->F.bytes < sizeof(double) * N * N)
+    if ((rc = m->F.alloc(s, sizeof(double) * std::max<int64_t>(N * N, 1)))) return rc;
+  m->has_result = false;
+  cudaMemsetAsync(s->tile_counter.ptr, 0, 8, s->stream);
+  cudaMemsetAsync(s->counters.ptr, 0, 64, s->stream);
+  cudaMemsetAsync(s->err.ptr, 0, sizeof(int), s->stream);
+  DevBuf log;
+  if (o->ray_log) {
+    if (o->ray_log_pm < T->pmax) return set_err(RVF_EINVAL, "ray_log_pm %d < points per element %d", o->ray_log_pm, T->pmax);
+    size_t lb = (size_t)N * N * o->ray_log_pm * o->ray_log_pm;
+    if ((rc = log.alloc(s, lb))) return rc;
+    cudaMemsetAsync(log.ptr, 0, lb, s->stream);
+  }
+  const bool occ = o->occlusion && m->n_nodes > 0;
+  PairArgs a{};
+  a.N = N;
+  a.nT = (N + kTile - 1) / kTile;
+  a.n_tiles = a.nT * (a.nT + 1) / 2;
+  a.pmax = T->pmax;
+  a.dim3 = (m->dim == 2);
+  a.tab = T->tab.as<double>();
+  a.np = T->np.as<int8_t>();
+  a.area = T->area.as<double>();
+  a.flat = T->flat.as<uint8_t>();
+  a.nrm = T->nrm.as<double>();
+  a.group = m->group.as<int32_t>();
+  a.F = m->F.as<double>();
+  a.nodes = occ ? m->nodes.as<NodeD>() : nullptr;
+  a.n_nodes = occ ? m->n_nodes : 0;
+  const size_t base_smem = pair_smem_bytes(T->pmax, 0);
+  a.nodes_in_smem = occ && (base_smem + sizeof(NodeD) * (size_t)m->n_nodes <= std::min<size_t>(s->smem_optin, 96 * 1024));
+  a.tris = occ ? (o->geometric_soup ? m->tris_geo.as<TriD>() : m->tris_ref.as<TriD>()) : nullptr;
+  a.segs = occ ? m->segs.as<SegD>() : nullptr;
+  a.tile_counter = s->tile_counter.as<unsigned long long>();
+  a.counters = s->counters.as<unsigned long long>();
+  a.err = s->err.as<int>();
+  a.ray_log = o->ray_log ? log.as<uint8_t>() : nullptr;
+  a.log_pm = o->ray_log_pm;
+  if (N > 0) {
+    if (N == 1) {
+      cudaMemsetAsync(m->F.ptr, 0, sizeof(double), s->stream);
+    }
+    EvTimer t(s->stream);
+    cudaError_t e = launch_pairs_fp64(a, s->sm_count, s->stream);
+    n_kernels += 1;
+    if (e != cudaSuccess) return cuda_err(e, "pair kernel launch");
+    S.ms_pairs = t.stop();
+    if ((rc = read_err(s))) return rc;
+    if (N == 1) {  // raw 1x1 zero, area 0 -> F = 0/0 (the reference's result for one element)
+      double nanv = std::nan("");
+      cudaMemcpyAsync(m->F.ptr, &nanv, sizeof(double), cudaMemcpyHostToDevice, s->stream);
+    }
+  }
+  {
+    EvTimer t(s->stream);
+    if ((rc = run_reduce(s, m, T))) return rc;
+    if (N > 0 && m->G > 0) n_kernels += 3;
+    S.ms_reduce = t.stop();
+  }
+  m->has_result = true;
+  m->result_nquad = o->nquad;
+  {
+    EvTimer t(s->stream);
+    cudaError_t e = cudaSuccess;
+    if (F_elem && N > 0) e = cudaMemcpyAsync(F_elem, m->F.ptr, sizeof(double) * N * N, cudaMemcpyDeviceToHost, s->stream);
+    if (e == cudaSuccess && A_elem && N > 0) e = cudaMemcpyAsync(A_elem, T->area.ptr, sizeof(double) * N, cudaMemcpyDeviceToHost, s->stream);
+    if (e == cudaSuccess && F_group && m->G > 0 && N > 0)
+      e = cudaMemcpyAsync(F_group, m->Fgroup.ptr, sizeof(double) * m->G * m->G, cudaMemcpyDeviceToHost, s->stream);
+    if (e == cudaSuccess && A_group && m->G > 0 && N > 0)
+      e = cudaMemcpyAsync(A_group, m->Agroup.ptr, sizeof(double) * m->G, cudaMemcpyDeviceToHost, s->stream);
+    if (e == cudaSuccess && row_sums && N > 0)
+      e = cudaMemcpyAsync(row_sums, m->rowsum.ptr, sizeof(double) * N, cudaMemcpyDeviceToHost, s->stream);
+    if (e == cudaSuccess && o->ray_log)
+      e = cudaMemcpyAsync(o->ray_log, log.ptr, log.bytes, cudaMemcpyDeviceToHost, s->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+    if (e != cudaSuccess) return cuda_err(e, "device->host copy");
+    S.ms_download = t.stop();
+  }
+  if (st) {
+    unsigned long long c[8] = {};
+    cudaMemcpy(c, s->counters.ptr, sizeof c, cudaMemcpyDeviceToHost);
+    S.n_pairs = N * (N - 1) / 2;
+    S.n_point_pairs = (int64_t)c[0];
+    S.n_rays = (int64_t)c[1];
+    S.n_rays_fp64 = (int64_t)c[1];
+    S.reserved[0] = (int64_t)c[2];
+    S.reserved[1] = (int64_t)c[3];
+    S.reserved[2] = n_kernels;
+    if (N > 0 && m->G > 0) {
+      std::vector<double> rs(N);
+      cudaMemcpy(rs.data(), m->rowsum.ptr, sizeof(double) * N, cudaMemcpyDeviceToHost);
+      double mx = 0.0;
+      for (double v : rs) mx = std::max(mx, std::fabs(v - 1.0));
+      S.max_row_sum_dev = mx;
+    }
+    S.ms_total = total.stop();
+    *st = S;
+  }
+  return RVF_OK;
+}
+
+int rvf_result_copy(rvf_session* s, rvf_mesh* m, double* F_elem, double* A_elem) {
+  if (!s || !m) return set_err(RVF_EINVAL, "null argument");
+  std::lock_guard<std::mutex> lk(s->mu);
+  if (!m->has_result) return set_err(RVF_EINVAL, "no result on this mesh yet");
+  cudaSetDevice(s->device);
+  Tables* T = m->tables[m->result_nquad].get();
+  cudaError_t e = cudaSuccess;
+  if (F_elem) e = cudaMemcpyAsync(F_elem, m->F.ptr, sizeof(double) * m->N * m->N, cudaMemcpyDeviceToHost, s->stream);
+  if (e == cudaSuccess && A_elem) e = cudaMemcpyAsync(A_elem, T->area.ptr, sizeof(double) * m->N, cudaMemcpyDeviceToHost, s->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+  return e == cudaSuccess ? RVF_OK : cuda_err(e, "rvf_result_copy");
+}
+
+int rvf_result_device(rvf_mesh* m, const double** F_dev, const double** A_dev) {
+  if (!m) return set_err(RVF_EINVAL, "null mesh");
+  if (!m->has_result) return set_err(RVF_EINVAL, "no result on this mesh yet");
+  if (F_dev) *F_dev = m->F.as<double>();
+  if (A_dev) *A_dev = m->tables[m->result_nquad]->area.as<double>();
+  return RVF_OK;
+}
+
+int rvf_host_alloc(size_t bytes, void** p) {
+  if (!p) return set_err(RVF_EINVAL, "null out");
+  cudaError_t e = cudaHostAlloc(p, bytes, cudaHostAllocDefault);
+  if (e != cudaSuccess) {
+    *p = nullptr;
+    return set_err(RVF_ENOMEM, "cudaHostAlloc(%zu): %s", bytes, cudaGetErrorString(e));
+  }
+  return RVF_OK;
+}
+
+int rvf_host_free(void* p) {
+  if (p) cudaFreeHost(p);
+  return RVF_OK;
+}
+
+int rvf_quadrature_rule(int32_t family, int32_t nquad, double* pts, double* wts, int32_t* n_pts) {
+  if (family < 0 || family > 5 || nquad < 1) return set_err(RVF_EINVAL, "bad family/nquad");
+  Rule r = (family == 0 || family == 2) ? gl2d(nquad) : (family == 1 || family == 3) ? tri_rule(nquad) : line_rule(nquad);
+  if (n_pts) *n_pts = r.size();
+  for (int k = 0; k < r.size(); ++k) {
+    if (pts) { pts[2 * k] = r.xi[k]; pts[2 * k + 1] = r.eta[k]; }
+    if (wts) wts[k] = r.w[k];
+  }
+  return RVF_OK;
+}
+
+int rvf_bvh_build_host(const double* soup, int32_t nv, int64_t n_prims, double* lo, double* hi, int32_t* meta,
+                       int32_t* tri_idx, int64_t* n_nodes) {
+  if (!soup || n_prims <= 0 || (nv != 2 && nv != 3)) return set_err(RVF_EINVAL, "bad soup");
+  HostBVH b = build_bvh(soup, nv, n_prims);
+  if (n_nodes) *n_nodes = (int64_t)b.nodes.size();
+  if (!lo) return RVF_OK;
+  for (size_t k = 0; k < b.nodes.size(); ++k) {
+    const HostBVH::Node& n = b.nodes[k];
+    for (int c = 0; c < 3; ++c) {
+      lo[3 * k + c] = n.lo[c];
+      if (hi) hi[3 * k + c] = n.hi[c];
+    }
+    if (meta) {
+      meta[5 * k + 0] = (int32_t)n.left;
+      meta[5 * k + 1] = (int32_t)n.right;
+      meta[5 * k + 2] = (int32_t)n.tri_start;
+      meta[5 * k + 3] = (int32_t)n.tri_count;
+      meta[5 * k + 4] = (int32_t)n.miss;
+    }
+  }
+  if (tri_idx)
+    for (int64_t t = 0; t < n_prims; ++t) tri_idx[t] = (int32_t)b.tri_idx[t];
+  return RVF_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,180 @@
+"""CPU tests of the boundary: the C-ABI library loads and exports every
+symbol declared in include/rvf_b200.h, its host-side pieces (quadrature rules,
+BVH build) match the oracle bit for bit, and the Python mirror of the
+reference API behaves like src/Assembly.jl.  No compute call needs a GPU."""
+import ctypes
+import re
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from conftest import ROOT, load_pkg
+
+HEADER = ROOT / "include" / "rvf_b200.h"
+
+
+@pytest.fixture(scope="module")
+def lib(rvf):
+    from importlib import import_module
+    import_module("rvf_b200.build").build()
+    return rvf.load_library()
+
+
+def declared_functions():
+    text = HEADER.read_text()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(rvf_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_exports_every_declared_symbol(lib, rvf):
+    names = declared_functions()
+    assert len(names) >= 15
+    for n in names:
+        assert hasattr(lib, n), f"{n} declared in rvf_b200.h but not exported"
+    # and the ctypes table binds exactly the declared set
+    from rvf_b200 import _abi
+    assert sorted(_abi.SIGNATURES) == names
+
+
+def test_version_and_defaults(lib, rvf):
+    from rvf_b200 import _abi
+    assert b"sm_100a" in lib.rvf_version()
+    assert lib.rvf_abi_version() == 1
+    o = _abi.default_options()
+    assert o.nquad == 4 and o.n_samples == 10000 and o.method == 0 and o.precision == 0
+    assert o.near_field_factor == 2.0
+
+
+def test_struct_sizes_match_header(lib):
+    """Compile-free layout check: the C ABI structs as ctypes sees them."""
+    from rvf_b200 import _abi
+    assert ctypes.sizeof(_abi.Options) == 4 * 4 + 8 + 4 * 4 + 8 + 8 + 4 + 4 * 8 + 4  # trailing pad to 8
+    assert ctypes.sizeof(_abi.MeshDesc) % 8 == 0
+
+
+def test_session_without_gpu_reports_enodev(lib, rvf):
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    with pytest.raises(rvf.RVFError) as ei:
+        rvf.Session(0)
+    assert ei.value.status == -8
+
+
+@pytest.mark.parametrize("family,code", [("quad", 0), ("tri", 1), ("line3", 4)])
+@pytest.mark.parametrize("nquad", [1, 2, 3, 4, 5, 6, 8])
+def test_quadrature_rules_bitwise(orc, family, code, nquad):
+    from rvf_b200 import _abi
+    P, W = _abi.quadrature_rule(code, nquad)
+    if family == "quad":
+        Po, Wo = orc.gl_2d(nquad)
+    elif family == "tri":
+        Po, Wo = orc.tri_rule(nquad)
+    else:
+        p, Wo = orc.gl_1d(nquad)
+        Po = np.vstack([p, np.zeros_like(p)])
+    assert P.shape == Po.shape
+    assert np.array_equal(P, Po) and np.array_equal(W, Wo)
+
+
+def _random_soup(rng, T, nv=3, jitter_ties=True):
+    s = rng.uniform(0, 1, size=(T, nv, 3))
+    if jitter_ties:  # many equal centroid keys: exercises the stable sort
+        s[: T // 2, :, 0] = np.round(s[: T // 2, :, 0], 1)
+    return s
+
+
+@pytest.mark.parametrize("T,nv", [(1, 3), (8, 3), (9, 3), (100, 3), (1728, 3), (37, 2), (800, 2)])
+def test_bvh_build_matches_oracle(orc, T, nv):
+    from rvf_b200 import _abi
+    rng = np.random.default_rng(T)
+    soup = _random_soup(rng, T, nv)
+    lo, hi, meta, idx = _abi.bvh_build_host(soup)
+    b = orc.BVH(soup)
+    lo2, hi2, meta2, idx2 = b.export()
+    assert np.array_equal(lo, lo2) and np.array_equal(hi, hi2)
+    assert np.array_equal(meta, meta2) and np.array_equal(idx, idx2)
+    # pre-order: every interior node's left child is the next node
+    for k in range(meta.shape[0]):
+        if meta[k, 0] != 0:
+            assert meta[k, 0] == k + 2
+
+
+def test_bvh_box_soup_matches_oracle(rvf, orc):
+    from rvf_b200 import _abi
+    soup = rvf.meshes.obstruction_box()
+    lo, hi, meta, idx = _abi.bvh_build_host(soup)
+    lo2, hi2, meta2, idx2 = orc.BVH(soup).export()
+    assert meta.shape[0] == 511
+    assert np.array_equal(meta, meta2) and np.array_equal(idx, idx2) and np.array_equal(lo, lo2)
+
+
+def test_flatten_mirrors_build_gpu_arrays(rvf):
+    md = rvf.meshes.parallel_plates(3, "quad")
+    node_idx, tables = rvf.flatten(md)
+    assert tables[0].shape == (18, 8) and all(t.shape[0] == 0 for f, t in enumerate(tables) if f != 0)
+    assert np.array_equal(node_idx, np.arange(1, 19))
+    assert np.array_equal(tables[0], md.elem_nodes)
+
+
+def test_merged_obstruction_order(rvf):
+    md = rvf.meshes.cube_enclosure(4, box_m=2)
+    soup, g = rvf.merged_obstruction(md, [7, 2, 99])
+    assert soup.shape == (48 + 32, 3, 3)
+    assert np.all(g[:48] == 7) and np.all(g[48:] == 2)
+    assert np.array_equal(soup[:48], md.group_tri_soup[7])
+
+
+def test_obs_soups_follow_reference_layout(rvf):
+    md = rvf.meshes.parallel_plates(2, "quad4")
+    s = md.group_tri_soup[1]
+    # quads split into (1,2,3) and (1,3,4), corner nodes (src/MeshIO.jl:660-671)
+    e0 = md.elem_nodes[0] - 1
+    X = md.coords.T
+    assert np.array_equal(s[0], X[[e0[0], e0[1], e0[2]]])
+    assert np.array_equal(s[1], X[[e0[0], e0[2], e0[3]]])
+
+
+def test_hook_registry_and_guards(rvf):
+    from rvf_b200 import assembly
+    md = rvf.meshes.parallel_plates(2, "quad4")
+    with pytest.raises(ValueError, match="cannot both be true"):
+        rvf.compute_view_factors(md, use_duffy=True, monte_carlo=True, backend=rvf.B200Backend())
+    with pytest.raises(NotImplementedError):
+        rvf.compute_view_factors(md, backend=rvf.CPU())
+    seen = {}
+
+    def fake(mesh, nquad, backend, FloatT, ArrayT, **kw):
+        seen.update(kw, nquad=nquad, FloatT=FloatT, ArrayT=ArrayT)
+        return "ok"
+    prev = assembly._GPU_HOOK_REF[0]
+    try:
+        rvf.register_gpu_hook(fake)
+        assert rvf.compute_view_factors(md, nquad=3, obstruction_groups=[1], verbose=False) == "ok"
+        assert seen["nquad"] == 3 and seen["obstruction_groups"] == [1] and seen["FloatT"] is np.float64
+        assert seen["monte_carlo"] is False and seen["n_samples"] == 10000
+        assert seen["ArrayT"] is np.ndarray
+    finally:
+        rvf.register_gpu_hook(prev)
+    assert assembly._GPU_HOOK_REF[0] is rvf.compute_view_factors_b200
+
+
+def test_unknown_backend_errors_like_reference(rvf):
+    md = rvf.meshes.parallel_plates(2, "quad4")
+
+    class Other:
+        pass
+    with pytest.raises(RuntimeError, match="No GPU array type registered"):
+        rvf.compute_view_factors(md, backend=Other())
+
+
+def test_curve_mesh_guard_for_backends_without_support(rvf):
+    md = rvf.meshes.cavity_2d(4, 4, 1)
+    from rvf_b200 import assembly
+
+    class Other:
+        pass
+    assert not assembly._gpu_supports(Other(), "curves")
+    with pytest.raises(ValueError, match="curve meshes"):
+        rvf.compute_view_factors(md, backend=Other())
