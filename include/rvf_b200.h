@@ -167,6 +167,26 @@ int rvf_quadrature_rule(int32_t family, int32_t nquad, double* pts, double* wts,
  * the denominator of the pair kernels' roofline (they are FMA-pipe bound). */
 int rvf_fma_peak(int32_t device, int32_t fp64, double* tflops);
 
+/* Plain FP64 assembly that allocates no memory (no counterpart in the
+ * reference).  For callers that cannot call cudaMalloc -- code under an
+ * allocator that owns all device memory, memory-capped services, hosts that
+ * hand the library pre-placed buffers only.  Inputs and outputs are the
+ * caller's device pointers: coords (3 x n_nodes column-major), elem_family
+ * (RVF_QUAD8..RVF_LINE2), elem_nodes (n_elems x 8 element-major, 1-based node
+ * ids, zero padded), elem_group; outputs F (n_elems^2 column-major, F[i,j] =
+ * raw/A_i as rvf_solve) and A (n_elems).  No obstruction, no group sums.
+ * Scratch lives in one fixed 16 MiB __device__ array inside the library
+ * (held by every GPU that loads the library until exit); a mesh whose tables
+ * need more (about 90 B per element + 1792 B per 32 elements per quadrature
+ * point) is rejected with RVF_EINVAL.  The first call on a device looks up
+ * that array's device address, so make it before any stream capture.  Calls
+ * share the array; they take a process-wide lock and synchronise `stream`
+ * (a cudaStream_t, NULL = legacy default stream) before returning, because
+ * calls that overlapped on the GPU would race on it. */
+int rvf_solve_fp64_noalloc(const double* coords, int64_t n_nodes, const int8_t* elem_family,
+                           const int32_t* elem_nodes, const int32_t* elem_group, int64_t n_elems, int32_t mesh_dim,
+                           int32_t nquad, double* F, double* A, void* stream);
+
 /* Host-side BVH build of rvf_mesh_upload (build_bvh, src/BVH.jl:71-148, plus
  * the miss links of src/GPUBVH.jl:69-82), exported for cross-checks; needs no
  * GPU.  Call with lo == NULL to get the node count in *n_nodes; then lo/hi

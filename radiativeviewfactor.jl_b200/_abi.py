@@ -83,6 +83,8 @@ SIGNATURES = {
     "rvf_quadrature_rule": (C.c_int, [C.c_int32, C.c_int32, _pd, _pd, _pi32]),
     "rvf_bvh_build_host": (C.c_int, [_pd, C.c_int32, C.c_int64, _pd, _pd, _pi32, _pi32, C.POINTER(C.c_int64)]),
     "rvf_fma_peak": (C.c_int, [C.c_int32, C.c_int32, _pd]),
+    "rvf_solve_fp64_noalloc": (C.c_int, [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64,
+                                         C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p]),
 }
 
 
