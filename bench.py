@@ -55,6 +55,9 @@ def load_pkg():
 def workload(rvf, size: str):
     if size == "small":  # quick check of the same shape at m = 12
         return rvf.meshes.cube_enclosure(12, box_m=4), "cube 12x12/face Tri3 (1,728 elements) + box"
+    if size == "medium":  # profiling size: F = 382 MB > L2, same box
+        return (rvf.meshes.cube_enclosure(24, jitter=0.3, seed=2, box=True, box_edge=0.3, box_m=12),
+                "cube 24x24/face jittered Tri3 (6,912 elements) + centred 0.3 box (1,728 tris), nquad=3")
     return (rvf.meshes.cube_enclosure(60, jitter=0.3, seed=2, box=True, box_edge=0.3, box_m=12),
             "closed cube 60x60/face jittered Tri3 (43,200 elements) + centred 0.3 box (1,728 tris), "
             "Dunavant 7-pt (nquad=3), dense FP64 F")
@@ -189,6 +192,34 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def timed_solves(dm, opts, steps, warmup, flush, ws, local):
+    """W untimed + K timed resident solves; returns per-step stats and clocks."""
+    import torch
+    for _ in range(warmup):
+        dm.solve(opts)
+    barrier(ws)
+    torch.cuda.synchronize()
+    stats = []
+    with Clocks(local) as clk:
+        for _ in range(steps):
+            flush.zero_()  # 256 MB write between steps (L2 flush)
+            torch.cuda.synchronize()
+            stats.append(dm.solve(opts).as_dict())
+    torch.cuda.synchronize()
+    barrier(ws)
+    return stats, clk.summary()
+
+
+def roofline(stats, peak, bound, kernel):
+    s0 = stats[-1]
+    pair_ms = statistics.mean(s["ms_pairs"] for s in stats)
+    flops = FLOP_POINT_PAIR * s0["n_point_pairs"] + FLOP_SLAB * s0["node_visits"] + FLOP_TRI * s0["prim_tests"]
+    achieved = flops / (pair_ms / 1e3) / 1e12
+    return {"bound": bound, "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+            "traffic": None, "peak_source": "measured by rvf_fma_peak (FMA microbenchmark) in this run",
+            "kernel": kernel, "kernel_ms": pair_ms, "algorithmic_flop_per_launch": flops}
+
+
 def run_ours(args):
     ws, rank, local = dist_setup()
     rvf = load_pkg()
@@ -203,37 +234,43 @@ def run_ours(args):
     pairs = N * (N - 1) // 2
     sess = _abi.Session(local)
     arrays = rvf.mesh_desc_arrays(md, OBSTRUCTION)
-    opts = rvf.make_options(NQUAD, precision=args.precision, seed=1)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")
-
-    # ---- value: mesh resident in HBM ----
-    dm = _abi.DeviceMesh(sess, arrays)
-    for _ in range(args.warmup):
-        dm.solve(opts)
-    barrier(ws)
-    torch.cuda.synchronize()
-    stats = []
-    with Clocks(local) as clk:
-        for _ in range(args.steps):
-            flush.zero_()
-            torch.cuda.synchronize()
-            stats.append(dm.solve(opts).as_dict())
-    torch.cuda.synchronize()
-    barrier(ws)
-    total_ms = sum(s["ms_total"] for s in stats)
-    total_ms = allreduce_max(total_ms, ws)
-    value = ws * pairs * args.steps / (total_ms / 1e3)
-    s0 = stats[-1]
-    pair_ms = statistics.mean(s["ms_pairs"] for s in stats)
-    flops = FLOP_POINT_PAIR * s0["n_point_pairs"] + FLOP_SLAB * s0["node_visits"] + FLOP_TRI * s0["prim_tests"]
+    precisions = ["fp64", "mixed"] if args.precision == "both" else [args.precision]
+    head = precisions[-1]
+    runs, meshes = {}, {}
+    for prec in precisions:
+        opts = rvf.make_options(NQUAD, precision=prec, seed=1)
+        dm = _abi.DeviceMesh(sess, arrays)
+        stats, clocks = timed_solves(dm, opts, args.steps, args.warmup, flush, ws, local)
+        total_ms = allreduce_max(sum(s["ms_total"] for s in stats), ws)
+        runs[prec] = {"stats": stats, "clocks": clocks, "ms": total_ms / args.steps,
+                      "value": ws * pairs * args.steps / (total_ms / 1e3)}
+        meshes[prec] = dm
+    accuracy = None
+    if len(precisions) == 2:
+        d = _abi.max_abs_diff(meshes["fp64"].result_device(), meshes["mixed"].result_device(), N * N)
+        accuracy = {"max_abs_dF_mixed_vs_fp64": d,
+                    "max_row_sum_dev_fp64": runs["fp64"]["stats"][-1]["max_row_sum_dev"],
+                    "max_row_sum_dev_mixed": runs["mixed"]["stats"][-1]["max_row_sum_dev"],
+                    "rays_fp64_retraced_mixed": runs["mixed"]["stats"][-1]["n_rays_fp64"],
+                    "pairs_fp64_mixed": runs["mixed"]["stats"][-1]["n_pairs_fp64"],
+                    "unsure_rays": {k: runs["mixed"]["stats"][-1][k] for k in
+                                    ("unsure_rays", "unsure_slab", "unsure_prim", "unsure_direction")},
+                    "graze_point_pairs": runs["mixed"]["stats"][-1]["graze_point_pairs"]}
+    for dm in meshes.values():
+        dm.release()
     peak64 = _abi.fma_peak(local, True)
-    achieved = flops / (pair_ms / 1e3) / 1e12
-    clocks = clk.summary()
+    peak32 = _abi.fma_peak(local, False)
+    H = runs[head]
+    if head == "mixed":
+        roof = roofline(H["stats"], peak32, "fp32_fma", "k_pairs_mixed<OCC>")
+    else:
+        roof = roofline(H["stats"], peak64, "fp64_fma", "k_pairs_fp64<DIM3,OCC>")
 
     # ---- e2e: through the C ABI with host buffers ----
     e2e = None
     if not args.no_e2e:
-        dm.release()
+        opts = rvf.make_options(NQUAD, precision=head, seed=1)
         h2d = sum(a.nbytes for k, a in arrays.items() if hasattr(a, "nbytes")) + sum(t.nbytes for t in arrays["nodes"])
         d2h = 8 * (N * N + N + G * G + G)
         try:
@@ -257,29 +294,31 @@ def run_ours(args):
         t = allreduce_max(sum(times), ws)
         e2e = {"value": ws * pairs * len(times) / t, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                "d2h_bytes_per_step": int(d2h), "host_buffer": "pinned" if pinned else "pageable",
-               "steps": len(times), "s_per_step": t / len(times)}
+               "steps": len(times), "s_per_step": t / len(times), "precision": head}
         if pinned:
             Fh.free()
-    else:
-        dm.release()
 
-    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32+f64",
+    s0 = H["stats"][-1]
+    line = {"metric": METRIC, "value": H["value"], "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": H["ms"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64" if head == "fp64" else "f32+f64",
             "data": "synthetic",
             "config": {"workload": desc, "n_elems": N, "pairs_per_step": pairs, "nquad": NQUAD,
-                       "precision": args.precision, "parallelism": f"replicas x{ws} (independent meshes)",
-                       "l2": "each step writes a 14.9 GB F matrix (>> 126 MB L2); a 256 MB buffer is also "
-                             "written between steps"},
+                       "precision": head, "parallelism": f"replicas x{ws} (independent meshes)",
+                       "l2": "each step writes the dense F matrix (C2: 14.9 GB >> 126 MB L2); a 256 MB "
+                             "buffer is also written between steps"},
             "e2e": e2e,
-            "gpu_launches": int(sum(s["gpu_kernels"] for s in stats)),
-            "roofline": {"bound": "fp64_fma", "achieved": achieved, "peak": peak64, "unit": "TFLOP/s",
-                         "frac": achieved / peak64, "traffic": None,
-                         "peak_source": "measured by rvf_fma_peak (FP64 FMA microbenchmark) in this run",
-                         "kernel": "k_pairs_fp64<DIM3,OCC>", "kernel_ms": pair_ms,
-                         "algorithmic_flop_per_launch": flops},
-            "clocks": clocks,
-            "counts": {k: s0[k] for k in ("n_point_pairs", "n_rays", "node_visits", "prim_tests")}}
+            "gpu_launches": int(sum(s["gpu_kernels"] for s in H["stats"])),
+            "roofline": roof,
+            "clocks": H["clocks"],
+            "counts": {k: s0[k] for k in ("n_point_pairs", "n_rays", "n_rays_fp64", "n_pairs_fp64", "node_visits",
+                                          "prim_tests")}}
+    if len(precisions) == 2:
+        line["fp64"] = {"value": runs["fp64"]["value"], "ms_per_step": runs["fp64"]["ms"],
+                        "roofline": roofline(runs["fp64"]["stats"], peak64, "fp64_fma", "k_pairs_fp64<DIM3,OCC>"),
+                        "clocks": runs["fp64"]["clocks"]}
+        line["mixed_over_fp64"] = runs["mixed"]["value"] / runs["fp64"]["value"]
+        line["accuracy"] = accuracy
     if rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(rvf, md, args.ref_seconds)
     if rank == 0:
@@ -297,8 +336,8 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
-    ap.add_argument("--size", choices=["full", "small"], default="full")
+    ap.add_argument("--precision", choices=["fp64", "mixed", "both"], default="both")
+    ap.add_argument("--size", choices=["full", "medium", "small"], default="full")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--e2e-warmup", type=int, default=1)

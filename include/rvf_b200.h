@@ -167,6 +167,10 @@ int rvf_quadrature_rule(int32_t family, int32_t nquad, double* pts, double* wts,
  * the denominator of the pair kernels' roofline (they are FMA-pipe bound). */
 int rvf_fma_peak(int32_t device, int32_t fp64, double* tflops);
 
+/* max |a - b| over n device doubles (for example two results of
+ * rvf_result_device: the mixed-precision F against the FP64 F). */
+int rvf_max_abs_diff(const double* a_dev, const double* b_dev, int64_t n, double* out);
+
 /* Plain FP64 assembly that allocates no memory (no counterpart in the
  * reference).  For callers that cannot call cudaMalloc -- code under an
  * allocator that owns all device memory, memory-capped services, hosts that

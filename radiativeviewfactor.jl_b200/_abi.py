@@ -60,6 +60,11 @@ class Stats(C.Structure):
         d["node_visits"] = int(self.reserved[0])
         d["prim_tests"] = int(self.reserved[1])
         d["gpu_kernels"] = int(self.reserved[2])
+        d["graze_point_pairs"] = int(self.reserved[3])
+        d["unsure_rays"] = int(self.reserved[4])
+        d["unsure_slab"] = int(self.reserved[5])
+        d["unsure_prim"] = int(self.reserved[6])
+        d["unsure_direction"] = int(self.reserved[7])
         return d
 
 
@@ -83,6 +88,7 @@ SIGNATURES = {
     "rvf_quadrature_rule": (C.c_int, [C.c_int32, C.c_int32, _pd, _pd, _pi32]),
     "rvf_bvh_build_host": (C.c_int, [_pd, C.c_int32, C.c_int64, _pd, _pd, _pi32, _pi32, C.POINTER(C.c_int64)]),
     "rvf_fma_peak": (C.c_int, [C.c_int32, C.c_int32, _pd]),
+    "rvf_max_abs_diff": (C.c_int, [_pd, _pd, C.c_int64, _pd]),
     "rvf_solve_fp64_noalloc": (C.c_int, [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64,
                                          C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p]),
 }
@@ -218,6 +224,12 @@ class DeviceMesh:
                                  ptr(row_sums, C.c_double), C.byref(st)), self.lib)
         return st
 
+    def result_device(self):
+        """Device address of the last solve's F (column-major N x N)."""
+        F = _pd()
+        check(self.lib.rvf_result_device(self.handle, C.byref(F), None), self.lib)
+        return F
+
     def result_copy(self, F_elem=None, A_elem=None):
         check(self.lib.rvf_result_copy(self.session.handle, self.handle, ptr(F_elem, C.c_double),
                                        ptr(A_elem, C.c_double)), self.lib)
@@ -245,6 +257,14 @@ def fma_peak(device: int = 0, fp64: bool = True) -> float:
     t = C.c_double()
     check(lib.rvf_fma_peak(device, int(fp64), C.byref(t)), lib)
     return t.value
+
+
+def max_abs_diff(a_dev, b_dev, n: int) -> float:
+    """max |a - b| over n doubles at two device addresses."""
+    lib = load_library()
+    out = C.c_double()
+    check(lib.rvf_max_abs_diff(a_dev, b_dev, n, C.byref(out)), lib)
+    return out.value
 
 
 def quadrature_rule(family: int, nquad: int):

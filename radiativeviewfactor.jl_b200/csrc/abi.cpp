@@ -141,13 +141,75 @@ int mesh_upload(Session* s, const rvf_mesh_desc* d, rvf_mesh** out) {
     m->h_members.insert(m->h_members.end(), mem[g].begin(), mem[g].end());
   }
 
+  // Internal element order: Morton (Z-order) curve of the element centroids,
+  // so that 32 consecutive elements form a compact patch and the shadow rays
+  // of one warp leave or reach neighbouring points.  Results stay in the
+  // caller's order (orig[internal] = original index).
+  m->h_orig.resize(N);
+  {
+    std::vector<double> cx(N), cy(N), cz(N);
+    double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+    for (int64_t e = 0; e < N; ++e) {
+      const int k = kFamNodes[m->h_fam[e]] == 8 ? 4 : kFamNodes[m->h_fam[e]] == 6 ? 3 : kFamNodes[m->h_fam[e]];
+      double c[3] = {0.0, 0.0, 0.0};
+      for (int a = 0; a < k; ++a)
+        for (int q = 0; q < 3; ++q) c[q] += d->coords[3 * (int64_t)m->h_enodes[(size_t)e * 8 + a] + q];
+      cx[e] = c[0] / k; cy[e] = c[1] / k; cz[e] = c[2] / k;
+      const double cc[3] = {cx[e], cy[e], cz[e]};
+      for (int q = 0; q < 3; ++q) { lo[q] = std::min(lo[q], cc[q]); hi[q] = std::max(hi[q], cc[q]); }
+    }
+    auto spread = [](uint64_t v) {  // 21 bits -> every third bit
+      v &= 0x1fffff;
+      v = (v | v << 32) & 0x1f00000000ffffULL;
+      v = (v | v << 16) & 0x1f0000ff0000ffULL;
+      v = (v | v << 8) & 0x100f00f00f00f00fULL;
+      v = (v | v << 4) & 0x10c30c30c30c30c3ULL;
+      v = (v | v << 2) & 0x1249249249249249ULL;
+      return v;
+    };
+    std::vector<std::pair<uint64_t, int32_t>> key(N);
+    for (int64_t e = 0; e < N; ++e) {
+      const double cc[3] = {cx[e], cy[e], cz[e]};
+      uint64_t q3[3];
+      for (int q = 0; q < 3; ++q) {
+        const double span = hi[q] - lo[q];
+        const double f = span > 0.0 ? (cc[q] - lo[q]) / span : 0.0;
+        q3[q] = (uint64_t)std::min(2097151.0, std::max(0.0, f * 2097151.0));
+      }
+      key[e] = {spread(q3[0]) | (spread(q3[1]) << 1) | (spread(q3[2]) << 2), (int32_t)e};
+    }
+    std::stable_sort(key.begin(), key.end(),
+                     [](const std::pair<uint64_t, int32_t>& a, const std::pair<uint64_t, int32_t>& b) {
+                       return a.first < b.first;
+                     });
+    for (int64_t e = 0; e < N; ++e) m->h_orig[e] = key[e].second;
+  }
+  std::vector<int32_t> p_enodes((size_t)N * 8), p_group(N);
+  std::vector<int8_t> p_fam(N);
+  for (int64_t e = 0; e < N; ++e) {
+    const int32_t o = m->h_orig[e];
+    for (int a = 0; a < 8; ++a) p_enodes[(size_t)e * 8 + a] = m->h_enodes[(size_t)o * 8 + a];
+    p_fam[e] = m->h_fam[o];
+    p_group[e] = m->h_group[o];
+  }
+
   int rc;
   if ((rc = upload(s, m->coords, d->coords, sizeof(double) * 3 * d->n_nodes))) return rc;
-  if ((rc = upload(s, m->enodes, m->h_enodes.data(), sizeof(int32_t) * 8 * N))) return rc;
-  if ((rc = upload(s, m->fam, m->h_fam.data(), N))) return rc;
-  if ((rc = upload(s, m->group, m->h_group.data(), sizeof(int32_t) * N))) return rc;
+  if ((rc = upload(s, m->enodes, p_enodes.data(), sizeof(int32_t) * 8 * N))) return rc;
+  if ((rc = upload(s, m->fam, p_fam.data(), N))) return rc;
+  if ((rc = upload(s, m->group, p_group.data(), sizeof(int32_t) * N))) return rc;
+  if ((rc = upload(s, m->orig, m->h_orig.data(), sizeof(int32_t) * N))) return rc;
   if ((rc = upload(s, m->member_off, m->h_member_off.data(), sizeof(int64_t) * (m->G + 1)))) return rc;
   if ((rc = upload(s, m->members, m->h_members.data(), sizeof(int32_t) * m->h_members.size()))) return rc;
+
+  {
+    double mx = 0.0;
+    for (int64_t k = 0; k < 3 * d->n_nodes; ++k) {
+      if (!std::isfinite(d->coords[k])) return set_err(RVF_EINVAL, "node %lld has a non-finite coordinate", (long long)(k / 3 + 1));
+      mx = std::max(mx, std::fabs(d->coords[k]));
+    }
+    m->extent = 1.0 + mx;
+  }
 
   // obstruction BVH (exact tree of src/BVH.jl over the merged soup)
   if (d->n_obs > 0) {
@@ -175,6 +237,19 @@ int mesh_upload(Session* s, const rvf_mesh_desc* d, rvf_mesh** out) {
     m->n_nodes = M;
     m->h_nodes = nodes;
     if ((rc = upload(s, m->nodes, nodes.data(), sizeof(NodeD) * M))) return rc;
+    // FP32 copy for the certified FP32 traversal (rounding is inside its error allowance)
+    std::vector<NodeF> nodesf(M);
+    for (int k = 0; k < M; ++k) {
+      for (int c = 0; c < 3; ++c) {
+        nodesf[k].lo[c] = (float)nodes[k].lo[c];
+        nodesf[k].hi[c] = (float)nodes[k].hi[c];
+      }
+      if (nodes[k].b > 15 || nodes[k].a >= (1 << 26)) return set_err(RVF_EINVAL, "internal: leaf does not fit NodeF");
+      nodesf[k].ab = (nodes[k].a << 4) | nodes[k].b;
+      nodesf[k].miss = nodes[k].miss;
+    }
+    if ((rc = upload(s, m->nodesf, nodesf.data(), sizeof(NodeF) * M))) return rc;
+    for (double v : m->h_soup) m->extent = std::max(m->extent, 1.0 + std::fabs(v));
     const int64_t T = d->n_obs;
     if (nv == 3) {
       std::vector<TriD> tref(T), tgeo(T);
@@ -201,6 +276,26 @@ int mesh_upload(Session* s, const rvf_mesh_desc* d, rvf_mesh** out) {
       }
       if ((rc = upload(s, m->tris_ref, tref.data(), sizeof(TriD) * T))) return rc;
       if ((rc = upload(s, m->tris_geo, tgeo.data(), sizeof(TriD) * T))) return rc;
+      for (int pass = 0; pass < 2; ++pass) {
+        const std::vector<TriD>& src = pass == 0 ? tref : tgeo;
+        std::vector<TriF> tf(T);
+        for (int64_t k = 0; k < T; ++k) {
+          double n1 = 0.0, n2 = 0.0;
+          for (int c = 0; c < 3; ++c) {
+            tf[k].v0[c] = (float)src[k].v0[c];
+            tf[k].e1[c] = (float)src[k].e1[c];
+            tf[k].e2[c] = (float)src[k].e2[c];
+            n1 += src[k].e1[c] * src[k].e1[c];
+            n2 += src[k].e2[c] * src[k].e2[c];
+          }
+          // |e1|, |e2| rounded up, kept as float bits for the error bounds
+          float f1 = std::nextafter((float)std::sqrt(n1), INFINITY), f2 = std::nextafter((float)std::sqrt(n2), INFINITY);
+          std::memcpy(&tf[k].pad0, &f1, 4);
+          std::memcpy(&tf[k].pad1, &f2, 4);
+          tf[k].group = src[k].group;
+        }
+        if ((rc = upload(s, pass == 0 ? m->trisf_ref : m->trisf_geo, tf.data(), sizeof(TriF) * T))) return rc;
+      }
     } else {
       std::vector<SegD> segs(T);
       for (int64_t k = 0; k < T; ++k) {
@@ -247,6 +342,7 @@ int ensure_tables(Session* s, rvf_mesh* m, int nquad, Tables** out) {
   if ((rc = upload(s, T->rules, rules.data(), sizeof(double) * rules.size()))) return rc;
   if ((rc = T->tab.alloc(s, sizeof(double) * nT * kComp * pmax * kTile))) return rc;
   if ((rc = T->area.alloc(s, sizeof(double) * std::max<int64_t>(N, 1)))) return rc;
+  if ((rc = T->area_orig.alloc(s, sizeof(double) * std::max<int64_t>(N, 1)))) return rc;
   if ((rc = T->np.alloc(s, std::max<int64_t>(N, 1)))) return rc;
   if ((rc = T->flat.alloc(s, std::max<int64_t>(N, 1)))) return rc;
   if ((rc = T->nrm.alloc(s, sizeof(double) * 3 * std::max<int64_t>(N, 1)))) return rc;
@@ -267,6 +363,8 @@ int ensure_tables(Session* s, rvf_mesh* m, int nquad, Tables** out) {
   a.nquadpts = q.size(); a.ntripts = t.size(); a.nline = l.size();
   a.tab = (double*)T->tab.ptr;
   a.area = (double*)T->area.ptr;
+  a.orig = m->orig.as<int32_t>();
+  a.area_orig = T->area_orig.as<double>();
   a.np = (int8_t*)T->np.ptr;
   a.flat = (uint8_t*)T->flat.ptr;
   a.nrm = (double*)T->nrm.ptr;
@@ -281,7 +379,10 @@ int ensure_tables(Session* s, rvf_mesh* m, int nquad, Tables** out) {
   if (e != cudaSuccess) return cuda_err(e, "prep kernel");
   if (herr & kErrBadInput)
     return set_err(RVF_EINVAL, "mesh holds a degenerate element (zero or non-finite area element at a quadrature point)");
-  if (N == 1) cudaMemsetAsync(T->area.ptr, 0, sizeof(double), s->stream);  // no pair writes area_out
+  if (N == 1) {  // no pair writes area_out
+    cudaMemsetAsync(T->area.ptr, 0, sizeof(double), s->stream);
+    cudaMemsetAsync(T->area_orig.ptr, 0, sizeof(double), s->stream);
+  }
   *out = T.get();
   m->tables[nquad] = std::move(T);
   return RVF_OK;

@@ -259,6 +259,7 @@ __device__ __forceinline__ bool seg_blocks(const SegD& s, const double* xi, cons
 // ---------------------------------------------------------------------------
 struct TravCount {
   uint64_t nodes = 0, prims = 0;
+  uint64_t unsure_slab = 0, unsure_prim = 0;  // FP32 traversal: decisions left to FP64
 };
 
 template <typename NodeT, typename SlabF, typename LeafF>
@@ -277,7 +278,7 @@ __device__ __forceinline__ bool packet_any_hit(bool alive, const NodeT* __restri
       node = __reduce_min_sync(kFull, w);
       continue;
     }
-    cnt.nodes += __popc(am);
+    cnt.nodes += act ? 1 : 0;
     bool sh = act && slab(nd);
     unsigned hm = __ballot_sync(kFull, sh);
     if (nd.b > 0) {

@@ -18,9 +18,11 @@ struct PrepArgs {
   // rules (device pointers)
   const double *qx, *qe, *qw, *tx, *te, *tw, *lx, *lw;
   int nquadpts, ntripts, nline;
+  const int32_t* orig;  // internal -> caller's element index (null: identity)
   // outputs
   double* tab;     // tiles x kComp x pmax x 32
   double* area;
+  double* area_orig;    // areas in the caller's order (or null)
   int8_t* np;
   uint8_t* flat;
   double* nrm;     // 3N
@@ -41,7 +43,8 @@ struct PairArgs {
   const uint8_t* flat;
   const double* nrm;
   const int32_t* group;
-  double* F;        // N x N column-major
+  const int32_t* orig;  // internal -> caller's element index (null: identity)
+  double* F;        // N x N column-major, caller's element order
   // occlusion (n_nodes == 0: none)
   const NodeD* nodes;
   int n_nodes;
@@ -70,7 +73,48 @@ struct RedArgs {
   double* Agroup;             // G
 };
 
+struct PrepF32Args {
+  int64_t N;
+  int pmax;
+  const double* tab;
+  float* tabf;
+  const int8_t* np;
+  const double* cen;
+};
+
+struct MixedArgs {
+  int64_t N, nT, n_tiles;
+  int pmax;
+  const double* tab;   // FP64 table (near field, grazing, re-tests)
+  const float* tabf;   // FP32 table (offsets from the element centroid)
+  const int8_t* np;
+  const double* area;
+  const uint8_t* flat;
+  const double* nrm;
+  const double* cen;
+  const double* diam;
+  double near_factor;
+  const int32_t* group;
+  const int32_t* orig;
+  double* F;
+  const NodeD* nodes;
+  const NodeF* nodesf;
+  int n_nodes;
+  bool nodesf_in_smem;
+  const TriD* tris;
+  const TriF* trisf;
+  float delta;  // absolute FP32 position error allowance (2^-20 x scene extent)
+  unsigned long long* tile_counter;
+  unsigned long long* counters;  // [-, rays, node tests, prim tests, FP64 rays, near pairs, grazing pp, unsure rays]
+  int* err;
+  uint8_t* ray_log;
+  int log_pm;
+};
+
 cudaError_t launch_prep(const PrepArgs& a, cudaStream_t st);
+cudaError_t launch_prep_f32(const PrepF32Args& a, cudaStream_t st);
+size_t mixed_smem_bytes(int pmax, int n_nodes_smem);
+cudaError_t launch_pairs_mixed(const MixedArgs& a, int sm_count, cudaStream_t st);
 size_t pair_smem_bytes(int pmax, int n_nodes_smem);
 cudaError_t launch_pairs_fp64(const PairArgs& a, int sm_count, cudaStream_t st);
 cudaError_t launch_reduce(const RedArgs& a, cudaStream_t st);

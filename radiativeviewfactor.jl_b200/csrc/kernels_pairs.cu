@@ -57,6 +57,7 @@ __global__ void k_prep(PrepArgs a) {
     if (!(dA > 0.0) || !(dA < 1e300)) atomicOr(a.err, kErrBadInput);
   }
   a.area[e] = A;
+  if (a.area_orig) a.area_orig[a.orig ? a.orig[e] : e] = A;
   a.np[e] = (int8_t)np;
   a.flat[e] = flat ? 1 : 0;
   a.nrm[3 * e + 0] = n0[0];
@@ -97,8 +98,7 @@ template <bool DIM3, bool OCC>
 __global__ void __launch_bounds__(256) k_pairs_fp64(PairArgs a) {
   extern __shared__ __align__(128) unsigned char smem[];
   double* iblk = reinterpret_cast<double*>(smem);
-  double* rawT = iblk + kComp * a.pmax * kTile;  // [32][33]
-  NodeD* snodes = reinterpret_cast<NodeD*>(rawT + kTile * (kTile + 1));
+  NodeD* snodes = reinterpret_cast<NodeD*>(iblk + kComp * a.pmax * kTile);
   uint64_t* bar = reinterpret_cast<uint64_t*>(snodes + (a.nodes_in_smem ? a.n_nodes : 0));
   __shared__ int64_t s_tile;
 
@@ -140,6 +140,8 @@ __global__ void __launch_bounds__(256) k_pairs_fp64(PairArgs a) {
     phase ^= 1u;
 
     const int64_t j = bj * kTile + lane;
+    const int64_t N = a.N;
+    const int64_t oj = (j < N) ? (a.orig ? (int64_t)a.orig[j] : j) : 0;
     const double* jb = a.tab + bj * kComp * a.pmax * kTile + lane;
     for (int rr = 0; rr < kTile / 8; ++rr) {
       const int li = warp + 8 * rr;
@@ -147,6 +149,9 @@ __global__ void __launch_bounds__(256) k_pairs_fp64(PairArgs a) {
       double acc = 0.0;
       if (i < a.N) {  // warp-uniform
         const bool valid = (j < a.N) && (i < j);
+        const int64_t oi = a.orig ? (int64_t)a.orig[i] : i;
+        // the reference casts from the element with the lower (caller's) index
+        const bool sw = valid && oi > oj;
         const int npi = a.np[i];
         int npj = valid ? a.np[j] : 0;
         // Two elements whose points all share one normal, bit for bit, have
@@ -158,7 +163,9 @@ __global__ void __launch_bounds__(256) k_pairs_fp64(PairArgs a) {
         const int32_t gi = a.group[i];
         const int32_t gj = valid ? a.group[j] : gi;
         const double* ib = iblk + li;
-        uint8_t* logp = (a.ray_log && valid) ? a.ray_log + ((uint64_t)i * a.N + j) * a.log_pm * a.log_pm : nullptr;
+        uint8_t* logp = (a.ray_log && valid)
+                            ? a.ray_log + ((uint64_t)(sw ? oj : oi) * a.N + (sw ? oi : oj)) * a.log_pm * a.log_pm
+                            : nullptr;
         for (int q = 0; q < qmax; ++q) {
           const bool lq = q < npj;
           double xj[3], nj[3], wj;
@@ -193,7 +200,7 @@ __global__ void __launch_bounds__(256) k_pairs_fp64(PairArgs a) {
               uint8_t lg = 0;
               if (DIM3) {
                 RayD R;
-                bool cast = (K > 0.0) && make_ray(xi, rx, ry, rz, r2, R);
+                bool cast = (K > 0.0) && (sw ? make_ray(xj, -rx, -ry, -rz, r2, R) : make_ray(xi, rx, ry, rz, r2, R));
                 n_rays += cast ? 1 : 0;
                 bool blocked = packet_any_hit(
                     cast, nodes, a.n_nodes, [&](const NodeD& nd) { return slab_d(nd, R); },
@@ -220,40 +227,25 @@ __global__ void __launch_bounds__(256) k_pairs_fp64(PairArgs a) {
                       const SegD sg = a.segs[k];
                       if (!test || sg.group == gi || sg.group == gj) return false;
                       ++tc.prims;
-                      return seg_blocks(sg, xi, xj);
+                      return sw ? seg_blocks(sg, xj, xi) : seg_blocks(sg, xi, xj);
                     },
                     tc);
                 if (cast) lg = blocked ? 2 : 1;
                 if (blocked) K = 0.0;
               }
-              if (logp && lq) logp[p * a.log_pm + q] = lg;
+              if (logp && lq) logp[sw ? q * a.log_pm + p : p * a.log_pm + q] = lg;
             }
             inner = fma(wi, K, inner);
           }
           acc = fma(wj, inner, acc);
         }
-      }
-      rawT[li * (kTile + 1) + lane] = acc;
-    }
-    __syncthreads();
-    // epilogue: F[i,j] = raw/A_i (column j contiguous in i), F[j,i] = raw/A_j
-    const int64_t N = a.N;
-    if (bi == bj) {
-      for (int c = warp; c < kTile; c += 8) {
-        const int64_t jj = bj * kTile + c, ii = bi * kTile + lane;
-        if (ii < N && jj < N) {
-          double r = (lane < c) ? rawT[lane * (kTile + 1) + c] : (lane > c) ? rawT[c * (kTile + 1) + lane] : 0.0;
-          a.F[ii + jj * N] = r / a.area[ii];
+        // F[i,j] = raw/A_i and F[j,i] = raw/A_j in the caller's element order
+        if (valid) {
+          a.F[oi + oj * N] = acc / a.area[i];
+          a.F[oj + oi * N] = acc / a.area[j];
+        } else if (j == i) {
+          a.F[oi + oi * N] = 0.0 / a.area[i];
         }
-      }
-    } else {
-      for (int c = warp; c < kTile; c += 8) {
-        const int64_t jj = bj * kTile + c, ii = bi * kTile + lane;
-        if (ii < N && jj < N) a.F[ii + jj * N] = rawT[lane * (kTile + 1) + c] / a.area[ii];
-      }
-      for (int c = warp; c < kTile; c += 8) {
-        const int64_t ii = bi * kTile + c, jj = bj * kTile + lane;
-        if (ii < N && jj < N) a.F[jj + ii * N] = rawT[c * (kTile + 1) + lane] / a.area[jj];
       }
     }
     __syncthreads();
@@ -353,8 +345,7 @@ cudaError_t launch_prep(const PrepArgs& a, cudaStream_t st) {
 }
 
 size_t pair_smem_bytes(int pmax, int n_nodes_smem) {
-  return (size_t)kComp * pmax * kTile * sizeof(double) + (size_t)kTile * (kTile + 1) * sizeof(double) +
-         (size_t)n_nodes_smem * sizeof(NodeD) + 16;
+  return (size_t)kComp * pmax * kTile * sizeof(double) + (size_t)n_nodes_smem * sizeof(NodeD) + 16;
 }
 
 template <bool D3, bool O>

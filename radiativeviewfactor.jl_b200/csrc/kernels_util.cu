@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <cstring>
 
 #include "../../include/rvf_b200.h"
 #include "rvf_internal.h"
@@ -26,9 +27,42 @@ __global__ void __launch_bounds__(256) k_fma_peak(T* out, int iters, T b, T c) {
   if (s == (T)-1.2345) out[blockIdx.x * blockDim.x + threadIdx.x] = s;
 }
 
+// max |a - b| over n doubles (NaN in exactly one of them counts as +inf);
+// non-negative doubles order like their bit patterns, so atomicMax on the
+// bits is a max on the values.
+__global__ void k_max_abs_diff(const double* __restrict__ a, const double* __restrict__ b, int64_t n,
+                               unsigned long long* out) {
+  double m = 0.0;
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+    const double x = a[k], y = b[k];
+    const bool nx = x != x, ny = y != y;
+    double d = (nx && ny) ? 0.0 : (nx || ny) ? INFINITY : fabs(x - y);
+    m = fmax(m, d);
+  }
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(out, (unsigned long long)__double_as_longlong(m));
+}
+
 }  // namespace rvf
 
 using namespace rvf;
+
+extern "C" int rvf_max_abs_diff(const double* a, const double* b, int64_t n, double* out) {
+  if (!out || n < 0 || (n > 0 && (!a || !b))) return set_err(RVF_EINVAL, "bad argument");
+  unsigned long long* d = nullptr;
+  cudaError_t e = cudaMalloc(&d, sizeof(unsigned long long));
+  if (e != cudaSuccess) return cuda_err(e, "cudaMalloc");
+  cudaMemset(d, 0, sizeof(unsigned long long));
+  if (n > 0) k_max_abs_diff<<<1184, 256>>>(a, b, n, d);
+  unsigned long long h = 0;
+  e = cudaMemcpy(&h, d, sizeof h, cudaMemcpyDeviceToHost);
+  cudaFree(d);
+  if (e != cudaSuccess) return cuda_err(e, "max_abs_diff");
+  double v;
+  std::memcpy(&v, &h, sizeof v);
+  *out = v;
+  return RVF_OK;
+}
 
 extern "C" int rvf_fma_peak(int32_t device, int32_t fp64, double* tflops) {
   if (!tflops) return set_err(RVF_EINVAL, "null out");

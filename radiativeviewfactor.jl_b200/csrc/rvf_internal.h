@@ -44,7 +44,9 @@ int upload(Session* s, DevBuf& b, const void* src, size_t n);
 
 struct Tables {
   int nquad = 0, pmax = 0;
-  DevBuf rules, tab, area, np, flat, nrm, cen, diam;
+  DevBuf rules, tab, area, np, flat, nrm, cen, diam;  // internal element order
+  DevBuf area_orig;                                   // areas in the caller's element order
+  DevBuf tabf;  // FP32 table, built on the first mixed-precision solve
 };
 
 }  // namespace rvf
@@ -68,7 +70,8 @@ struct rvf_mesh {
   int dim = 2;
   int64_t N = 0, Nn = 0;
   // host copies
-  std::vector<int32_t> h_enodes;  // N x 8, 0-based
+  std::vector<int32_t> h_enodes;  // N x 8, 0-based, caller's element order
+  std::vector<int32_t> h_orig;    // internal (Morton) position -> caller's element index
   std::vector<int8_t> h_fam;
   std::vector<int32_t> h_group;
   std::vector<int32_t> h_tags;
@@ -79,8 +82,11 @@ struct rvf_mesh {
   std::vector<rvf::NodeD> h_nodes;
   int G = 0;
   // device
-  rvf::DevBuf coords, enodes, fam, group, member_off, members;
+  rvf::DevBuf coords, enodes, fam, group, member_off, members;  // per-element arrays in internal order
+  rvf::DevBuf orig;                                             // int32 internal -> caller's index
   rvf::DevBuf nodes, tris_ref, tris_geo, segs;
+  rvf::DevBuf nodesf, trisf_ref, trisf_geo;  // FP32 copies (mixed precision)
+  double extent = 1.0;                        // 1 + max |coordinate| of the mesh and the soup
   int n_nodes = 0;
   int64_t n_obs = 0;
   std::map<int, std::unique_ptr<rvf::Tables>> tables;

@@ -81,7 +81,7 @@ int run_reduce(Session* s, rvf_mesh* m, Tables* T) {
   r.G = m->G;
   r.n_chunks = n_chunks;
   r.F = m->F.as<double>();
-  r.area = T->area.as<double>();
+  r.area = T->area_orig.as<double>();  // reductions work in the caller's element order
   r.member_off = m->member_off.as<int64_t>();
   r.members = m->members.as<int32_t>();
   r.part = m->part.as<double>();
@@ -216,7 +216,9 @@ int rvf_solve(rvf_session* s, rvf_mesh* m, const rvf_options* o, double* F_elem,
   if (rc) return rc;
   if (o->method == RVF_METHOD_MONTE_CARLO) return set_err(RVF_EUNSUPPORTED, "Monte Carlo is not available in this build");
   if (o->use_duffy) return set_err(RVF_EUNSUPPORTED, "use_duffy is not available in this build");
-  if (o->precision == RVF_PREC_MIXED) return set_err(RVF_EUNSUPPORTED, "mixed precision is not available in this build");
+  // mixed precision covers surface meshes; curve meshes run the FP64 path
+  const bool mixed = (o->precision == RVF_PREC_MIXED) && (m->dim == 2);
+  if (mixed && !(o->near_field_factor >= 0.0)) return set_err(RVF_EINVAL, "near_field_factor must be >= 0");
   rvf_stats S{};
   int64_t n_kernels = 0;  // kernels of this library launched by this call
   EvTimer total(s->stream);
@@ -233,7 +235,7 @@ int rvf_solve(rvf_session* s, rvf_mesh* m, const rvf_options* o, double* F_elem,
     if ((rc = m->F.alloc(s, sizeof(double) * std::max<int64_t>(N * N, 1)))) return rc;
   m->has_result = false;
   cudaMemsetAsync(s->tile_counter.ptr, 0, 8, s->stream);
-  cudaMemsetAsync(s->counters.ptr, 0, 64, s->stream);
+  cudaMemsetAsync(s->counters.ptr, 0, 256, s->stream);
   cudaMemsetAsync(s->err.ptr, 0, sizeof(int), s->stream);
   DevBuf log;
   if (o->ray_log) {
@@ -255,6 +257,7 @@ int rvf_solve(rvf_session* s, rvf_mesh* m, const rvf_options* o, double* F_elem,
   a.flat = T->flat.as<uint8_t>();
   a.nrm = T->nrm.as<double>();
   a.group = m->group.as<int32_t>();
+  a.orig = m->orig.as<int32_t>();
   a.F = m->F.as<double>();
   a.nodes = occ ? m->nodes.as<NodeD>() : nullptr;
   a.n_nodes = occ ? m->n_nodes : 0;
@@ -271,8 +274,31 @@ int rvf_solve(rvf_session* s, rvf_mesh* m, const rvf_options* o, double* F_elem,
     if (N == 1) {
       cudaMemsetAsync(m->F.ptr, 0, sizeof(double), s->stream);
     }
+    cudaError_t e = cudaSuccess;
+    MixedArgs x{};
+    if (mixed) {
+      if (!T->tabf.ptr) {
+        if ((rc = T->tabf.alloc(s, sizeof(float) * a.nT * kComp * T->pmax * kTile))) return rc;
+        cudaMemsetAsync(T->tabf.ptr, 0, T->tabf.bytes, s->stream);
+        PrepF32Args pf{N, T->pmax, T->tab.as<double>(), T->tabf.as<float>(), T->np.as<int8_t>(), T->cen.as<double>()};
+        if ((e = launch_prep_f32(pf, s->stream)) != cudaSuccess) return cuda_err(e, "FP32 table kernel launch");
+        n_kernels += 1;
+      }
+      x.N = N; x.nT = a.nT; x.n_tiles = a.n_tiles; x.pmax = a.pmax;
+      x.tab = a.tab; x.tabf = T->tabf.as<float>(); x.np = a.np; x.area = a.area; x.flat = a.flat; x.nrm = a.nrm;
+      x.cen = T->cen.as<double>(); x.diam = T->diam.as<double>(); x.near_factor = o->near_field_factor;
+      x.group = a.group; x.orig = a.orig; x.F = a.F;
+      x.nodes = a.nodes; x.n_nodes = a.n_nodes;
+      x.nodesf = occ ? m->nodesf.as<NodeF>() : nullptr;
+      x.nodesf_in_smem = occ && (mixed_smem_bytes(T->pmax, m->n_nodes) <= std::min<size_t>(s->smem_optin, 96 * 1024));
+      x.tris = a.tris;
+      x.trisf = occ ? (o->geometric_soup ? m->trisf_geo.as<TriF>() : m->trisf_ref.as<TriF>()) : nullptr;
+      x.delta = (float)std::ldexp(m->extent, -20);
+      x.tile_counter = a.tile_counter; x.counters = a.counters; x.err = a.err;
+      x.ray_log = a.ray_log; x.log_pm = a.log_pm;
+    }
     EvTimer t(s->stream);
-    cudaError_t e = launch_pairs_fp64(a, s->sm_count, s->stream);
+    e = mixed ? launch_pairs_mixed(x, s->sm_count, s->stream) : launch_pairs_fp64(a, s->sm_count, s->stream);
     n_kernels += 1;
     if (e != cudaSuccess) return cuda_err(e, "pair kernel launch");
     S.ms_pairs = t.stop();
@@ -294,7 +320,7 @@ int rvf_solve(rvf_session* s, rvf_mesh* m, const rvf_options* o, double* F_elem,
     EvTimer t(s->stream);
     cudaError_t e = cudaSuccess;
     if (F_elem && N > 0) e = cudaMemcpyAsync(F_elem, m->F.ptr, sizeof(double) * N * N, cudaMemcpyDeviceToHost, s->stream);
-    if (e == cudaSuccess && A_elem && N > 0) e = cudaMemcpyAsync(A_elem, T->area.ptr, sizeof(double) * N, cudaMemcpyDeviceToHost, s->stream);
+    if (e == cudaSuccess && A_elem && N > 0) e = cudaMemcpyAsync(A_elem, T->area_orig.ptr, sizeof(double) * N, cudaMemcpyDeviceToHost, s->stream);
     if (e == cudaSuccess && F_group && m->G > 0 && N > 0)
       e = cudaMemcpyAsync(F_group, m->Fgroup.ptr, sizeof(double) * m->G * m->G, cudaMemcpyDeviceToHost, s->stream);
     if (e == cudaSuccess && A_group && m->G > 0 && N > 0)
@@ -308,15 +334,21 @@ int rvf_solve(rvf_session* s, rvf_mesh* m, const rvf_options* o, double* F_elem,
     S.ms_download = t.stop();
   }
   if (st) {
-    unsigned long long c[8] = {};
+    unsigned long long c[16] = {};
     cudaMemcpy(c, s->counters.ptr, sizeof c, cudaMemcpyDeviceToHost);
     S.n_pairs = N * (N - 1) / 2;
     S.n_point_pairs = (int64_t)c[0];
     S.n_rays = (int64_t)c[1];
-    S.n_rays_fp64 = (int64_t)c[1];
+    S.n_rays_fp64 = mixed ? (int64_t)c[4] : (int64_t)c[1];
+    S.n_pairs_fp64 = mixed ? (int64_t)c[5] : S.n_pairs;
     S.reserved[0] = (int64_t)c[2];
     S.reserved[1] = (int64_t)c[3];
     S.reserved[2] = n_kernels;
+    S.reserved[3] = mixed ? (int64_t)c[6] : 0;  // grazing point pairs re-evaluated in FP64
+    S.reserved[4] = mixed ? (int64_t)c[7] : 0;  // FP32 rays with an uncertain decision
+    S.reserved[5] = mixed ? (int64_t)c[8] : 0;  // ... of which at a slab test
+    S.reserved[6] = mixed ? (int64_t)c[9] : 0;  // ... of which at a triangle test
+    S.reserved[7] = mixed ? (int64_t)c[10] : 0; // rays with a direction component below 1e-4
     if (N > 0 && m->G > 0) {
       std::vector<double> rs(N);
       cudaMemcpy(rs.data(), m->rowsum.ptr, sizeof(double) * N, cudaMemcpyDeviceToHost);
@@ -338,7 +370,7 @@ int rvf_result_copy(rvf_session* s, rvf_mesh* m, double* F_elem, double* A_elem)
   Tables* T = m->tables[m->result_nquad].get();
   cudaError_t e = cudaSuccess;
   if (F_elem) e = cudaMemcpyAsync(F_elem, m->F.ptr, sizeof(double) * m->N * m->N, cudaMemcpyDeviceToHost, s->stream);
-  if (e == cudaSuccess && A_elem) e = cudaMemcpyAsync(A_elem, T->area.ptr, sizeof(double) * m->N, cudaMemcpyDeviceToHost, s->stream);
+  if (e == cudaSuccess && A_elem) e = cudaMemcpyAsync(A_elem, T->area_orig.ptr, sizeof(double) * m->N, cudaMemcpyDeviceToHost, s->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
   return e == cudaSuccess ? RVF_OK : cuda_err(e, "rvf_result_copy");
 }
@@ -347,7 +379,7 @@ int rvf_result_device(rvf_mesh* m, const double** F_dev, const double** A_dev) {
   if (!m) return set_err(RVF_EINVAL, "null mesh");
   if (!m->has_result) return set_err(RVF_EINVAL, "no result on this mesh yet");
   if (F_dev) *F_dev = m->F.as<double>();
-  if (A_dev) *A_dev = m->tables[m->result_nquad]->area.as<double>();
+  if (A_dev) *A_dev = m->tables[m->result_nquad]->area_orig.as<double>();
   return RVF_OK;
 }
 
