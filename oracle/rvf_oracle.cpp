@@ -843,8 +843,10 @@ double mc_pair(const orc_mesh* m, const orc_bvh* bvh, int64_t i, int64_t j, int 
   const int64_t N = m->n_elems;
   const bool two_d = (m->mesh_dim == 1);
   int fi = m->family[i], fj = m->family[j];
-  int32_t gi = exclude_groups ? m->elem_group[i] : 0;
-  int32_t gj = exclude_groups ? m->elem_group[j] : 0;
+  // curves always skip their own groups, as the quadrature path's 2-D test does
+  const bool excl = exclude_groups || two_d;
+  int32_t gi = excl ? m->elem_group[i] : 0;
+  int32_t gj = excl ? m->elem_group[j] : 0;
   uint64_t tid = (uint64_t)(i * N + j + 1);  // (i-1)*N + j with 1-based i, j
   uint64_t st = orc_init_rng(seed, tid);
   double Ai = 0.0, Aj = 0.0, Ks = 0.0;

@@ -199,6 +199,11 @@ int mesh_upload(Session* s, const rvf_mesh_desc* d, rvf_mesh** out) {
   if ((rc = upload(s, m->fam, p_fam.data(), N))) return rc;
   if ((rc = upload(s, m->group, p_group.data(), sizeof(int32_t) * N))) return rc;
   if ((rc = upload(s, m->orig, m->h_orig.data(), sizeof(int32_t) * N))) return rc;
+  {
+    std::vector<int32_t> inv(N);
+    for (int64_t e = 0; e < N; ++e) inv[m->h_orig[e]] = (int32_t)e;
+    if ((rc = upload(s, m->inv, inv.data(), sizeof(int32_t) * N))) return rc;
+  }
   if ((rc = upload(s, m->member_off, m->h_member_off.data(), sizeof(int64_t) * (m->G + 1)))) return rc;
   if ((rc = upload(s, m->members, m->h_members.data(), sizeof(int32_t) * m->h_members.size()))) return rc;
 

@@ -111,6 +111,61 @@ struct MixedArgs {
   int log_pm;
 };
 
+// A Quad8 pair sharing corner nodes (src/DuffyKernel.jl:95-115), i < j in the
+// caller's order (the reference integrates with elem_i = the lower index).
+struct DuffyPair {
+  int32_t i, j;      // caller's element indices
+  int32_t ii, jj;    // internal positions (node table rows)
+  int32_t stype;     // 1 = common vertex, 2 = common edge
+  int32_t ci0, cj0;  // first shared corner on each element (1-based)
+  int32_t edge_i, edge_j;  // _corners_to_edge of the first two shared corners
+  int32_t gi, gj;
+  int32_t pad;
+};
+
+struct DuffyArgs {
+  int64_t N;
+  int nq;
+  const double* p01;  // Gauss-Legendre points on [0,1]
+  const double* w01;
+  const DuffyPair* pairs;
+  int64_t n_pairs;
+  const double* coords;
+  const int32_t* enodes;  // internal order, 0-based
+  const double* area_orig;
+  double* F;
+  const NodeD* nodes;
+  int n_nodes;
+  const TriD* tris;
+  unsigned long long* counters;
+};
+
+cudaError_t launch_duffy(const DuffyArgs& a, cudaStream_t st);
+
+struct McArgs {
+  int64_t N, nT, n_tiles;
+  int n_samples;
+  uint64_t seed;
+  bool exclude;  // skip source / destination groups in the traversal
+  bool dim3;
+  const double* coords;
+  const int32_t* enodes;  // internal order, 0-based
+  const int8_t* fam;      // internal order
+  const int32_t* group;   // internal order
+  const int32_t* orig;    // internal -> caller's index
+  const int32_t* inv;     // caller's index -> internal
+  double* area_orig;      // written by the area-rule kernel
+  double* F;
+  const NodeD* nodes;
+  int n_nodes;
+  const TriD* tris;
+  const SegD* segs;
+  unsigned long long* tile_counter;
+  unsigned long long* counters;
+  uint8_t* ray_log;  // [(i*N + j) * n_samples + k] for caller indices i < j
+};
+
+cudaError_t launch_mc(const McArgs& a, int sm_count, cudaStream_t st);
 cudaError_t launch_prep(const PrepArgs& a, cudaStream_t st);
 cudaError_t launch_prep_f32(const PrepF32Args& a, cudaStream_t st);
 size_t mixed_smem_bytes(int pmax, int n_nodes_smem);

@@ -84,15 +84,22 @@ struct rvf_mesh {
   // device
   rvf::DevBuf coords, enodes, fam, group, member_off, members;  // per-element arrays in internal order
   rvf::DevBuf orig;                                             // int32 internal -> caller's index
+  rvf::DevBuf inv;                                              // int32 caller's index -> internal
+  rvf::DevBuf mc_area;                                          // Monte Carlo areas (caller's order)
   rvf::DevBuf nodes, tris_ref, tris_geo, segs;
   rvf::DevBuf nodesf, trisf_ref, trisf_geo;  // FP32 copies (mixed precision)
   double extent = 1.0;                        // 1 + max |coordinate| of the mesh and the soup
   int n_nodes = 0;
   int64_t n_obs = 0;
   std::map<int, std::unique_ptr<rvf::Tables>> tables;
+  // Quad8 pairs sharing corners (built on the first use_duffy solve)
+  bool duffy_built = false;
+  int64_t n_duffy = 0;
+  rvf::DevBuf duffy_pairs;
+  std::map<int, std::unique_ptr<rvf::DevBuf>> duffy_rules;  // nquad -> [p01 | w01]
   // results of the last solve
   rvf::DevBuf F, part, rowgroup, rowsum, Fgroup, Agroup;
-  int result_nquad = -1;
+  const double* result_area = nullptr;  // areas (caller's order) of the last result
   bool has_result = false;
 };
 

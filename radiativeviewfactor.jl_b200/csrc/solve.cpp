@@ -61,7 +61,7 @@ int validate_options(const rvf_mesh* m, const rvf_options* o) {
   return RVF_OK;
 }
 
-int run_reduce(Session* s, rvf_mesh* m, Tables* T) {
+int run_reduce(Session* s, rvf_mesh* m, const double* area) {
   const int64_t N = m->N;
   if (N == 0 || m->G == 0) return RVF_OK;
   int n_chunks = (int)std::min<int64_t>(256, std::max<int64_t>(1, (1 << 20) / std::max<int64_t>(N, 1)));
@@ -81,7 +81,7 @@ int run_reduce(Session* s, rvf_mesh* m, Tables* T) {
   r.G = m->G;
   r.n_chunks = n_chunks;
   r.F = m->F.as<double>();
-  r.area = T->area_orig.as<double>();  // reductions work in the caller's element order
+  r.area = area;  // reductions work in the caller's element order
   r.member_off = m->member_off.as<int64_t>();
   r.members = m->members.as<int32_t>();
   r.part = m->part.as<double>();
@@ -91,6 +91,80 @@ int run_reduce(Session* s, rvf_mesh* m, Tables* T) {
   r.Agroup = m->Agroup.as<double>();
   cudaError_t e = launch_reduce(r, s->stream);
   return e == cudaSuccess ? RVF_OK : cuda_err(e, "reduction kernels");
+}
+
+// Quad8 pairs that share corner nodes, in the reference's classification
+// (singularity_type, src/DuffyKernel.jl:95-115): corners 1-4 compared by node
+// index, ci outer / cj inner, the first two matches kept.
+int ensure_duffy(Session* s, rvf_mesh* m, int nquad, const double** p01, const double** w01) {
+  if (!m->duffy_built) {
+    const int64_t N = m->N;
+    std::vector<int32_t> inv(N);
+    for (int64_t e = 0; e < N; ++e) inv[m->h_orig[e]] = (int32_t)e;
+    std::map<int32_t, std::vector<int32_t>> by_node;
+    for (int64_t e = 0; e < N; ++e)
+      if (m->h_fam[e] == 0)
+        for (int c = 0; c < 4; ++c) by_node[m->h_enodes[(size_t)e * 8 + c]].push_back((int32_t)e);
+    auto corners_to_edge = [](int c1, int c2) {  // src/DuffyKernel.jl:411-419
+      int a = std::min(c1, c2), b = std::max(c1, c2);
+      if (a == 1 && b == 2) return 1;
+      if (a == 2 && b == 3) return 2;
+      if (a == 3 && b == 4) return 3;
+      if (a == 1 && b == 4) return 4;
+      return 1;
+    };
+    std::vector<DuffyPair> pairs;
+    for (int64_t i = 0; i < N; ++i) {
+      if (m->h_fam[i] != 0) continue;
+      std::vector<int32_t> cand;
+      for (int c = 0; c < 4; ++c)
+        for (int32_t j : by_node[m->h_enodes[(size_t)i * 8 + c]])
+          if (j > i) cand.push_back(j);
+      std::sort(cand.begin(), cand.end());
+      cand.erase(std::unique(cand.begin(), cand.end()), cand.end());
+      const int32_t* a = &m->h_enodes[(size_t)i * 8];
+      for (int32_t j : cand) {
+        const int32_t* b = &m->h_enodes[(size_t)j * 8];
+        int n = 0, ci[2] = {0, 0}, cj[2] = {0, 0};
+        for (int x = 0; x < 4; ++x)
+          for (int y = 0; y < 4; ++y)
+            if (a[x] == b[y]) {
+              if (n < 2) { ci[n] = x + 1; cj[n] = y + 1; }
+              ++n;
+            }
+        if (n == 0) continue;
+        DuffyPair P{};
+        P.i = (int32_t)i; P.j = j; P.ii = inv[i]; P.jj = inv[j];
+        P.stype = n == 1 ? 1 : 2;
+        P.ci0 = ci[0]; P.cj0 = cj[0];
+        P.edge_i = n >= 2 ? corners_to_edge(ci[0], ci[1]) : 1;
+        P.edge_j = n >= 2 ? corners_to_edge(cj[0], cj[1]) : 1;
+        P.gi = m->h_group[i]; P.gj = m->h_group[j];
+        pairs.push_back(P);
+      }
+    }
+    int rc;
+    if (!pairs.empty() && (rc = upload(s, m->duffy_pairs, pairs.data(), sizeof(DuffyPair) * pairs.size()))) return rc;
+    m->n_duffy = (int64_t)pairs.size();
+    m->duffy_built = true;
+  }
+  auto it = m->duffy_rules.find(nquad);
+  if (it == m->duffy_rules.end()) {
+    std::vector<double> p, w;
+    gl1d(nquad, p, w);
+    std::vector<double> buf(2 * nquad);
+    for (int k = 0; k < nquad; ++k) {  // src/DuffyKernel.jl:226-229
+      buf[k] = (p[k] + 1.0) / 2.0;
+      buf[nquad + k] = w[k] / 2.0;
+    }
+    auto b = std::make_unique<DevBuf>();
+    int rc;
+    if ((rc = upload(s, *b, buf.data(), sizeof(double) * buf.size()))) return rc;
+    it = m->duffy_rules.emplace(nquad, std::move(b)).first;
+  }
+  *p01 = it->second->as<double>();
+  *w01 = *p01 + nquad;
+  return RVF_OK;
 }
 
 }  // namespace
@@ -214,22 +288,28 @@ int rvf_solve(rvf_session* s, rvf_mesh* m, const rvf_options* o, double* F_elem,
   cudaSetDevice(s->device);
   int rc = validate_options(m, o);
   if (rc) return rc;
-  if (o->method == RVF_METHOD_MONTE_CARLO) return set_err(RVF_EUNSUPPORTED, "Monte Carlo is not available in this build");
-  if (o->use_duffy) return set_err(RVF_EUNSUPPORTED, "use_duffy is not available in this build");
-  // mixed precision covers surface meshes; curve meshes run the FP64 path
-  const bool mixed = (o->precision == RVF_PREC_MIXED) && (m->dim == 2);
+  const bool mc = (o->method == RVF_METHOD_MONTE_CARLO);
+  // mixed precision covers quadrature on surface meshes; curve meshes and
+  // Monte Carlo (which reproduces the reference's streams) run in FP64
+  const bool mixed = (o->precision == RVF_PREC_MIXED) && (m->dim == 2) && !mc;
   if (mixed && !(o->near_field_factor >= 0.0)) return set_err(RVF_EINVAL, "near_field_factor must be >= 0");
   rvf_stats S{};
   int64_t n_kernels = 0;  // kernels of this library launched by this call
   EvTimer total(s->stream);
   const int64_t N = m->N;
   Tables* T = nullptr;
-  {
+  const double* area_res = nullptr;  // element areas of this result, caller's order
+  if (!mc) {
     EvTimer t(s->stream);
     const bool fresh = m->tables.find(o->nquad) == m->tables.end();
     if ((rc = ensure_tables(s, m, o->nquad, &T))) return rc;
     if (fresh && N > 0) n_kernels += 1;
     S.ms_prep = t.stop();
+    area_res = T->area_orig.as<double>();
+  } else {
+    if (m->mc_area.bytes < sizeof(double) * std::max<int64_t>(N, 1))
+      if ((rc = m->mc_area.alloc(s, sizeof(double) * std::max<int64_t>(N, 1)))) return rc;
+    area_res = m->mc_area.as<double>();
   }
   if (m->F.bytes < sizeof(double) * N * N)
     if ((rc = m->F.alloc(s, sizeof(double) * std::max<int64_t>(N * N, 1)))) return rc;
@@ -239,12 +319,47 @@ int rvf_solve(rvf_session* s, rvf_mesh* m, const rvf_options* o, double* F_elem,
   cudaMemsetAsync(s->err.ptr, 0, sizeof(int), s->stream);
   DevBuf log;
   if (o->ray_log) {
-    if (o->ray_log_pm < T->pmax) return set_err(RVF_EINVAL, "ray_log_pm %d < points per element %d", o->ray_log_pm, T->pmax);
-    size_t lb = (size_t)N * N * o->ray_log_pm * o->ray_log_pm;
+    if (!mc && o->ray_log_pm < T->pmax)
+      return set_err(RVF_EINVAL, "ray_log_pm %d < points per element %d", o->ray_log_pm, T->pmax);
+    // quadrature: [(i*N + j) * pm + p] * pm + q; Monte Carlo: (i*N + j) * n_samples + k
+    size_t lb = (size_t)N * N * (mc ? (size_t)o->n_samples : (size_t)o->ray_log_pm * o->ray_log_pm);
     if ((rc = log.alloc(s, lb))) return rc;
     cudaMemsetAsync(log.ptr, 0, lb, s->stream);
   }
   const bool occ = o->occlusion && m->n_nodes > 0;
+  if (mc) {  // src/GPUMCKernels.jl:295-328
+    McArgs c{};
+    c.N = N;
+    c.nT = (N + kTile - 1) / kTile;
+    c.n_tiles = c.nT * (c.nT + 1) / 2;
+    c.n_samples = o->n_samples;
+    c.seed = o->seed;
+    c.exclude = o->mc_exclude_groups != 0 || m->dim == 1;
+    c.dim3 = (m->dim == 2);
+    c.coords = m->coords.as<double>();
+    c.enodes = m->enodes.as<int32_t>();
+    c.fam = m->fam.as<int8_t>();
+    c.group = m->group.as<int32_t>();
+    c.orig = m->orig.as<int32_t>();
+    c.inv = m->inv.as<int32_t>();
+    c.area_orig = m->mc_area.as<double>();
+    c.F = m->F.as<double>();
+    c.nodes = occ ? m->nodes.as<NodeD>() : nullptr;
+    c.n_nodes = occ ? m->n_nodes : 0;
+    c.tris = occ ? (o->geometric_soup ? m->tris_geo.as<TriD>() : m->tris_ref.as<TriD>()) : nullptr;
+    c.segs = occ ? m->segs.as<SegD>() : nullptr;
+    c.tile_counter = s->tile_counter.as<unsigned long long>();
+    c.counters = s->counters.as<unsigned long long>();
+    c.ray_log = o->ray_log ? log.as<uint8_t>() : nullptr;
+    if (N > 0) {
+      EvTimer t(s->stream);
+      cudaError_t e = launch_mc(c, s->sm_count, s->stream);
+      if (e != cudaSuccess) return cuda_err(e, "Monte Carlo kernel launch");
+      n_kernels += 2;
+      S.ms_pairs = t.stop();
+      if ((rc = read_err(s))) return rc;
+    }
+  } else {
   PairArgs a{};
   a.N = N;
   a.nT = (N + kTile - 1) / kTile;
@@ -303,24 +418,51 @@ int rvf_solve(rvf_session* s, rvf_mesh* m, const rvf_options* o, double* F_elem,
     if (e != cudaSuccess) return cuda_err(e, "pair kernel launch");
     S.ms_pairs = t.stop();
     if ((rc = read_err(s))) return rc;
+    // Duffy integrals overwrite the singular Quad8 pairs (Duffy for
+    // Quad8-Quad8 surface pairs only, src/DuffyKernel.jl:461-463)
+    if (o->use_duffy && m->dim == 2) {
+      EvTimer td(s->stream);
+      DuffyArgs d{};
+      if ((rc = ensure_duffy(s, m, o->nquad, &d.p01, &d.w01))) return rc;
+      d.N = N;
+      d.nq = o->nquad;
+      d.pairs = m->duffy_pairs.as<DuffyPair>();
+      d.n_pairs = m->n_duffy;
+      d.coords = m->coords.as<double>();
+      d.enodes = m->enodes.as<int32_t>();
+      d.area_orig = T->area_orig.as<double>();
+      d.F = m->F.as<double>();
+      d.nodes = a.nodes;
+      d.n_nodes = a.n_nodes;
+      d.tris = a.tris;
+      d.counters = a.counters;
+      if (d.n_pairs > 0) {
+        if ((e = launch_duffy(d, s->stream)) != cudaSuccess) return cuda_err(e, "Duffy kernel launch");
+        n_kernels += 1;
+      }
+      S.ms_duffy = td.stop();
+      S.n_duffy_pairs = m->n_duffy;
+      if ((rc = read_err(s))) return rc;
+    }
     if (N == 1) {  // raw 1x1 zero, area 0 -> F = 0/0 (the reference's result for one element)
       double nanv = std::nan("");
       cudaMemcpyAsync(m->F.ptr, &nanv, sizeof(double), cudaMemcpyHostToDevice, s->stream);
     }
   }
+  }  // quadrature
   {
     EvTimer t(s->stream);
-    if ((rc = run_reduce(s, m, T))) return rc;
+    if ((rc = run_reduce(s, m, area_res))) return rc;
     if (N > 0 && m->G > 0) n_kernels += 3;
     S.ms_reduce = t.stop();
   }
   m->has_result = true;
-  m->result_nquad = o->nquad;
+  m->result_area = area_res;
   {
     EvTimer t(s->stream);
     cudaError_t e = cudaSuccess;
     if (F_elem && N > 0) e = cudaMemcpyAsync(F_elem, m->F.ptr, sizeof(double) * N * N, cudaMemcpyDeviceToHost, s->stream);
-    if (e == cudaSuccess && A_elem && N > 0) e = cudaMemcpyAsync(A_elem, T->area_orig.ptr, sizeof(double) * N, cudaMemcpyDeviceToHost, s->stream);
+    if (e == cudaSuccess && A_elem && N > 0) e = cudaMemcpyAsync(A_elem, area_res, sizeof(double) * N, cudaMemcpyDeviceToHost, s->stream);
     if (e == cudaSuccess && F_group && m->G > 0 && N > 0)
       e = cudaMemcpyAsync(F_group, m->Fgroup.ptr, sizeof(double) * m->G * m->G, cudaMemcpyDeviceToHost, s->stream);
     if (e == cudaSuccess && A_group && m->G > 0 && N > 0)
@@ -367,10 +509,9 @@ int rvf_result_copy(rvf_session* s, rvf_mesh* m, double* F_elem, double* A_elem)
   std::lock_guard<std::mutex> lk(s->mu);
   if (!m->has_result) return set_err(RVF_EINVAL, "no result on this mesh yet");
   cudaSetDevice(s->device);
-  Tables* T = m->tables[m->result_nquad].get();
   cudaError_t e = cudaSuccess;
   if (F_elem) e = cudaMemcpyAsync(F_elem, m->F.ptr, sizeof(double) * m->N * m->N, cudaMemcpyDeviceToHost, s->stream);
-  if (e == cudaSuccess && A_elem) e = cudaMemcpyAsync(A_elem, T->area_orig.ptr, sizeof(double) * m->N, cudaMemcpyDeviceToHost, s->stream);
+  if (e == cudaSuccess && A_elem) e = cudaMemcpyAsync(A_elem, m->result_area, sizeof(double) * m->N, cudaMemcpyDeviceToHost, s->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
   return e == cudaSuccess ? RVF_OK : cuda_err(e, "rvf_result_copy");
 }
@@ -379,7 +520,7 @@ int rvf_result_device(rvf_mesh* m, const double** F_dev, const double** A_dev) {
   if (!m) return set_err(RVF_EINVAL, "null mesh");
   if (!m->has_result) return set_err(RVF_EINVAL, "no result on this mesh yet");
   if (F_dev) *F_dev = m->F.as<double>();
-  if (A_dev) *A_dev = m->tables[m->result_nquad]->area_orig.as<double>();
+  if (A_dev) *A_dev = m->result_area;
   return RVF_OK;
 }
 
