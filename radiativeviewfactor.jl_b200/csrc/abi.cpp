@@ -236,6 +236,8 @@ int mesh_upload(Session* s, const rvf_mesh_desc* d, rvf_mesh** out) {
       if (h.left != 0 && h.left != k + 2) return set_err(RVF_EINVAL, "internal: BVH is not in pre-order");
       n.a = h.tri_count > 0 ? (int32_t)(h.tri_start - 1) : 0;
       n.b = (int32_t)h.tri_count;
+      // the batched traversal deals at most 32 x 8 leaf tests out per round
+      if (n.b > 8) return set_err(RVF_EINVAL, "internal: BVH leaf holds more than 8 primitives");
       n.miss = h.miss == 0 ? M : (int32_t)(h.miss - 1);
       n.pad = 0;
     }

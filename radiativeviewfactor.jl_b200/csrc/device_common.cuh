@@ -257,9 +257,9 @@ __device__ __forceinline__ bool seg_blocks(const SegD& s, const double* xi, cons
 // and reaches the same any-hit answer.  The walk descends when any awake lane
 // hits, and jumps to the smallest wake-up node when no lane is awake.
 // ---------------------------------------------------------------------------
-struct TravCount {
-  uint64_t nodes = 0, prims = 0;
-  uint64_t unsure_slab = 0, unsure_prim = 0;  // FP32 traversal: decisions left to FP64
+struct TravCount {  // per-thread counts (a thread's share stays far below 2^32)
+  uint32_t nodes = 0, prims = 0;
+  uint32_t unsure_slab = 0, unsure_prim = 0;  // FP32 traversal: decisions left to FP64
 };
 
 template <typename NodeT, typename SlabF, typename LeafF>

@@ -1,0 +1,287 @@
+// device_trace.cuh -- compacted shadow-ray batches traced one ray per lane.
+//
+// The pair kernels do not trace a ray when they form it.  A ray whose
+// segment misses the root box of the obstruction BVH is visible (the
+// reference's walk, src/GPUBVH.jl:216-282, ends at the root); every other ray
+// is appended to a per-warp buffer, and a full buffer of 32 rays is traced at
+// once, one ray per lane:
+//   * interior phase: each lane walks its own ray through the pre-order tree
+//     (slab test, descend to node+1 on a pass, jump to the miss link on a
+//     miss) until it reaches a leaf whose box it passes, or the end;
+//   * leaf phase: the primitives of all pending leaves of the warp are dealt
+//     out to the 32 lanes (a lane may test another lane's ray, read from the
+//     warp's shared-memory ray bank), so a leaf of 8 triangles costs one
+//     primitive test per lane instead of eight on one lane.
+// The set of (ray, triangle) tests is exactly the set the reference's walk
+// performs up to its first hit, so the any-hit answer is the reference's.
+#pragma once
+
+#include "device_mixed.cuh"
+
+namespace rvf {
+
+// Per-warp shared-memory scratch: the ray bank with the leaf-phase work
+// lists (RayBank) and, for the fused kernel, the compaction buffers.  3D FP64 rays use o/d/tmax; 2-D segments store
+// their two end points in o (x, y) and d (x, y); FP32 rays use the *f arrays.
+struct RayBank {
+  double o[3][32];
+  double d[3][32];
+  double tmax[32];
+  float of[3][32];
+  float df[3][32];
+  float tmaxf[32];
+  float deltaf[32];
+  int32_t gi[32], gj[32];
+  uint8_t owner[256];     // leaf phase: owning lane of each (ray, primitive) item
+  uint8_t hit[32];
+  uint8_t unsure[32];
+};
+
+struct WarpScratch {
+  RayBank bank;
+  double contrib[2][64];  // [0] FP64 / main buffer, [1] FP32 buffer (mixed)
+  uint32_t meta[2][64];
+};
+
+// buffer entry: owner lane (5 bits), swapped (1 bit), source point p (6 bits),
+// destination point q (6 bits)
+__device__ __forceinline__ uint32_t enc_entry(int lane, bool sw, int p, int q) {
+  return (uint32_t)lane | ((uint32_t)sw << 5) | ((uint32_t)p << 6) | ((uint32_t)q << 12);
+}
+__device__ __forceinline__ int ent_lane(uint32_t e) { return (int)(e & 31u); }
+__device__ __forceinline__ bool ent_sw(uint32_t e) { return ((e >> 5) & 1u) != 0; }
+__device__ __forceinline__ int ent_p(uint32_t e) { return (int)((e >> 6) & 63u); }
+__device__ __forceinline__ int ent_q(uint32_t e) { return (int)((e >> 12) & 63u); }
+
+__device__ __forceinline__ uint32_t lanemask_lt() {
+  uint32_t m;
+  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+  return m;
+}
+
+// Appends the lanes with `push` to buffer b (count n, warp-uniform).
+__device__ __forceinline__ void buf_push(WarpScratch& ws, int b, int& n, bool push, uint32_t meta, double contrib) {
+  const uint32_t m = __ballot_sync(kFull, push);
+  if (m == 0) return;
+  if (push) {
+    const int pos = n + __popc(m & lanemask_lt());
+    ws.meta[b][pos] = meta;
+    ws.contrib[b][pos] = contrib;
+  }
+  n += __popc(m);
+  __syncwarp();
+}
+
+// After the first `used` entries (used <= 32) were consumed: move the rest down.
+__device__ __forceinline__ void buf_shift(WarpScratch& ws, int b, int& n, int used) {
+  const int rest = n - used;
+  const int lane = threadIdx.x & 31;
+  uint32_t m = 0;
+  double c = 0.0;
+  if (lane < rest) {
+    m = ws.meta[b][used + lane];
+    c = ws.contrib[b][used + lane];
+  }
+  __syncwarp();
+  if (lane < rest) {
+    ws.meta[b][lane] = m;
+    ws.contrib[b][lane] = c;
+  }
+  n = rest;
+  __syncwarp();
+}
+
+// Owners add the contributions of their visible entries, in entry order.
+__device__ __forceinline__ void buf_collect(const WarpScratch& ws, int b, int n, uint32_t visible, double& acc) {
+  const int lane = threadIdx.x & 31;
+  for (int t = 0; t < n; ++t) {
+    const uint32_t e = ws.meta[b][t];
+    if (ent_lane(e) == lane && ((visible >> t) & 1u)) acc += ws.contrib[b][t];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Generic batch traversal.  Pol provides
+//   node(const Node&) -> int   kHit / kMiss / kUnsure for the lane's own ray
+//   leaf(const Node&, int& first, int& count)
+//   prim(ws, owner, k) -> int  kHit / kMiss / kUnsure for owner's ray
+// Returns kHit (blocked), kMiss (visible) or kUnsure (FP32 only: some
+// decision of the walk was not certain and no certain hit was found).
+// ---------------------------------------------------------------------------
+template <typename Node, typename Pol>
+__device__ __forceinline__ int trace_batch(bool have, const Node* __restrict__ nodes, int n_nodes, RayBank& ws,
+                                           Pol& pol, TravCount& cnt) {
+  const int lane = threadIdx.x & 31;
+  ws.hit[lane] = 0;
+  ws.unsure[lane] = 0;
+  __syncwarp();
+  int k = 0;
+  bool done = !have;
+  bool unsure = false;
+  for (int round = 0;; ++round) {
+    int la = 0, lc = 0;
+    while (!done && lc == 0) {
+      const Node nd = nodes[k];
+      ++cnt.nodes;
+      const int s = pol.node(nd);
+      int first, count;
+      pol.leaf(nd, first, count);
+      if (s == kUnsure) {
+        unsure = true;
+        ++cnt.unsure_slab;
+        done = true;
+      } else if (s == kHit && count > 0) {
+        la = first;
+        lc = count;
+        k = pol.miss(nd);
+      } else {
+        k = (s == kHit) ? k + 1 : pol.miss(nd);
+      }
+      if (lc == 0 && k >= n_nodes) done = true;
+    }
+    // leaf phase: deal the pending (ray, primitive) tests out to the lanes
+    int incl = lc;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int v = __shfl_up_sync(kFull, incl, o);
+      if (lane >= o) incl += v;
+    }
+    const int total = __shfl_sync(kFull, incl, 31);
+    if (total == 0) break;
+    const int excl = incl - lc;
+    for (int u = 0; u < lc; ++u) ws.owner[excl + u] = (uint8_t)lane;
+    __syncwarp();
+    for (int base = 0; base < total; base += 32) {
+      const int t = base + lane;
+      const int o = (t < total) ? (int)ws.owner[t] : 0;
+      const int oa = __shfl_sync(kFull, la, o);
+      const int oe = __shfl_sync(kFull, excl, o);
+      if (t < total) {
+        const int r = pol.prim(ws, o, oa + (t - oe), cnt);
+        if (r == kHit) ws.hit[o] = 1;
+        else if (r == kUnsure) ws.unsure[o] = 1;
+      }
+      __syncwarp();
+    }
+    if (lc > 0) {
+      if (ws.hit[lane]) done = true;
+      else if (k >= n_nodes) done = true;
+    }
+    __syncwarp();
+  }
+  __syncwarp();
+  const bool hit = ws.hit[lane] != 0;
+  unsure = unsure || ws.unsure[lane] != 0;
+  __syncwarp();
+  if (!have) return kMiss;
+  if (hit) return kHit;
+  return unsure ? kUnsure : kMiss;
+}
+
+// FP64 3D rays, reference arithmetic (slab_d / mt_d).
+struct PolD3 {
+  RayD R;
+  const TriD* tris;
+  __device__ __forceinline__ void store(RayBank& ws, int lane, int32_t gi, int32_t gj) const {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      ws.o[c][lane] = R.o[c];
+      ws.d[c][lane] = R.d[c];
+    }
+    ws.tmax[lane] = R.tmax;
+    ws.gi[lane] = gi;
+    ws.gj[lane] = gj;
+  }
+  __device__ __forceinline__ int node(const NodeD& nd) const { return slab_d(nd, R) ? kHit : kMiss; }
+  __device__ __forceinline__ void leaf(const NodeD& nd, int& first, int& count) const {
+    first = nd.a;
+    count = nd.b;
+  }
+  __device__ __forceinline__ int miss(const NodeD& nd) const { return nd.miss; }
+  __device__ __forceinline__ int prim(const RayBank& ws, int o, int k, TravCount& cnt) const {
+    const TriD tr = tris[k];
+    if (tr.group == ws.gi[o] || tr.group == ws.gj[o]) return kMiss;
+    ++cnt.prims;
+    RayD Q;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      Q.o[c] = ws.o[c][o];
+      Q.d[c] = ws.d[c][o];
+    }
+    Q.tmax = ws.tmax[o];
+    return mt_d(tr, Q) ? kHit : kMiss;
+  }
+};
+
+// FP64 2-D segments (src/BVH.jl:265-322): a = first end point, b = second,
+// exactly as seg_blocks receives them.
+struct PolD2 {
+  double a[2], b[2];
+  const SegD* segs;
+  __device__ __forceinline__ void store(RayBank& ws, int lane, int32_t gi, int32_t gj) const {
+    ws.o[0][lane] = a[0];
+    ws.o[1][lane] = a[1];
+    ws.d[0][lane] = b[0];
+    ws.d[1][lane] = b[1];
+    ws.gi[lane] = gi;
+    ws.gj[lane] = gj;
+  }
+  __device__ __forceinline__ int node(const NodeD& nd) const {
+    const double xlo = fmin(a[0], b[0]), xhi = fmax(a[0], b[0]);
+    const double ylo = fmin(a[1], b[1]), yhi = fmax(a[1], b[1]);
+    return (nd.lo[0] > xhi || nd.hi[0] < xlo || nd.lo[1] > yhi || nd.hi[1] < ylo) ? kMiss : kHit;
+  }
+  __device__ __forceinline__ void leaf(const NodeD& nd, int& first, int& count) const {
+    first = nd.a;
+    count = nd.b;
+  }
+  __device__ __forceinline__ int miss(const NodeD& nd) const { return nd.miss; }
+  __device__ __forceinline__ int prim(const RayBank& ws, int o, int k, TravCount& cnt) const {
+    const SegD sg = segs[k];
+    if (sg.group == ws.gi[o] || sg.group == ws.gj[o]) return kMiss;
+    ++cnt.prims;
+    const double xa[2] = {ws.o[0][o], ws.o[1][o]}, xb[2] = {ws.d[0][o], ws.d[1][o]};
+    return seg_blocks(sg, xa, xb) ? kHit : kMiss;
+  }
+};
+
+// FP32 3D rays with certified decisions (slab_f / mt_f).
+struct PolF3 {
+  RayF R;
+  const TriF* tris;
+  __device__ __forceinline__ void store(RayBank& ws, int lane, int32_t gi, int32_t gj) const {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      ws.of[c][lane] = R.o[c];
+      ws.df[c][lane] = R.d[c];
+    }
+    ws.tmaxf[lane] = R.tmax;
+    ws.deltaf[lane] = R.delta;
+    ws.gi[lane] = gi;
+    ws.gj[lane] = gj;
+  }
+  __device__ __forceinline__ int node(const NodeF& nd) const { return slab_f(nd, R); }
+  __device__ __forceinline__ void leaf(const NodeF& nd, int& first, int& count) const {
+    first = nd.ab >> 4;
+    count = nd.ab & 15;
+  }
+  __device__ __forceinline__ int miss(const NodeF& nd) const { return nd.miss; }
+  __device__ __forceinline__ int prim(const RayBank& ws, int o, int k, TravCount& cnt) const {
+    const TriF tr = tris[k];
+    if (tr.group == ws.gi[o] || tr.group == ws.gj[o]) return kMiss;
+    ++cnt.prims;
+    RayF Q;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      Q.o[c] = ws.of[c][o];
+      Q.d[c] = ws.df[c][o];
+    }
+    Q.tmax = ws.tmaxf[o];
+    Q.delta = ws.deltaf[o];
+    const int r = mt_f(tr, Q);
+    if (r == kUnsure) ++cnt.unsure_prim;
+    return r;
+  }
+};
+
+}  // namespace rvf

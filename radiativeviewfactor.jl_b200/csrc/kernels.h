@@ -9,6 +9,37 @@
 
 namespace rvf {
 
+// Wavefront pipeline state (kernels_wave.cu).
+enum : int {
+  kCtrTile = 0,    // tile claims
+  kCtrResv = 1,    // reserved queue records
+  kCtrResvS = 2,   // reserved pending-pair slots
+  kCtrRec64 = 3,   // records in the FP64 queue
+  kCtrRec32 = 4,   // records in the FP32 queue
+  kCtrSlots = 5,   // pending-pair slots in use
+  kCtrHead64 = 6,  // traversal progress, FP64 queue
+  kCtrHead32 = 7,  // traversal progress, FP32 queue
+  kCtrCount = 8
+};
+
+// A pair with queued rays: internal element indices and the sum of its
+// immediately decided terms.
+struct PendSlot {
+  int32_t i, j;
+  double acc;
+};
+
+struct WaveQ {
+  uint64_t* rec64;  // FP64 ray queue
+  uint64_t* rec32;  // FP32 ray queue (mixed precision)
+  int64_t cap;      // records per queue
+  PendSlot* slots;
+  unsigned long long* vis;  // slots x vis_words visibility bits, bit p*pmax+q
+  int64_t scap;
+  int vis_words;
+  unsigned long long* ctr;  // kCtrCount counters
+};
+
 struct PrepArgs {
   int64_t N;
   int pmax;
@@ -56,6 +87,7 @@ struct PairArgs {
   int* err;
   uint8_t* ray_log;              // device, or null
   int log_pm;
+  WaveQ q;                       // wavefront queues (the fused kernel ignores them)
 };
 
 struct RedArgs {
@@ -109,7 +141,53 @@ struct MixedArgs {
   int* err;
   uint8_t* ray_log;
   int log_pm;
+  WaveQ q;
 };
+
+struct TraceArgs {
+  int64_t N;
+  int pmax;
+  bool dim3;
+  const double* tab;
+  const float* tabf;
+  const double* cen;
+  const int32_t* group;
+  const int32_t* orig;
+  const NodeD* nodes;
+  const NodeF* nodesf;
+  int n_nodes;
+  bool nodes_in_smem;
+  const TriD* tris;
+  const TriF* trisf;
+  const SegD* segs;
+  float delta;
+  WaveQ q;
+  unsigned long long* counters;
+  uint8_t* ray_log;
+  int log_pm;
+};
+
+struct ResolveArgs {
+  int64_t N;
+  int pmax;
+  bool dim3;
+  const double* tab;
+  const float* tabf;
+  const double* cen;
+  const double* diam;
+  double near_factor;
+  const double* area;
+  const int32_t* orig;
+  double* F;
+  WaveQ q;
+};
+
+size_t gen_smem_bytes(bool mixed, int pmax, int n_nodes_smem, bool occ);
+size_t trace_smem_bytes(bool fp32, int n_nodes_smem);
+cudaError_t launch_gen_fp64(const PairArgs& a, int sm_count, cudaStream_t st);
+cudaError_t launch_gen_mixed(const MixedArgs& a, int sm_count, cudaStream_t st);
+cudaError_t launch_trace(const TraceArgs& a, bool fp32, int sm_count, cudaStream_t st);
+cudaError_t launch_resolve(const ResolveArgs& a, bool mixed, int sm_count, cudaStream_t st);
 
 // A Quad8 pair sharing corner nodes (src/DuffyKernel.jl:95-115), i < j in the
 // caller's order (the reference integrates with elem_i = the lower index).
@@ -168,9 +246,7 @@ struct McArgs {
 cudaError_t launch_mc(const McArgs& a, int sm_count, cudaStream_t st);
 cudaError_t launch_prep(const PrepArgs& a, cudaStream_t st);
 cudaError_t launch_prep_f32(const PrepF32Args& a, cudaStream_t st);
-size_t mixed_smem_bytes(int pmax, int n_nodes_smem);
-cudaError_t launch_pairs_mixed(const MixedArgs& a, int sm_count, cudaStream_t st);
-size_t pair_smem_bytes(int pmax, int n_nodes_smem);
+size_t pair_smem_bytes(int pmax, int n_nodes_smem, bool occ);
 cudaError_t launch_pairs_fp64(const PairArgs& a, int sm_count, cudaStream_t st);
 cudaError_t launch_reduce(const RedArgs& a, cudaStream_t st);
 

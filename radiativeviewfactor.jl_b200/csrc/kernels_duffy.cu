@@ -184,12 +184,11 @@ __global__ void __launch_bounds__(256) k_duffy(DuffyArgs a) {
   }
   if (a.counters) {
     rays = warp_sum_u64(rays);
-    tc.prims = warp_sum_u64(tc.prims);
-    tc.nodes = warp_sum_u64(tc.nodes);
+    const uint64_t s_prims = warp_sum_u64(tc.prims), s_nodes = warp_sum_u64(tc.nodes);
     if ((threadIdx.x & 31) == 0) {
       atomicAdd(a.counters + 1, rays);
-      atomicAdd(a.counters + 2, tc.nodes);
-      atomicAdd(a.counters + 3, tc.prims);
+      atomicAdd(a.counters + 2, s_nodes);
+      atomicAdd(a.counters + 3, s_prims);
     }
   }
 }

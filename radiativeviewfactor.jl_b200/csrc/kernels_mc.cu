@@ -208,13 +208,12 @@ __global__ void __launch_bounds__(256) k_pairs_mc(McArgs a) {
   }
   n_rays = warp_sum_u64(n_rays);
   n_pp = warp_sum_u64(n_pp);
-  tc.nodes = warp_sum_u64(tc.nodes);
-  tc.prims = warp_sum_u64(tc.prims);
+  const uint64_t s_nodes = warp_sum_u64(tc.nodes), s_prims = warp_sum_u64(tc.prims);
   if (lane == 0 && a.counters) {
     atomicAdd(a.counters + 0, n_pp);
     atomicAdd(a.counters + 1, n_rays);
-    atomicAdd(a.counters + 2, tc.nodes);
-    atomicAdd(a.counters + 3, tc.prims);
+    atomicAdd(a.counters + 2, s_nodes);
+    atomicAdd(a.counters + 3, s_prims);
   }
 }
 

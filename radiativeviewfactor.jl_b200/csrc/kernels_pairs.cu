@@ -9,7 +9,7 @@
 
 #include <cstdint>
 
-#include "device_common.cuh"
+#include "device_trace.cuh"
 #include "kernels.h"
 
 namespace rvf {
@@ -88,21 +88,80 @@ __global__ void k_prep(PrepArgs a) {
 // points x 7 doubles) is staged into shared memory with one cp.async.bulk;
 // warp w integrates rows i = 32 bi + w + 8k against the 32 destination
 // elements j = 32 bj + lane, whose points are read as coalesced SoA loads.
-// Each lane keeps one destination point in registers and loops over the
-// warp-uniform source points, so every shadow ray of a warp step leaves the
-// same origin towards 32 neighbouring targets and the traversal is coherent.
-// The raw tile goes through shared memory so that both F[i,j] = raw/A_i and
-// F[j,i] = raw/A_j are written as full 256-byte column segments.
+//
+// Shadow rays (src/GPUKernels.jl:289-304) are formed with the reference's
+// arithmetic.  A ray that misses the root box is visible and its term is
+// summed at once; the others go to the warp's buffer with their term
+// w_j (w_i K), and every 32 buffered rays are traced together, one per lane
+// (device_trace.cuh).  The owners add the terms of their visible rays in
+// buffer order after each batch, and the last partial batch of a row is
+// traced before the row's F entries are written.
 // ---------------------------------------------------------------------------
+// Traces the first n buffered rays of the warp (rows of one source element
+// against the destination tile jt) and adds the visible terms to accd.  Kept
+// out of line: it runs once per 32 rays and would otherwise raise the
+// register pressure of the quadrature loop.
+template <bool DIM3>
+__device__ __noinline__ void flush_fp64(const PairArgs& a, WarpScratch& ws, const NodeD* nodes, const double* ib,
+                                        const double* jt, int n, int& nbuf, int32_t gi, int32_t gj, int64_t oi,
+                                        int64_t oj, double& accd, TravCount& tc) {
+  const int lane = threadIdx.x & 31;
+  const int pm = a.pmax;
+  const bool have = lane < n;
+  const uint32_t e = have ? ws.meta[0][lane] : 0u;
+  const int L = ent_lane(e), p = ent_p(e), q = ent_q(e);
+  const bool esw = ent_sw(e);
+  const int32_t gL = __shfl_sync(kFull, gj, L);
+  const int64_t oL = __shfl_sync(kFull, oj, L);
+  double xi[3], xj[3];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    xi[c] = have ? ib[(c * pm + p) * kTile] : 0.0;
+    xj[c] = have ? jt[(c * pm + q) * kTile + L] : 0.0;
+  }
+  int r;
+  if (DIM3) {
+    PolD3 pol;
+    pol.tris = a.tris;
+    const double rx = xj[0] - xi[0], ry = xj[1] - xi[1], rz = xj[2] - xi[2];
+    const double r2 = (rx * rx + ry * ry) + rz * rz;
+    if (have) {
+      if (esw) make_ray(xj, -rx, -ry, -rz, r2, pol.R);
+      else make_ray(xi, rx, ry, rz, r2, pol.R);
+      pol.store(ws.bank, lane, gi, gL);
+    }
+    r = trace_batch(have, nodes, a.n_nodes, ws.bank, pol, tc);
+  } else {
+    PolD2 pol;
+    pol.segs = a.segs;
+    pol.a[0] = esw ? xj[0] : xi[0];
+    pol.a[1] = esw ? xj[1] : xi[1];
+    pol.b[0] = esw ? xi[0] : xj[0];
+    pol.b[1] = esw ? xi[1] : xj[1];
+    if (have) pol.store(ws.bank, lane, gi, gL);
+    r = trace_batch(have, nodes, a.n_nodes, ws.bank, pol, tc);
+  }
+  if (have && a.ray_log) {
+    uint8_t* lp = a.ray_log + ((uint64_t)(esw ? oL : oi) * a.N + (esw ? oi : oL)) * a.log_pm * a.log_pm;
+    lp[esw ? q * a.log_pm + p : p * a.log_pm + q] = (r == kHit) ? 2 : 1;
+  }
+  const uint32_t vis = __ballot_sync(kFull, have && r != kHit);
+  buf_collect(ws, 0, n, vis, accd);
+  buf_shift(ws, 0, nbuf, n);
+}
+
 template <bool DIM3, bool OCC>
-__global__ void __launch_bounds__(256) k_pairs_fp64(PairArgs a) {
+__global__ void __launch_bounds__(256, 2) k_pairs_fp64(PairArgs a) {
   extern __shared__ __align__(128) unsigned char smem[];
+  const int pm = a.pmax;
   double* iblk = reinterpret_cast<double*>(smem);
-  NodeD* snodes = reinterpret_cast<NodeD*>(iblk + kComp * a.pmax * kTile);
-  uint64_t* bar = reinterpret_cast<uint64_t*>(snodes + (a.nodes_in_smem ? a.n_nodes : 0));
+  NodeD* snodes = reinterpret_cast<NodeD*>(iblk + kComp * pm * kTile);
+  WarpScratch* wsa = reinterpret_cast<WarpScratch*>(snodes + (a.nodes_in_smem ? a.n_nodes : 0));
+  uint64_t* bar = reinterpret_cast<uint64_t*>(wsa + (OCC ? 8 : 0));
   __shared__ int64_t s_tile;
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  WarpScratch& ws = wsa[OCC ? warp : 0];
   const NodeD* nodes = a.nodes;
   if (OCC && a.nodes_in_smem) {
     const int4* src = reinterpret_cast<const int4*>(a.nodes);
@@ -113,9 +172,9 @@ __global__ void __launch_bounds__(256) k_pairs_fp64(PairArgs a) {
   if (threadIdx.x == 0) mbar_init(bar, 1);
   __syncthreads();
 
-  const uint32_t blk_bytes = (uint32_t)(kComp * a.pmax * kTile * sizeof(double));
+  const uint32_t blk_bytes = (uint32_t)(kComp * pm * kTile * sizeof(double));
   uint32_t phase = 0;
-  uint64_t n_rays = 0, n_pp = 0;
+  uint32_t n_rays = 0, n_pp = 0;
   TravCount tc;
   for (;;) {
     if (threadIdx.x == 0) {
@@ -124,7 +183,7 @@ __global__ void __launch_bounds__(256) k_pairs_fp64(PairArgs a) {
         int64_t bi, bj;
         tile_coords(s_tile, a.nT, bi, bj);
         mbar_expect_tx(bar, blk_bytes);
-        bulk_g2s(iblk, a.tab + bi * kComp * a.pmax * kTile, blk_bytes, bar);
+        bulk_g2s(iblk, a.tab + bi * kComp * pm * kTile, blk_bytes, bar);
       }
     }
     __syncthreads();
@@ -139,127 +198,112 @@ __global__ void __launch_bounds__(256) k_pairs_fp64(PairArgs a) {
     }
     phase ^= 1u;
 
-    const int64_t j = bj * kTile + lane;
     const int64_t N = a.N;
+    const int64_t j = bj * kTile + lane;
     const int64_t oj = (j < N) ? (a.orig ? (int64_t)a.orig[j] : j) : 0;
-    const double* jb = a.tab + bj * kComp * a.pmax * kTile + lane;
+    const double* jt = a.tab + bj * kComp * pm * kTile;  // destination tile block
+    const double* jb = jt + lane;
     for (int rr = 0; rr < kTile / 8; ++rr) {
       const int li = warp + 8 * rr;
       const int64_t i = bi * kTile + li;
-      double acc = 0.0;
-      if (i < a.N) {  // warp-uniform
-        const bool valid = (j < a.N) && (i < j);
-        const int64_t oi = a.orig ? (int64_t)a.orig[i] : i;
-        // the reference casts from the element with the lower (caller's) index
-        const bool sw = valid && oi > oj;
-        const int npi = a.np[i];
-        int npj = valid ? a.np[j] : 0;
-        // Two elements whose points all share one normal, bit for bit, have
-        // cos_j = -cos_i exactly at every point pair: K = 0, no rays.
-        if (valid && a.flat[i] && a.flat[j] && a.nrm[3 * i] == a.nrm[3 * j] &&
-            a.nrm[3 * i + 1] == a.nrm[3 * j + 1] && a.nrm[3 * i + 2] == a.nrm[3 * j + 2])
-          npj = 0;
-        const int qmax = __reduce_max_sync(kFull, npj);
-        const int32_t gi = a.group[i];
-        const int32_t gj = valid ? a.group[j] : gi;
-        const double* ib = iblk + li;
-        uint8_t* logp = (a.ray_log && valid)
-                            ? a.ray_log + ((uint64_t)(sw ? oj : oi) * a.N + (sw ? oi : oj)) * a.log_pm * a.log_pm
-                            : nullptr;
-        for (int q = 0; q < qmax; ++q) {
-          const bool lq = q < npj;
-          double xj[3], nj[3], wj;
-          if (lq) {
-            xj[0] = jb[(0 * a.pmax + q) * kTile];
-            xj[1] = jb[(1 * a.pmax + q) * kTile];
-            xj[2] = jb[(2 * a.pmax + q) * kTile];
-            nj[0] = jb[(3 * a.pmax + q) * kTile];
-            nj[1] = jb[(4 * a.pmax + q) * kTile];
-            nj[2] = jb[(5 * a.pmax + q) * kTile];
-            wj = jb[(6 * a.pmax + q) * kTile];
-          } else {
-            xj[0] = xj[1] = xj[2] = 0.0;
-            nj[0] = nj[1] = nj[2] = 0.0;
-            wj = 0.0;
-          }
-          double inner = 0.0;
-          for (int p = 0; p < npi; ++p) {
-            double xi[3], ni[3];
-            xi[0] = ib[(0 * a.pmax + p) * kTile];
-            xi[1] = ib[(1 * a.pmax + p) * kTile];
-            xi[2] = ib[(2 * a.pmax + p) * kTile];
-            ni[0] = ib[(3 * a.pmax + p) * kTile];
-            ni[1] = ib[(4 * a.pmax + p) * kTile];
-            ni[2] = ib[(5 * a.pmax + p) * kTile];
-            const double wi = ib[(6 * a.pmax + p) * kTile];
-            const double rx = xj[0] - xi[0], ry = xj[1] - xi[1], rz = xj[2] - xi[2];
-            const double r2 = (rx * rx + ry * ry) + rz * rz;
-            double K = lq ? k_fast<DIM3>(rx, ry, rz, r2, ni, nj) : 0.0;
-            n_pp += lq ? 1 : 0;
-            if (OCC) {
-              uint8_t lg = 0;
-              if (DIM3) {
-                RayD R;
-                bool cast = (K > 0.0) && (sw ? make_ray(xj, -rx, -ry, -rz, r2, R) : make_ray(xi, rx, ry, rz, r2, R));
-                n_rays += cast ? 1 : 0;
-                bool blocked = packet_any_hit(
-                    cast, nodes, a.n_nodes, [&](const NodeD& nd) { return slab_d(nd, R); },
-                    [&](int k, bool test) {
-                      const TriD tr = a.tris[k];
-                      if (!test || tr.group == gi || tr.group == gj) return false;
-                      ++tc.prims;
-                      return mt_d(tr, R);
-                    },
-                    tc);
-                if (cast) lg = blocked ? 2 : 1;
-                if (blocked) K = 0.0;
-              } else {
-                bool cast = K > 0.0;
-                n_rays += cast ? 1 : 0;
-                const double rxlo = fmin(xi[0], xj[0]), rxhi = fmax(xi[0], xj[0]);
-                const double rylo = fmin(xi[1], xj[1]), ryhi = fmax(xi[1], xj[1]);
-                bool blocked = packet_any_hit(
-                    cast, nodes, a.n_nodes,
-                    [&](const NodeD& nd) {
-                      return !(nd.lo[0] > rxhi || nd.hi[0] < rxlo || nd.lo[1] > ryhi || nd.hi[1] < rylo);
-                    },
-                    [&](int k, bool test) {
-                      const SegD sg = a.segs[k];
-                      if (!test || sg.group == gi || sg.group == gj) return false;
-                      ++tc.prims;
-                      return sw ? seg_blocks(sg, xj, xi) : seg_blocks(sg, xi, xj);
-                    },
-                    tc);
-                if (cast) lg = blocked ? 2 : 1;
-                if (blocked) K = 0.0;
+      if (i >= N) continue;  // warp-uniform
+      const bool valid = (j < N) && (i < j);
+      const int64_t oi = a.orig ? (int64_t)a.orig[i] : i;
+      // the reference casts from the element with the lower (caller's) index
+      const bool sw = valid && oi > oj;
+      const int npi = a.np[i];
+      int npj = valid ? a.np[j] : 0;
+      // Two elements whose points all share one normal, bit for bit, have
+      // cos_j = -cos_i exactly at every point pair: K = 0, no rays.
+      if (valid && a.flat[i] && a.flat[j] && a.nrm[3 * i] == a.nrm[3 * j] &&
+          a.nrm[3 * i + 1] == a.nrm[3 * j + 1] && a.nrm[3 * i + 2] == a.nrm[3 * j + 2])
+        npj = 0;
+      const int qmax = __reduce_max_sync(kFull, npj);
+      const int32_t gi = a.group[i];
+      const int32_t gj = valid ? a.group[j] : gi;
+      const double* ib = iblk + li;
+      uint8_t* logp = (a.ray_log && valid)
+                          ? a.ray_log + ((uint64_t)(sw ? oj : oi) * N + (sw ? oi : oj)) * a.log_pm * a.log_pm
+                          : nullptr;
+      double acc = 0.0, accd = 0.0;
+      int nbuf = 0;  // warp-uniform buffer fill
+
+      for (int q = 0; q < qmax; ++q) {
+        const bool lq = q < npj;
+        double xj[3], nj[3], wj;
+        if (lq) {
+          xj[0] = jb[(0 * pm + q) * kTile];
+          xj[1] = jb[(1 * pm + q) * kTile];
+          xj[2] = jb[(2 * pm + q) * kTile];
+          nj[0] = jb[(3 * pm + q) * kTile];
+          nj[1] = jb[(4 * pm + q) * kTile];
+          nj[2] = jb[(5 * pm + q) * kTile];
+          wj = jb[(6 * pm + q) * kTile];
+        } else {
+          xj[0] = xj[1] = xj[2] = 0.0;
+          nj[0] = nj[1] = nj[2] = 0.0;
+          wj = 0.0;
+        }
+        double inner = 0.0;
+        for (int p = 0; p < npi; ++p) {
+          double xi[3], ni[3];
+          xi[0] = ib[(0 * pm + p) * kTile];
+          xi[1] = ib[(1 * pm + p) * kTile];
+          xi[2] = ib[(2 * pm + p) * kTile];
+          ni[0] = ib[(3 * pm + p) * kTile];
+          ni[1] = ib[(4 * pm + p) * kTile];
+          ni[2] = ib[(5 * pm + p) * kTile];
+          const double wi = ib[(6 * pm + p) * kTile];
+          const double rx = xj[0] - xi[0], ry = xj[1] - xi[1], rz = xj[2] - xi[2];
+          const double r2 = (rx * rx + ry * ry) + rz * rz;
+          double K = lq ? k_fast<DIM3>(rx, ry, rz, r2, ni, nj) : 0.0;
+          n_pp += lq ? 1 : 0;
+          if (OCC) {
+            bool cast, defer = false;
+            const NodeD& root = nodes[0];
+            if (DIM3) {
+              RayD R;
+              cast = (K > 0.0) && (sw ? make_ray(xj, -rx, -ry, -rz, r2, R) : make_ray(xi, rx, ry, rz, r2, R));
+              if (cast) defer = slab_d(root, R);
+            } else {
+              cast = K > 0.0;
+              if (cast) {
+                PolD2 pol;
+                pol.a[0] = xi[0]; pol.a[1] = xi[1];
+                pol.b[0] = xj[0]; pol.b[1] = xj[1];
+                defer = pol.node(root) == kHit;
               }
-              if (logp && lq) logp[sw ? q * a.log_pm + p : p * a.log_pm + q] = lg;
             }
-            inner = fma(wi, K, inner);
+            n_rays += cast ? 1 : 0;
+            if (logp && cast && !defer) logp[sw ? q * a.log_pm + p : p * a.log_pm + q] = 1;
+            buf_push(ws, 0, nbuf, defer, enc_entry(lane, sw, p, q), wj * (wi * K));
+            if (defer) K = 0.0;
+            if (nbuf >= 32) flush_fp64<DIM3>(a, ws, nodes, ib, jt, 32, nbuf, gi, gj, oi, oj, accd, tc);
           }
-          acc = fma(wj, inner, acc);
+          inner = fma(wi, K, inner);
         }
-        // F[i,j] = raw/A_i and F[j,i] = raw/A_j in the caller's element order
-        if (valid) {
-          a.F[oi + oj * N] = acc / a.area[i];
-          a.F[oj + oi * N] = acc / a.area[j];
-        } else if (j == i) {
-          a.F[oi + oi * N] = 0.0 / a.area[i];
-        }
+        acc = fma(wj, inner, acc);
+      }
+      if (OCC && nbuf > 0) flush_fp64<DIM3>(a, ws, nodes, ib, jt, nbuf, nbuf, gi, gj, oi, oj, accd, tc);
+      const double raw = acc + accd;
+      // F[i,j] = raw/A_i and F[j,i] = raw/A_j in the caller's element order
+      if (valid) {
+        a.F[oi + oj * N] = raw / a.area[i];
+        a.F[oj + oi * N] = raw / a.area[j];
+      } else if (j == i) {
+        a.F[oi + oi * N] = 0.0 / a.area[i];
       }
     }
     __syncthreads();
   }
   // counters (one atomic per warp)
-  n_rays = warp_sum_u64(n_rays);
-  n_pp = warp_sum_u64(n_pp);
-  tc.nodes = warp_sum_u64(tc.nodes);
-  tc.prims = warp_sum_u64(tc.prims);
+  const uint64_t s_rays = warp_sum_u64(n_rays), s_pp = warp_sum_u64(n_pp), s_nodes = warp_sum_u64(tc.nodes),
+                 s_prims = warp_sum_u64(tc.prims);
   if (lane == 0 && a.counters) {
-    atomicAdd(a.counters + 0, n_pp);
-    atomicAdd(a.counters + 1, n_rays);
-    atomicAdd(a.counters + 2, tc.nodes);
-    atomicAdd(a.counters + 3, tc.prims);
+    atomicAdd(a.counters + 0, s_pp);
+    atomicAdd(a.counters + 1, s_rays);
+    atomicAdd(a.counters + 2, s_nodes);
+    atomicAdd(a.counters + 3, s_prims);
   }
 }
 
@@ -344,8 +388,9 @@ cudaError_t launch_prep(const PrepArgs& a, cudaStream_t st) {
   return cudaGetLastError();
 }
 
-size_t pair_smem_bytes(int pmax, int n_nodes_smem) {
-  return (size_t)kComp * pmax * kTile * sizeof(double) + (size_t)n_nodes_smem * sizeof(NodeD) + 16;
+size_t pair_smem_bytes(int pmax, int n_nodes_smem, bool occ) {
+  return (size_t)kComp * pmax * kTile * sizeof(double) + (size_t)n_nodes_smem * sizeof(NodeD) +
+         (occ ? 8 * sizeof(WarpScratch) : 0) + 16;
 }
 
 template <bool D3, bool O>
@@ -358,7 +403,7 @@ static cudaError_t launch_pairs_t(const PairArgs& a, int grid, size_t smem, cuda
 }
 
 cudaError_t launch_pairs_fp64(const PairArgs& a, int sm_count, cudaStream_t st) {
-  const size_t smem = pair_smem_bytes(a.pmax, a.nodes_in_smem ? a.n_nodes : 0);
+  const size_t smem = pair_smem_bytes(a.pmax, a.nodes_in_smem ? a.n_nodes : 0, a.n_nodes > 0);
   int per_sm = (int)((200 * 1024) / (smem + 1024));
   if (per_sm < 1) per_sm = 1;
   if (per_sm > 4) per_sm = 4;

@@ -1,0 +1,879 @@
+// kernels_wave.cu -- the wavefront pair pipeline with occlusion.
+//
+// Replaces _vf_pair_kernel! (src/GPUKernels.jl:226-323) with its shadow rays
+// (src/GPUKernels.jl:289-304, gpu_intersect_bvh src/GPUBVH.jl:202-285) when
+// the mesh has obstructions.  One chunk of the upper-triangle tiles runs as
+//   1. generation: the quadrature of every pair (tile-staged as in the fused
+//      kernel).  A ray that misses the root box is visible and its term is
+//      summed at once; every other ray is appended to a global ray queue as
+//      (pending-pair slot, p, q, swapped), and its pair gets a slot holding
+//      (i, j, sum of the immediate terms).  Pairs without queued rays write F.
+//   2. traversal: one queued ray per lane, 32 rays per warp traced together
+//      (device_trace.cuh), at the occupancy a traversal-only kernel allows.
+//      Each visible ray sets its (p, q) bit in its slot's visibility words
+//      with an integer atomicOr -- order-independent, hence deterministic.
+//   3. resolve: per pending pair, the terms of the visible queued rays are
+//      formed again with the generation's arithmetic and added, in (p, q)
+//      order, to the immediate sum; F[i,j] and F[j,i] are written.
+// Mixed precision adds an FP32 queue: FP32 rays whose certified traversal is
+// uncertain are appended to the FP64 queue, which is traced after it.
+//
+// Queue capacity is reserved per tile for the worst case (every point pair
+// queued) when a block claims the tile and released down to the actual use
+// when the tile ends, so a chunk never overflows; the host runs chunks until
+// every tile is claimed.
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "device_trace.cuh"
+#include "kernels.h"
+
+namespace rvf {
+
+namespace {
+
+// ray record: q (6 bits), p (6 bits), swapped (1 bit), slot
+__device__ __forceinline__ uint64_t rec_make(int64_t slot, bool sw, int p, int q) {
+  return ((uint64_t)slot << 13) | ((uint64_t)sw << 12) | ((uint64_t)p << 6) | (uint64_t)q;
+}
+__device__ __forceinline__ int64_t rec_slot(uint64_t r) { return (int64_t)(r >> 13); }
+__device__ __forceinline__ bool rec_sw(uint64_t r) { return ((r >> 12) & 1u) != 0; }
+__device__ __forceinline__ int rec_p(uint64_t r) { return (int)((r >> 6) & 63u); }
+__device__ __forceinline__ int rec_q(uint64_t r) { return (int)(r & 63u); }
+
+// (element e, component c, point p) in a tile-blocked table
+__device__ __forceinline__ int64_t tab_at(int64_t e, int c, int p, int pm) {
+  return ((e >> 5) * kComp + c) * (int64_t)pm * kTile + (int64_t)p * kTile + (e & 31);
+}
+
+__device__ __forceinline__ unsigned long long neg(unsigned long long v) { return ~v + 1ull; }
+
+// Per-warp staging of queue records in shared memory.
+__device__ __forceinline__ void stage_push(uint64_t* st, int& n, bool push, uint64_t rec) {
+  const uint32_t m = __ballot_sync(kFull, push);
+  if (m == 0) return;
+  if (push) st[n + __popc(m & lanemask_lt())] = rec;
+  n += __popc(m);
+  __syncwarp();
+}
+
+// Appends the first k (<= 32) staged records to the queue; keeps the rest.
+__device__ __forceinline__ void stage_flush(uint64_t* st, int& n, int k, uint64_t* queue,
+                                            unsigned long long* count, unsigned long long* tile_used) {
+  const int lane = threadIdx.x & 31;
+  unsigned long long base = 0;
+  if (lane == 0) {
+    base = atomicAdd(count, (unsigned long long)k);
+    atomicAdd(tile_used, (unsigned long long)k);
+  }
+  base = __shfl_sync(kFull, base, 0);
+  if (lane < k) queue[base + lane] = st[lane];
+  const int rest = n - k;
+  const uint64_t v = (lane < rest) ? st[k + lane] : 0;
+  __syncwarp();
+  if (lane < rest) st[lane] = v;
+  n = rest;
+  __syncwarp();
+}
+
+// Gives lanes with `need` a fresh pending-pair slot and clears its visibility words.
+__device__ __forceinline__ void slot_alloc(const WaveQ& q, bool need, int64_t& slot, unsigned long long* tile_slots) {
+  const uint32_t m = __ballot_sync(kFull, need);
+  if (m == 0) return;
+  const int lane = threadIdx.x & 31;
+  unsigned long long base = 0;
+  if (lane == 0) {
+    base = atomicAdd(q.ctr + kCtrSlots, (unsigned long long)__popc(m));
+    atomicAdd(tile_slots, (unsigned long long)__popc(m));
+  }
+  base = __shfl_sync(kFull, base, 0);
+  if (need) {
+    slot = (int64_t)base + __popc(m & lanemask_lt());
+    for (int w = 0; w < q.vis_words; ++w) q.vis[slot * q.vis_words + w] = 0ull;
+  }
+}
+
+// Block-level tile claim with worst-case queue reservation.  Returns the
+// tile, or -1 when the chunk is full or every tile is claimed.
+__device__ __forceinline__ int64_t claim_tile(const WaveQ& q, int64_t n_tiles, bool occ,
+                                              unsigned long long need, unsigned long long need_s) {
+  if (occ) {
+    const unsigned long long r = atomicAdd(q.ctr + kCtrResv, need);
+    const unsigned long long rs = atomicAdd(q.ctr + kCtrResvS, need_s);
+    if (r + need > (unsigned long long)q.cap || rs + need_s > (unsigned long long)q.scap) {
+      atomicAdd(q.ctr + kCtrResv, neg(need));
+      atomicAdd(q.ctr + kCtrResvS, neg(need_s));
+      return -1;
+    }
+  }
+  const int64_t t = (int64_t)atomicAdd(q.ctr + kCtrTile, 1ull);
+  if (t >= n_tiles) {
+    if (occ) {
+      atomicAdd(q.ctr + kCtrResv, neg(need));
+      atomicAdd(q.ctr + kCtrResvS, neg(need_s));
+    }
+    return -1;
+  }
+  return t;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// 1. Generation, FP64 (surfaces and curves).
+// ---------------------------------------------------------------------------
+template <bool DIM3, bool OCC>
+__global__ void __launch_bounds__(256, 2) k_gen_fp64(PairArgs a) {
+  extern __shared__ __align__(128) unsigned char smem[];
+  const int pm = a.pmax;
+  double* iblk = reinterpret_cast<double*>(smem);
+  NodeD* snodes = reinterpret_cast<NodeD*>(iblk + kComp * pm * kTile);
+  uint64_t* stage_all = reinterpret_cast<uint64_t*>(snodes + (a.nodes_in_smem ? a.n_nodes : 0));
+  uint64_t* bar = stage_all + (OCC ? 8 * 64 : 0);
+  __shared__ int64_t s_tile;
+  __shared__ unsigned long long s_used, s_slots;
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  uint64_t* stage = stage_all + warp * 64;
+  const NodeD* nodes = a.nodes;
+  if (OCC && a.nodes_in_smem) {
+    const int4* src = reinterpret_cast<const int4*>(a.nodes);
+    int4* dst = reinterpret_cast<int4*>(snodes);
+    for (int k = threadIdx.x; k < a.n_nodes * 4; k += blockDim.x) dst[k] = src[k];
+    nodes = snodes;
+  }
+  if (threadIdx.x == 0) mbar_init(bar, 1);
+  __syncthreads();
+
+  const WaveQ& Q = a.q;
+  const unsigned long long need = (unsigned long long)kTile * kTile * pm * pm, need_s = kTile * kTile;
+  const uint32_t blk_bytes = (uint32_t)(kComp * pm * kTile * sizeof(double));
+  uint32_t phase = 0;
+  uint32_t n_rays = 0, n_pp = 0;
+  for (;;) {
+    if (threadIdx.x == 0) {
+      s_tile = claim_tile(Q, a.n_tiles, OCC, need, need_s);
+      s_used = 0;
+      s_slots = 0;
+      if (s_tile >= 0) {
+        int64_t bi, bj;
+        tile_coords(s_tile, a.nT, bi, bj);
+        mbar_expect_tx(bar, blk_bytes);
+        bulk_g2s(iblk, a.tab + bi * kComp * pm * kTile, blk_bytes, bar);
+      }
+    }
+    __syncthreads();
+    const int64_t t = s_tile;
+    if (t < 0) break;
+    int64_t bi, bj;
+    tile_coords(t, a.nT, bi, bj);
+    const bool ok = mbar_wait_bounded(bar, phase);
+    if (__syncthreads_or(!ok)) {
+      if (threadIdx.x == 0) {
+        atomicOr(a.err, kErrWaitTimeout);
+        if (OCC) {  // give the whole reservation back
+          atomicAdd(Q.ctr + kCtrResv, neg(need));
+          atomicAdd(Q.ctr + kCtrResvS, neg(need_s));
+        }
+      }
+      break;
+    }
+    phase ^= 1u;
+
+    const int64_t N = a.N;
+    const int64_t j = bj * kTile + lane;
+    const int64_t oj = (j < N) ? (a.orig ? (int64_t)a.orig[j] : j) : 0;
+    const double* jb = a.tab + bj * kComp * pm * kTile + lane;
+    for (int rr = 0; rr < kTile / 8; ++rr) {
+      const int li = warp + 8 * rr;
+      const int64_t i = bi * kTile + li;
+      if (i >= N) continue;  // warp-uniform
+      const bool valid = (j < N) && (i < j);
+      const int64_t oi = a.orig ? (int64_t)a.orig[i] : i;
+      const bool sw = valid && oi > oj;  // the reference casts from the lower caller index
+      const int npi = a.np[i];
+      int npj = valid ? a.np[j] : 0;
+      // Two elements whose points all share one normal, bit for bit, have
+      // cos_j = -cos_i exactly at every point pair: K = 0, no rays.
+      if (valid && a.flat[i] && a.flat[j] && a.nrm[3 * i] == a.nrm[3 * j] &&
+          a.nrm[3 * i + 1] == a.nrm[3 * j + 1] && a.nrm[3 * i + 2] == a.nrm[3 * j + 2])
+        npj = 0;
+      const int qmax = __reduce_max_sync(kFull, npj);
+      const double* ib = iblk + li;
+      uint8_t* logp = (a.ray_log && valid)
+                          ? a.ray_log + ((uint64_t)(sw ? oj : oi) * N + (sw ? oi : oj)) * a.log_pm * a.log_pm
+                          : nullptr;
+      double acc = 0.0;
+      int64_t slot = -1;
+      int nst = 0;
+      for (int q = 0; q < qmax; ++q) {
+        const bool lq = q < npj;
+        double xj[3], nj[3], wj;
+        if (lq) {
+          xj[0] = jb[(0 * pm + q) * kTile];
+          xj[1] = jb[(1 * pm + q) * kTile];
+          xj[2] = jb[(2 * pm + q) * kTile];
+          nj[0] = jb[(3 * pm + q) * kTile];
+          nj[1] = jb[(4 * pm + q) * kTile];
+          nj[2] = jb[(5 * pm + q) * kTile];
+          wj = jb[(6 * pm + q) * kTile];
+        } else {
+          xj[0] = xj[1] = xj[2] = 0.0;
+          nj[0] = nj[1] = nj[2] = 0.0;
+          wj = 0.0;
+        }
+        double inner = 0.0;
+        for (int p = 0; p < npi; ++p) {
+          double xi[3], ni[3];
+          xi[0] = ib[(0 * pm + p) * kTile];
+          xi[1] = ib[(1 * pm + p) * kTile];
+          xi[2] = ib[(2 * pm + p) * kTile];
+          ni[0] = ib[(3 * pm + p) * kTile];
+          ni[1] = ib[(4 * pm + p) * kTile];
+          ni[2] = ib[(5 * pm + p) * kTile];
+          const double wi = ib[(6 * pm + p) * kTile];
+          const double rx = xj[0] - xi[0], ry = xj[1] - xi[1], rz = xj[2] - xi[2];
+          const double r2 = (rx * rx + ry * ry) + rz * rz;
+          double K = lq ? k_fast<DIM3>(rx, ry, rz, r2, ni, nj) : 0.0;
+          n_pp += lq ? 1 : 0;
+          if (OCC) {
+            bool cast, defer = false;
+            const NodeD& root = nodes[0];
+            if (DIM3) {
+              RayD R;
+              cast = (K > 0.0) && (sw ? make_ray(xj, -rx, -ry, -rz, r2, R) : make_ray(xi, rx, ry, rz, r2, R));
+              if (cast) defer = slab_d(root, R);
+            } else {
+              cast = K > 0.0;
+              if (cast) {
+                PolD2 pol;
+                pol.a[0] = xi[0]; pol.a[1] = xi[1];
+                pol.b[0] = xj[0]; pol.b[1] = xj[1];
+                defer = pol.node(root) == kHit;
+              }
+            }
+            n_rays += cast ? 1 : 0;
+            if (logp && cast && !defer) logp[sw ? q * a.log_pm + p : p * a.log_pm + q] = 1;
+            slot_alloc(Q, defer && slot < 0, slot, &s_slots);
+            stage_push(stage, nst, defer, rec_make(slot, sw, p, q));
+            if (nst >= 32) stage_flush(stage, nst, 32, Q.rec64, Q.ctr + kCtrRec64, &s_used);
+            if (defer) K = 0.0;
+          }
+          inner = fma(wi, K, inner);
+        }
+        acc = fma(wj, inner, acc);
+      }
+      if (OCC && nst > 0) stage_flush(stage, nst, nst, Q.rec64, Q.ctr + kCtrRec64, &s_used);
+      if (slot >= 0) {
+        PendSlot ps;
+        ps.i = (int32_t)i;
+        ps.j = (int32_t)j;
+        ps.acc = acc;
+        Q.slots[slot] = ps;
+      } else if (valid) {
+        // F[i,j] = raw/A_i and F[j,i] = raw/A_j in the caller's element order
+        a.F[oi + oj * N] = acc / a.area[i];
+        a.F[oj + oi * N] = acc / a.area[j];
+      } else if (j == i) {
+        a.F[oi + oi * N] = 0.0 / a.area[i];
+      }
+    }
+    __syncthreads();
+    if (OCC && threadIdx.x == 0) {  // keep only what the tile used
+      atomicAdd(Q.ctr + kCtrResv, neg(need - s_used));
+      atomicAdd(Q.ctr + kCtrResvS, neg(need_s - s_slots));
+    }
+  }
+  const uint64_t s_rays = warp_sum_u64(n_rays), s_pp = warp_sum_u64(n_pp);
+  if (lane == 0 && a.counters) {
+    atomicAdd(a.counters + 0, s_pp);
+    atomicAdd(a.counters + 1, s_rays);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// 1'. Generation, mixed precision (surfaces).
+// ---------------------------------------------------------------------------
+
+// FP64 point pair of the mixed generation (near field, grazing, or an FP32
+// direction unusable for the certified traversal): the reference's K when
+// exactK, the FP32 term otherwise, and the reference's ray.
+template <bool OCC>
+__device__ __noinline__ void gen_mixed64(const MixedArgs& a, const NodeD* nodes, const double* it64,
+                                         const double* jb64, int p, int q, bool need64, bool exactK_in, bool graze,
+                                         bool sw, double contrib32, uint8_t* logp, bool& defer64, double& accd,
+                                         uint32_t& n_rays, uint32_t& n_rays64, uint32_t& n_graze) {
+  const int pm = a.pmax;
+  double xi[3], ni[3];
+  xi[0] = it64[(0 * pm + p) * kTile]; xi[1] = it64[(1 * pm + p) * kTile]; xi[2] = it64[(2 * pm + p) * kTile];
+  ni[0] = it64[(3 * pm + p) * kTile]; ni[1] = it64[(4 * pm + p) * kTile]; ni[2] = it64[(5 * pm + p) * kTile];
+  const double wi64 = it64[(6 * pm + p) * kTile];
+  double xj[3] = {0.0, 0.0, 0.0}, nj[3] = {0.0, 0.0, 0.0}, wj64 = 0.0;
+  if (need64) {
+    xj[0] = jb64[(0 * pm + q) * kTile]; xj[1] = jb64[(1 * pm + q) * kTile]; xj[2] = jb64[(2 * pm + q) * kTile];
+    nj[0] = jb64[(3 * pm + q) * kTile]; nj[1] = jb64[(4 * pm + q) * kTile]; nj[2] = jb64[(5 * pm + q) * kTile];
+    wj64 = jb64[(6 * pm + q) * kTile];
+  }
+  const double rx64 = xj[0] - xi[0], ry64 = xj[1] - xi[1], rz64 = xj[2] - xi[2];
+  const double r264 = (rx64 * rx64 + ry64 * ry64) + rz64 * rz64;
+  const bool exactK = need64 && exactK_in;
+  const double K64 = exactK ? k_fast<true>(rx64, ry64, rz64, r264, ni, nj) : 0.0;
+  n_graze += (exactK && graze) ? 1 : 0;
+  const double contrib64 = exactK ? wj64 * (wi64 * K64) : contrib32;
+  bool cast64 = false;
+  defer64 = false;
+  if (OCC && need64 && (!exactK || K64 > 0.0)) {
+    RayD R64;
+    cast64 = sw ? make_ray(xj, -rx64, -ry64, -rz64, r264, R64) : make_ray(xi, rx64, ry64, rz64, r264, R64);
+    if (cast64) defer64 = slab_d(nodes[0], R64);
+    if (cast64 && !defer64 && logp) logp[sw ? q * a.log_pm + p : p * a.log_pm + q] = 1;
+  }
+  n_rays64 += cast64 ? 1 : 0;
+  n_rays += (cast64 && exactK) ? 1 : 0;
+  if (need64 && !defer64) accd += contrib64;
+}
+
+template <bool OCC>
+__global__ void __launch_bounds__(256, 2) k_gen_mixed(MixedArgs a) {
+  extern __shared__ __align__(128) unsigned char smem[];
+  const int pm = a.pmax;
+  float* iblk = reinterpret_cast<float*>(smem);
+  NodeF* snodes = reinterpret_cast<NodeF*>(smem + (size_t)kComp * pm * kTile * sizeof(float));
+  uint64_t* stage_all = reinterpret_cast<uint64_t*>(snodes + (a.nodesf_in_smem ? a.n_nodes : 0));
+  uint64_t* bar = stage_all + (OCC ? 8 * 128 : 0);
+  __shared__ int64_t s_tile;
+  __shared__ unsigned long long s_used, s_slots;
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  uint64_t* st64 = stage_all + warp * 128;
+  uint64_t* st32 = st64 + 64;
+  const NodeF* nodesf = a.nodesf;
+  if (OCC && a.nodesf_in_smem) {
+    const int4* src = reinterpret_cast<const int4*>(a.nodesf);
+    int4* dst = reinterpret_cast<int4*>(snodes);
+    for (int k = threadIdx.x; k < a.n_nodes * 2; k += blockDim.x) dst[k] = src[k];
+    nodesf = snodes;
+  }
+  if (threadIdx.x == 0) mbar_init(bar, 1);
+  __syncthreads();
+
+  const WaveQ& Q = a.q;
+  const unsigned long long need = (unsigned long long)kTile * kTile * pm * pm, need_s = kTile * kTile;
+  const uint32_t blk_bytes = (uint32_t)(kComp * pm * kTile * sizeof(float));
+  uint32_t phase = 0;
+  uint32_t n_pp = 0, n_rays = 0, n_rays64 = 0, n_near = 0, n_graze = 0, n_baddir = 0;
+  for (;;) {
+    if (threadIdx.x == 0) {
+      s_tile = claim_tile(Q, a.n_tiles, OCC, need, need_s);
+      s_used = 0;
+      s_slots = 0;
+      if (s_tile >= 0) {
+        int64_t bi, bj;
+        tile_coords(s_tile, a.nT, bi, bj);
+        mbar_expect_tx(bar, blk_bytes);
+        bulk_g2s(iblk, a.tabf + bi * kComp * pm * kTile, blk_bytes, bar);
+      }
+    }
+    __syncthreads();
+    const int64_t t = s_tile;
+    if (t < 0) break;
+    int64_t bi, bj;
+    tile_coords(t, a.nT, bi, bj);
+    const bool ok = mbar_wait_bounded(bar, phase);
+    if (__syncthreads_or(!ok)) {
+      if (threadIdx.x == 0) {
+        atomicOr(a.err, kErrWaitTimeout);
+        if (OCC) {
+          atomicAdd(Q.ctr + kCtrResv, neg(need));
+          atomicAdd(Q.ctr + kCtrResvS, neg(need_s));
+        }
+      }
+      break;
+    }
+    phase ^= 1u;
+
+    const int64_t N = a.N;
+    const int64_t j = bj * kTile + lane;
+    const int64_t oj = (j < N) ? (a.orig ? (int64_t)a.orig[j] : j) : 0;
+    const float* jbf = a.tabf + bj * kComp * pm * kTile + lane;
+    const double* jb64 = a.tab + bj * kComp * pm * kTile + lane;
+    for (int rr = 0; rr < kTile / 8; ++rr) {
+      const int li = warp + 8 * rr;
+      const int64_t i = bi * kTile + li;
+      if (i >= N) continue;  // warp-uniform
+      const bool valid = (j < N) && (i < j);
+      const int64_t oi = a.orig ? (int64_t)a.orig[i] : i;
+      const bool sw = valid && oi > oj;  // rays leave the element with the lower caller index
+      const int npi = a.np[i];
+      int npj = valid ? a.np[j] : 0;
+      if (valid && a.flat[i] && a.flat[j] && a.nrm[3 * i] == a.nrm[3 * j] &&
+          a.nrm[3 * i + 1] == a.nrm[3 * j + 1] && a.nrm[3 * i + 2] == a.nrm[3 * j + 2])
+        npj = 0;
+      const int qmax = __reduce_max_sync(kFull, npj);
+      const double ci0 = a.cen[3 * i], ci1 = a.cen[3 * i + 1], ci2 = a.cen[3 * i + 2];
+      double dc0 = 0.0, dc1 = 0.0, dc2 = 0.0;
+      bool near = false;
+      if (valid) {
+        dc0 = a.cen[3 * j] - ci0; dc1 = a.cen[3 * j + 1] - ci1; dc2 = a.cen[3 * j + 2] - ci2;
+        const double dm = fmax(a.diam[i], a.diam[j]) * a.near_factor;
+        near = (dc0 * dc0 + dc1 * dc1 + dc2 * dc2) < dm * dm;
+      }
+      n_near += (near && npj > 0) ? 1 : 0;
+      const float d0 = (float)dc0, d1 = (float)dc1, d2 = (float)dc2;
+      // FP32 ray origin anchor: the centroid of the casting element
+      const float an0 = (float)(ci0 + (sw ? dc0 : 0.0)), an1 = (float)(ci1 + (sw ? dc1 : 0.0)),
+                  an2 = (float)(ci2 + (sw ? dc2 : 0.0));
+      const float* ibf = iblk + li;
+      const double* it64 = a.tab + bi * kComp * pm * kTile + li;
+      uint8_t* logp = (a.ray_log && valid)
+                          ? a.ray_log + ((uint64_t)(sw ? oj : oi) * N + (sw ? oi : oj)) * a.log_pm * a.log_pm
+                          : nullptr;
+      double accd = 0.0;   // FP64 terms
+      float acc32 = 0.0f;  // FP32 far-field terms
+      int64_t slot = -1;
+      int n64 = 0, n32 = 0;
+      for (int q = 0; q < qmax; ++q) {
+        const bool lq = q < npj;
+        const bool far = lq && !near;
+        float oq0 = 0.f, oq1 = 0.f, oq2 = 0.f, nq0 = 0.f, nq1 = 0.f, nq2 = 0.f, wq = 0.f;
+        if (far) {
+          oq0 = jbf[(0 * pm + q) * kTile]; oq1 = jbf[(1 * pm + q) * kTile]; oq2 = jbf[(2 * pm + q) * kTile];
+          nq0 = jbf[(3 * pm + q) * kTile]; nq1 = jbf[(4 * pm + q) * kTile]; nq2 = jbf[(5 * pm + q) * kTile];
+          wq = jbf[(6 * pm + q) * kTile];
+        }
+        float inner = 0.0f;
+        for (int p = 0; p < npi; ++p) {
+          const float op0 = ibf[(0 * pm + p) * kTile], op1 = ibf[(1 * pm + p) * kTile], op2 = ibf[(2 * pm + p) * kTile];
+          const float np0 = ibf[(3 * pm + p) * kTile], np1 = ibf[(4 * pm + p) * kTile], np2 = ibf[(5 * pm + p) * kTile];
+          const float wp = ibf[(6 * pm + p) * kTile];
+          const float rx = d0 + (oq0 - op0), ry = d1 + (oq1 - op1), rz = d2 + (oq2 - op2);
+          const float r2 = fmaf(rx, rx, fmaf(ry, ry, rz * rz));
+          const float di = fmaf(np0, rx, fmaf(np1, ry, np2 * rz));
+          const float dj = -fmaf(nq0, rx, fmaf(nq1, ry, nq2 * rz));
+          const bool graze = far && (di * di <= 1e-10f * r2 || dj * dj <= 1e-10f * r2 || r2 < 1e-18f);
+          float K32 = 0.0f;
+          if (far && !graze && di > 0.0f && dj > 0.0f) K32 = (di * dj) * rcp_approx(3.14159265f * (r2 * r2));
+          const bool cast32 = far && !graze && K32 > 0.0f;
+          bool badray = false, defer32 = false;
+          n_pp += lq ? 1 : 0;
+          if (OCC && cast32) {
+            RayF R;
+            const float xo[3] = {an0 + (sw ? oq0 : op0), an1 + (sw ? oq1 : op1), an2 + (sw ? oq2 : op2)};
+            const bool rok =
+                sw ? make_ray_f(xo, -rx, -ry, -rz, r2, a.delta, R) : make_ray_f(xo, rx, ry, rz, r2, a.delta, R);
+            badray = !rok;
+            if (rok) {
+              defer32 = slab_f(nodesf[0], R) != kMiss;
+              if (!defer32 && logp) logp[sw ? q * a.log_pm + p : p * a.log_pm + q] = 1;
+            }
+          }
+          n_rays += cast32 ? 1 : 0;
+          n_baddir += badray ? 1 : 0;
+          // FP64: near field, grazing point pairs, unusable FP32 directions
+          const bool need64 = lq && (near || graze || badray);
+          bool defer64 = false;
+          if (__any_sync(kFull, need64))
+            gen_mixed64<OCC>(a, a.nodes, it64, jb64, p, q, need64, near || graze, graze, sw,
+                             (double)(wq * (wp * K32)), logp, defer64, accd, n_rays, n_rays64, n_graze);
+          if (OCC) {
+            slot_alloc(Q, (defer32 || defer64) && slot < 0, slot, &s_slots);
+            stage_push(st64, n64, defer64, rec_make(slot, sw, p, q));
+            if (n64 >= 32) stage_flush(st64, n64, 32, Q.rec64, Q.ctr + kCtrRec64, &s_used);
+            stage_push(st32, n32, defer32, rec_make(slot, sw, p, q));
+            if (n32 >= 32) stage_flush(st32, n32, 32, Q.rec32, Q.ctr + kCtrRec32, &s_used);
+          }
+          if (far && !graze && !badray && !defer32) inner = fmaf(wp, K32, inner);
+        }
+        acc32 = fmaf(wq, inner, acc32);
+      }
+      if (OCC) {
+        if (n64 > 0) stage_flush(st64, n64, n64, Q.rec64, Q.ctr + kCtrRec64, &s_used);
+        if (n32 > 0) stage_flush(st32, n32, n32, Q.rec32, Q.ctr + kCtrRec32, &s_used);
+      }
+      const double raw = accd + (double)acc32;
+      if (slot >= 0) {
+        PendSlot ps;
+        ps.i = (int32_t)i;
+        ps.j = (int32_t)j;
+        ps.acc = raw;
+        Q.slots[slot] = ps;
+      } else if (valid) {
+        a.F[oi + oj * N] = raw / a.area[i];
+        a.F[oj + oi * N] = raw / a.area[j];
+      } else if (j == i) {
+        a.F[oi + oi * N] = 0.0 / a.area[i];
+      }
+    }
+    __syncthreads();
+    if (OCC && threadIdx.x == 0) {
+      atomicAdd(Q.ctr + kCtrResv, neg(need - s_used));
+      atomicAdd(Q.ctr + kCtrResvS, neg(need_s - s_slots));
+    }
+  }
+  const uint64_t s_pp = warp_sum_u64(n_pp), s_rays = warp_sum_u64(n_rays), s_r64 = warp_sum_u64(n_rays64),
+                 s_near = warp_sum_u64(n_near), s_graze = warp_sum_u64(n_graze), s_bad = warp_sum_u64(n_baddir);
+  if (lane == 0 && a.counters) {
+    atomicAdd(a.counters + 0, s_pp);
+    atomicAdd(a.counters + 1, s_rays);
+    atomicAdd(a.counters + 4, s_r64);
+    atomicAdd(a.counters + 5, s_near);
+    atomicAdd(a.counters + 6, s_graze);
+    atomicAdd(a.counters + 10, s_bad);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// 2. Traversal kernels.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void log_ray(const TraceArgs& a, int64_t i, int64_t j, bool sw, int p, int q, uint8_t v) {
+  const int64_t oi = a.orig ? (int64_t)a.orig[i] : i, oj = a.orig ? (int64_t)a.orig[j] : j;
+  uint8_t* lp = a.ray_log + ((uint64_t)(sw ? oj : oi) * a.N + (sw ? oi : oj)) * a.log_pm * a.log_pm;
+  lp[sw ? q * a.log_pm + p : p * a.log_pm + q] = v;
+}
+
+__device__ __forceinline__ void set_visible(const WaveQ& Q, int64_t slot, int pm, int p, int q) {
+  const int b = p * pm + q;
+  atomicOr(reinterpret_cast<unsigned long long*>(Q.vis + slot * Q.vis_words + (b >> 6)), 1ull << (b & 63));
+}
+
+template <bool DIM3>
+__global__ void __launch_bounds__(256, 3) k_trace64(TraceArgs a) {
+  extern __shared__ __align__(128) unsigned char smem[];
+  NodeD* snodes = reinterpret_cast<NodeD*>(smem);
+  RayBank* wsa = reinterpret_cast<RayBank*>(snodes + (a.nodes_in_smem ? a.n_nodes : 0));
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  RayBank& ws = wsa[warp];
+  const NodeD* nodes = a.nodes;
+  if (a.nodes_in_smem) {
+    const int4* src = reinterpret_cast<const int4*>(a.nodes);
+    int4* dst = reinterpret_cast<int4*>(snodes);
+    for (int k = threadIdx.x; k < a.n_nodes * 4; k += blockDim.x) dst[k] = src[k];
+    nodes = snodes;
+  }
+  __syncthreads();
+  const WaveQ& Q = a.q;
+  const int pm = a.pmax;
+  const unsigned long long n = *(volatile unsigned long long*)(Q.ctr + kCtrRec64);
+  TravCount tc;
+  for (;;) {
+    unsigned long long base = 0;
+    if (lane == 0) base = atomicAdd(Q.ctr + kCtrHead64, 32ull);
+    base = __shfl_sync(kFull, base, 0);
+    if (base >= n) break;
+    const bool have = base + lane < n;
+    const uint64_t r = have ? Q.rec64[base + lane] : 0ull;
+    const int64_t slot = rec_slot(r);
+    const bool sw = rec_sw(r);
+    const int p = rec_p(r), q = rec_q(r);
+    int64_t i = 0, j = 0;
+    if (have) {
+      const PendSlot ps = Q.slots[slot];
+      i = ps.i;
+      j = ps.j;
+    }
+    double xi[3], xj[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      xi[c] = have ? a.tab[tab_at(i, c, p, pm)] : 0.0;
+      xj[c] = have ? a.tab[tab_at(j, c, q, pm)] : 0.0;
+    }
+    const int32_t gi = have ? a.group[i] : 0, gj = have ? a.group[j] : 0;
+    int res;
+    if (DIM3) {
+      PolD3 pol;
+      pol.tris = a.tris;
+      const double rx = xj[0] - xi[0], ry = xj[1] - xi[1], rz = xj[2] - xi[2];
+      const double r2 = (rx * rx + ry * ry) + rz * rz;
+      if (have) {
+        if (sw) make_ray(xj, -rx, -ry, -rz, r2, pol.R);
+        else make_ray(xi, rx, ry, rz, r2, pol.R);
+        pol.store(ws, lane, gi, gj);
+      }
+      res = trace_batch(have, nodes, a.n_nodes, ws, pol, tc);
+    } else {
+      PolD2 pol;
+      pol.segs = a.segs;
+      pol.a[0] = sw ? xj[0] : xi[0];
+      pol.a[1] = sw ? xj[1] : xi[1];
+      pol.b[0] = sw ? xi[0] : xj[0];
+      pol.b[1] = sw ? xi[1] : xj[1];
+      if (have) pol.store(ws, lane, gi, gj);
+      res = trace_batch(have, nodes, a.n_nodes, ws, pol, tc);
+    }
+    if (have && res != kHit) set_visible(Q, slot, pm, p, q);
+    if (have && a.ray_log) log_ray(a, i, j, sw, p, q, res == kHit ? 2 : 1);
+  }
+  const uint64_t s_nodes = warp_sum_u64(tc.nodes), s_prims = warp_sum_u64(tc.prims);
+  if (lane == 0 && a.counters) {
+    atomicAdd(a.counters + 2, s_nodes);
+    atomicAdd(a.counters + 3, s_prims);
+  }
+}
+
+__global__ void __launch_bounds__(256, 4) k_trace32(TraceArgs a) {
+  extern __shared__ __align__(128) unsigned char smem[];
+  NodeF* snodes = reinterpret_cast<NodeF*>(smem);
+  RayBank* wsa = reinterpret_cast<RayBank*>(snodes + (a.nodes_in_smem ? a.n_nodes : 0));
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  RayBank& ws = wsa[warp];
+  const NodeF* nodesf = a.nodesf;
+  if (a.nodes_in_smem) {
+    const int4* src = reinterpret_cast<const int4*>(a.nodesf);
+    int4* dst = reinterpret_cast<int4*>(snodes);
+    for (int k = threadIdx.x; k < a.n_nodes * 2; k += blockDim.x) dst[k] = src[k];
+    nodesf = snodes;
+  }
+  __syncthreads();
+  const WaveQ& Q = a.q;
+  const int pm = a.pmax;
+  const unsigned long long n = *(volatile unsigned long long*)(Q.ctr + kCtrRec32);
+  TravCount tc;
+  uint32_t n_unsure = 0;
+  for (;;) {
+    unsigned long long base = 0;
+    if (lane == 0) base = atomicAdd(Q.ctr + kCtrHead32, 32ull);
+    base = __shfl_sync(kFull, base, 0);
+    if (base >= n) break;
+    const bool have = base + lane < n;
+    const uint64_t r = have ? Q.rec32[base + lane] : 0ull;
+    const int64_t slot = rec_slot(r);
+    const bool sw = rec_sw(r);
+    const int p = rec_p(r), q = rec_q(r);
+    int64_t i = 0, j = 0;
+    if (have) {
+      const PendSlot ps = Q.slots[slot];
+      i = ps.i;
+      j = ps.j;
+    }
+    PolF3 pol;
+    pol.tris = a.trisf;
+    if (have) {
+      // the generation's FP32 ray, operation for operation
+      const double ci0 = a.cen[3 * i], ci1 = a.cen[3 * i + 1], ci2 = a.cen[3 * i + 2];
+      const double dc0 = a.cen[3 * j] - ci0, dc1 = a.cen[3 * j + 1] - ci1, dc2 = a.cen[3 * j + 2] - ci2;
+      const float d0 = (float)dc0, d1 = (float)dc1, d2 = (float)dc2;
+      const float an0 = (float)(ci0 + (sw ? dc0 : 0.0)), an1 = (float)(ci1 + (sw ? dc1 : 0.0)),
+                  an2 = (float)(ci2 + (sw ? dc2 : 0.0));
+      const float op0 = a.tabf[tab_at(i, 0, p, pm)], op1 = a.tabf[tab_at(i, 1, p, pm)], op2 = a.tabf[tab_at(i, 2, p, pm)];
+      const float oq0 = a.tabf[tab_at(j, 0, q, pm)], oq1 = a.tabf[tab_at(j, 1, q, pm)], oq2 = a.tabf[tab_at(j, 2, q, pm)];
+      const float rx = d0 + (oq0 - op0), ry = d1 + (oq1 - op1), rz = d2 + (oq2 - op2);
+      const float r2 = fmaf(rx, rx, fmaf(ry, ry, rz * rz));
+      const float xo[3] = {an0 + (sw ? oq0 : op0), an1 + (sw ? oq1 : op1), an2 + (sw ? oq2 : op2)};
+      if (sw) make_ray_f(xo, -rx, -ry, -rz, r2, a.delta, pol.R);
+      else make_ray_f(xo, rx, ry, rz, r2, a.delta, pol.R);
+      pol.store(ws, lane, a.group[i], a.group[j]);
+    }
+    const int res = trace_batch(have, nodesf, a.n_nodes, ws, pol, tc);
+    if (have && res == kMiss) set_visible(Q, slot, pm, p, q);
+    if (have && a.ray_log && res != kUnsure) log_ray(a, i, j, sw, p, q, res == kHit ? 2 : 1);
+    // uncertain rays go to the FP64 queue
+    const bool uns = have && res == kUnsure;
+    const uint32_t m = __ballot_sync(kFull, uns);
+    if (m) {
+      unsigned long long b64 = 0;
+      if (lane == 0) b64 = atomicAdd(Q.ctr + kCtrRec64, (unsigned long long)__popc(m));
+      b64 = __shfl_sync(kFull, b64, 0);
+      if (uns) Q.rec64[b64 + __popc(m & lanemask_lt())] = r;
+    }
+    n_unsure += uns ? 1 : 0;
+  }
+  const uint64_t s_nodes = warp_sum_u64(tc.nodes), s_prims = warp_sum_u64(tc.prims),
+                 s_us = warp_sum_u64(tc.unsure_slab), s_up = warp_sum_u64(tc.unsure_prim),
+                 s_un = warp_sum_u64(n_unsure);
+  if (lane == 0 && a.counters) {
+    atomicAdd(a.counters + 2, s_nodes);
+    atomicAdd(a.counters + 3, s_prims);
+    atomicAdd(a.counters + 4, s_un);
+    atomicAdd(a.counters + 7, s_un);
+    atomicAdd(a.counters + 8, s_us);
+    atomicAdd(a.counters + 9, s_up);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// 3. Resolve: one thread per pending pair.
+// ---------------------------------------------------------------------------
+template <bool DIM3>
+__global__ void __launch_bounds__(256) k_resolve64(ResolveArgs a) {
+  const WaveQ& Q = a.q;
+  const unsigned long long ns = *(volatile unsigned long long*)(Q.ctr + kCtrSlots);
+  const int pm = a.pmax;
+  for (unsigned long long s = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; s < ns;
+       s += (unsigned long long)gridDim.x * blockDim.x) {
+    const PendSlot ps = Q.slots[s];
+    const int64_t i = ps.i, j = ps.j;
+    double raw = ps.acc;
+    for (int w = 0; w < Q.vis_words; ++w) {
+      unsigned long long bits = Q.vis[s * Q.vis_words + w];
+      while (bits) {
+        const int b = w * 64 + (__ffsll((long long)bits) - 1);
+        bits &= bits - 1ull;
+        const int p = b / pm, q = b - p * pm;
+        double xi[3], ni[3], xj[3], nj[3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          xi[c] = a.tab[tab_at(i, c, p, pm)];
+          ni[c] = a.tab[tab_at(i, 3 + c, p, pm)];
+          xj[c] = a.tab[tab_at(j, c, q, pm)];
+          nj[c] = a.tab[tab_at(j, 3 + c, q, pm)];
+        }
+        const double wi = a.tab[tab_at(i, 6, p, pm)], wj = a.tab[tab_at(j, 6, q, pm)];
+        const double rx = xj[0] - xi[0], ry = xj[1] - xi[1], rz = xj[2] - xi[2];
+        const double r2 = (rx * rx + ry * ry) + rz * rz;
+        const double K = k_fast<DIM3>(rx, ry, rz, r2, ni, nj);
+        raw += wj * (wi * K);
+      }
+    }
+    const int64_t oi = a.orig ? (int64_t)a.orig[i] : i, oj = a.orig ? (int64_t)a.orig[j] : j;
+    a.F[oi + oj * a.N] = raw / a.area[i];
+    a.F[oj + oi * a.N] = raw / a.area[j];
+  }
+}
+
+__global__ void __launch_bounds__(256) k_resolve_mixed(ResolveArgs a) {
+  const WaveQ& Q = a.q;
+  const unsigned long long ns = *(volatile unsigned long long*)(Q.ctr + kCtrSlots);
+  const int pm = a.pmax;
+  for (unsigned long long s = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; s < ns;
+       s += (unsigned long long)gridDim.x * blockDim.x) {
+    const PendSlot ps = Q.slots[s];
+    const int64_t i = ps.i, j = ps.j;
+    double raw = ps.acc;
+    // the generation's near-field and FP32 quantities, operation for operation
+    const double ci0 = a.cen[3 * i], ci1 = a.cen[3 * i + 1], ci2 = a.cen[3 * i + 2];
+    const double dc0 = a.cen[3 * j] - ci0, dc1 = a.cen[3 * j + 1] - ci1, dc2 = a.cen[3 * j + 2] - ci2;
+    const double dm = fmax(a.diam[i], a.diam[j]) * a.near_factor;
+    const bool near = (dc0 * dc0 + dc1 * dc1 + dc2 * dc2) < dm * dm;
+    const float d0 = (float)dc0, d1 = (float)dc1, d2 = (float)dc2;
+    for (int w = 0; w < Q.vis_words; ++w) {
+      unsigned long long bits = Q.vis[s * Q.vis_words + w];
+      while (bits) {
+        const int b = w * 64 + (__ffsll((long long)bits) - 1);
+        bits &= bits - 1ull;
+        const int p = b / pm, q = b - p * pm;
+        bool exact = near;
+        double c = 0.0;
+        if (!near) {
+          const float op0 = a.tabf[tab_at(i, 0, p, pm)], op1 = a.tabf[tab_at(i, 1, p, pm)], op2 = a.tabf[tab_at(i, 2, p, pm)];
+          const float np0 = a.tabf[tab_at(i, 3, p, pm)], np1 = a.tabf[tab_at(i, 4, p, pm)], np2 = a.tabf[tab_at(i, 5, p, pm)];
+          const float wp = a.tabf[tab_at(i, 6, p, pm)];
+          const float oq0 = a.tabf[tab_at(j, 0, q, pm)], oq1 = a.tabf[tab_at(j, 1, q, pm)], oq2 = a.tabf[tab_at(j, 2, q, pm)];
+          const float nq0 = a.tabf[tab_at(j, 3, q, pm)], nq1 = a.tabf[tab_at(j, 4, q, pm)], nq2 = a.tabf[tab_at(j, 5, q, pm)];
+          const float wq = a.tabf[tab_at(j, 6, q, pm)];
+          const float rx = d0 + (oq0 - op0), ry = d1 + (oq1 - op1), rz = d2 + (oq2 - op2);
+          const float r2 = fmaf(rx, rx, fmaf(ry, ry, rz * rz));
+          const float di = fmaf(np0, rx, fmaf(np1, ry, np2 * rz));
+          const float dj = -fmaf(nq0, rx, fmaf(nq1, ry, nq2 * rz));
+          const bool graze = (di * di <= 1e-10f * r2 || dj * dj <= 1e-10f * r2 || r2 < 1e-18f);
+          if (graze) {
+            exact = true;
+          } else {
+            float K32 = 0.0f;
+            if (di > 0.0f && dj > 0.0f) K32 = (di * dj) * rcp_approx(3.14159265f * (r2 * r2));
+            c = (double)(wq * (wp * K32));
+          }
+        }
+        if (exact) {
+          double xi[3], ni[3], xj[3], nj[3];
+#pragma unroll
+          for (int k = 0; k < 3; ++k) {
+            xi[k] = a.tab[tab_at(i, k, p, pm)];
+            ni[k] = a.tab[tab_at(i, 3 + k, p, pm)];
+            xj[k] = a.tab[tab_at(j, k, q, pm)];
+            nj[k] = a.tab[tab_at(j, 3 + k, q, pm)];
+          }
+          const double wi = a.tab[tab_at(i, 6, p, pm)], wj = a.tab[tab_at(j, 6, q, pm)];
+          const double rx = xj[0] - xi[0], ry = xj[1] - xi[1], rz = xj[2] - xi[2];
+          const double r2 = (rx * rx + ry * ry) + rz * rz;
+          c = wj * (wi * k_fast<true>(rx, ry, rz, r2, ni, nj));
+        }
+        raw += c;
+      }
+    }
+    const int64_t oi = a.orig ? (int64_t)a.orig[i] : i, oj = a.orig ? (int64_t)a.orig[j] : j;
+    a.F[oi + oj * a.N] = raw / a.area[i];
+    a.F[oj + oi * a.N] = raw / a.area[j];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// host launchers
+// ---------------------------------------------------------------------------
+size_t gen_smem_bytes(bool mixed, int pmax, int n_nodes_smem, bool occ) {
+  const size_t tab = (size_t)kComp * pmax * kTile * (mixed ? sizeof(float) : sizeof(double));
+  const size_t nodes = (size_t)n_nodes_smem * (mixed ? sizeof(NodeF) : sizeof(NodeD));
+  const size_t stage = occ ? (size_t)8 * (mixed ? 128 : 64) * sizeof(uint64_t) : 0;
+  return tab + nodes + stage + 16;
+}
+
+size_t trace_smem_bytes(bool fp32, int n_nodes_smem) {
+  return (size_t)n_nodes_smem * (fp32 ? sizeof(NodeF) : sizeof(NodeD)) + 8 * sizeof(RayBank);
+}
+
+template <typename F>
+static cudaError_t set_smem(F fn, size_t smem) {
+  return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+}
+
+template <typename F>
+static int grid_for(F fn, size_t smem, int sm_count, int cap) {
+  int per_sm = 1;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 256, smem) != cudaSuccess || per_sm < 1) per_sm = 1;
+  if (per_sm > cap) per_sm = cap;
+  return sm_count * per_sm;
+}
+
+cudaError_t launch_gen_fp64(const PairArgs& a, int sm_count, cudaStream_t st) {
+  const bool occ = a.n_nodes > 0;
+  const size_t smem = gen_smem_bytes(false, a.pmax, a.nodes_in_smem ? a.n_nodes : 0, occ);
+  auto launch = [&](auto fn) -> cudaError_t {
+    cudaError_t e = set_smem(fn, smem);
+    if (e != cudaSuccess) return e;
+    int64_t grid = grid_for(fn, smem, sm_count, 4);
+    if (grid > a.n_tiles) grid = a.n_tiles;
+    if (grid < 1) grid = 1;
+    fn<<<(unsigned)grid, 256, smem, st>>>(a);
+    return cudaGetLastError();
+  };
+  if (a.dim3) return occ ? launch(k_gen_fp64<true, true>) : launch(k_gen_fp64<true, false>);
+  return occ ? launch(k_gen_fp64<false, true>) : launch(k_gen_fp64<false, false>);
+}
+
+cudaError_t launch_gen_mixed(const MixedArgs& a, int sm_count, cudaStream_t st) {
+  const bool occ = a.n_nodes > 0;
+  const size_t smem = gen_smem_bytes(true, a.pmax, a.nodesf_in_smem ? a.n_nodes : 0, occ);
+  auto launch = [&](auto fn) -> cudaError_t {
+    cudaError_t e = set_smem(fn, smem);
+    if (e != cudaSuccess) return e;
+    int64_t grid = grid_for(fn, smem, sm_count, 4);
+    if (grid > a.n_tiles) grid = a.n_tiles;
+    if (grid < 1) grid = 1;
+    fn<<<(unsigned)grid, 256, smem, st>>>(a);
+    return cudaGetLastError();
+  };
+  return occ ? launch(k_gen_mixed<true>) : launch(k_gen_mixed<false>);
+}
+
+cudaError_t launch_trace(const TraceArgs& a, bool fp32, int sm_count, cudaStream_t st) {
+  const size_t smem = trace_smem_bytes(fp32, a.nodes_in_smem ? a.n_nodes : 0);
+  auto launch = [&](auto fn) -> cudaError_t {
+    cudaError_t e = set_smem(fn, smem);
+    if (e != cudaSuccess) return e;
+    const int grid = grid_for(fn, smem, sm_count, 8);
+    fn<<<(unsigned)grid, 256, smem, st>>>(a);
+    return cudaGetLastError();
+  };
+  if (fp32) return launch(k_trace32);
+  return a.dim3 ? launch(k_trace64<true>) : launch(k_trace64<false>);
+}
+
+cudaError_t launch_resolve(const ResolveArgs& a, bool mixed, int sm_count, cudaStream_t st) {
+  const int grid = sm_count * 8;
+  if (mixed) k_resolve_mixed<<<grid, 256, 0, st>>>(a);
+  else if (a.dim3) k_resolve64<true><<<grid, 256, 0, st>>>(a);
+  else k_resolve64<false><<<grid, 256, 0, st>>>(a);
+  return cudaGetLastError();
+}
+
+}  // namespace rvf

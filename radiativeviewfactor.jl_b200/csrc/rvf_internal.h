@@ -61,6 +61,8 @@ struct rvf_session {
   rvf::DevBuf err;           // int
   rvf::DevBuf tile_counter;  // u64
   rvf::DevBuf counters;      // u64 x 8
+  // wavefront pair pipeline (kernels_wave.cu)
+  rvf::DevBuf wq_ctr, wq_rec64, wq_rec32, wq_slots, wq_vis;
   std::set<rvf_mesh*> meshes;
   cudaEvent_t ev[8] = {};
 };

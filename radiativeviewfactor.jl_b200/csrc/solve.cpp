@@ -93,6 +93,54 @@ int run_reduce(Session* s, rvf_mesh* m, const double* area) {
   return e == cudaSuccess ? RVF_OK : cuda_err(e, "reduction kernels");
 }
 
+// Ray queues of the wavefront pipeline, kept by the session and grown on
+// demand.  Capacity: every point pair of every tile when that is small,
+// otherwise up to 2^29 records per queue (4 GiB) within the HBM budget, and
+// never below a few tiles' worst case.
+int ensure_wave(Session* s, bool two_queues, bool occ, int pmax, int64_t n_tiles, WaveQ& q) {
+  int rc = 0;
+  if (!s->wq_ctr.ptr && (rc = s->wq_ctr.alloc(s, sizeof(unsigned long long) * kCtrCount))) return rc;
+  q = WaveQ{};
+  q.ctr = s->wq_ctr.as<unsigned long long>();
+  q.vis_words = (pmax * pmax + 63) / 64;
+  if (!occ) return 0;
+  const int64_t per_tile = (int64_t)kTile * kTile * pmax * pmax;
+  const int64_t want = std::min<int64_t>(n_tiles * per_tile, (int64_t)1 << 29);
+  const int64_t floor_recs = std::min<int64_t>(n_tiles * per_tile, 4 * per_tile);
+  const int64_t want_s = std::min<int64_t>(n_tiles * kTile * kTile, (int64_t)1 << 25);
+  const int64_t floor_s = std::min<int64_t>(n_tiles * kTile * kTile, 4 * kTile * kTile);
+  const int nq = two_queues ? 2 : 1;
+  const size_t slot_bytes = sizeof(PendSlot) + sizeof(unsigned long long) * q.vis_words;
+  auto have = [&](int64_t recs, int64_t slots) {
+    return s->wq_rec64.bytes >= sizeof(uint64_t) * recs && (!two_queues || s->wq_rec32.bytes >= sizeof(uint64_t) * recs) &&
+           s->wq_slots.bytes >= sizeof(PendSlot) * slots &&
+           s->wq_vis.bytes >= sizeof(unsigned long long) * q.vis_words * slots;
+  };
+  int64_t recs = want, slots = want_s;
+  if (!have(recs, slots)) {
+    // release and size against the budget left
+    s->wq_rec64.free_(); s->wq_rec32.free_(); s->wq_slots.free_(); s->wq_vis.free_();
+    const size_t left = s->budget > s->used ? s->budget - s->used : 0;
+    while ((size_t)(recs * 8 * nq) + (size_t)slots * slot_bytes > left / 2 && (recs > floor_recs || slots > floor_s)) {
+      recs = std::max<int64_t>(floor_recs, recs / 2);
+      slots = std::max<int64_t>(floor_s, slots / 2);
+    }
+    if ((rc = s->wq_rec64.alloc(s, sizeof(uint64_t) * recs))) return rc;
+    if (two_queues && (rc = s->wq_rec32.alloc(s, sizeof(uint64_t) * recs))) return rc;
+    if ((rc = s->wq_slots.alloc(s, sizeof(PendSlot) * slots))) return rc;
+    if ((rc = s->wq_vis.alloc(s, sizeof(unsigned long long) * q.vis_words * slots))) return rc;
+  }
+  q.rec64 = s->wq_rec64.as<uint64_t>();
+  q.rec32 = two_queues ? s->wq_rec32.as<uint64_t>() : nullptr;
+  q.cap = (int64_t)(s->wq_rec64.bytes / sizeof(uint64_t));
+  if (two_queues) q.cap = std::min<int64_t>(q.cap, (int64_t)(s->wq_rec32.bytes / sizeof(uint64_t)));
+  q.slots = s->wq_slots.as<PendSlot>();
+  q.vis = s->wq_vis.as<unsigned long long>();
+  q.scap = std::min<int64_t>((int64_t)(s->wq_slots.bytes / sizeof(PendSlot)),
+                             (int64_t)(s->wq_vis.bytes / (sizeof(unsigned long long) * q.vis_words)));
+  return 0;
+}
+
 // Quad8 pairs that share corner nodes, in the reference's classification
 // (singularity_type, src/DuffyKernel.jl:95-115): corners 1-4 compared by node
 // index, ci outer / cj inner, the first two matches kept.
@@ -237,6 +285,7 @@ int rvf_session_destroy(rvf_session* s) {
     s->err.free_();
     s->tile_counter.free_();
     s->counters.free_();
+    s->wq_ctr.free_(); s->wq_rec64.free_(); s->wq_rec32.free_(); s->wq_slots.free_(); s->wq_vis.free_();
     cudaStreamDestroy(s->stream);
   }
   delete s;
@@ -376,8 +425,8 @@ int rvf_solve(rvf_session* s, rvf_mesh* m, const rvf_options* o, double* F_elem,
   a.F = m->F.as<double>();
   a.nodes = occ ? m->nodes.as<NodeD>() : nullptr;
   a.n_nodes = occ ? m->n_nodes : 0;
-  const size_t base_smem = pair_smem_bytes(T->pmax, 0);
-  a.nodes_in_smem = occ && (base_smem + sizeof(NodeD) * (size_t)m->n_nodes <= std::min<size_t>(s->smem_optin, 96 * 1024));
+  const size_t smem_cap = std::min<size_t>(s->smem_optin, 110 * 1024);
+  a.nodes_in_smem = occ && gen_smem_bytes(false, T->pmax, m->n_nodes, occ) <= smem_cap;
   a.tris = occ ? (o->geometric_soup ? m->tris_geo.as<TriD>() : m->tris_ref.as<TriD>()) : nullptr;
   a.segs = occ ? m->segs.as<SegD>() : nullptr;
   a.tile_counter = s->tile_counter.as<unsigned long long>();
@@ -405,7 +454,7 @@ int rvf_solve(rvf_session* s, rvf_mesh* m, const rvf_options* o, double* F_elem,
       x.group = a.group; x.orig = a.orig; x.F = a.F;
       x.nodes = a.nodes; x.n_nodes = a.n_nodes;
       x.nodesf = occ ? m->nodesf.as<NodeF>() : nullptr;
-      x.nodesf_in_smem = occ && (mixed_smem_bytes(T->pmax, m->n_nodes) <= std::min<size_t>(s->smem_optin, 96 * 1024));
+      x.nodesf_in_smem = occ && gen_smem_bytes(true, T->pmax, m->n_nodes, occ) <= smem_cap;
       x.tris = a.tris;
       x.trisf = occ ? (o->geometric_soup ? m->trisf_geo.as<TriF>() : m->trisf_ref.as<TriF>()) : nullptr;
       x.delta = (float)std::ldexp(m->extent, -20);
@@ -413,9 +462,49 @@ int rvf_solve(rvf_session* s, rvf_mesh* m, const rvf_options* o, double* F_elem,
       x.ray_log = a.ray_log; x.log_pm = a.log_pm;
     }
     EvTimer t(s->stream);
-    e = mixed ? launch_pairs_mixed(x, s->sm_count, s->stream) : launch_pairs_fp64(a, s->sm_count, s->stream);
-    n_kernels += 1;
-    if (e != cudaSuccess) return cuda_err(e, "pair kernel launch");
+    WaveQ wq{};
+    if ((rc = ensure_wave(s, mixed && occ, occ, T->pmax, a.n_tiles, wq))) return rc;
+    a.q = wq;
+    x.q = wq;
+    TraceArgs ta{};
+    ResolveArgs ra{};
+    if (occ) {
+      ta.N = N; ta.pmax = a.pmax; ta.dim3 = a.dim3; ta.tab = a.tab; ta.tabf = x.tabf; ta.cen = T->cen.as<double>();
+      ta.group = a.group; ta.orig = a.orig; ta.nodes = a.nodes; ta.nodesf = x.nodesf; ta.n_nodes = a.n_nodes;
+      ta.tris = a.tris; ta.trisf = x.trisf; ta.segs = a.segs; ta.delta = x.delta; ta.q = wq;
+      ta.counters = a.counters; ta.ray_log = a.ray_log; ta.log_pm = a.log_pm;
+      ra.N = N; ra.pmax = a.pmax; ra.dim3 = a.dim3; ra.tab = a.tab; ra.tabf = x.tabf; ra.cen = T->cen.as<double>();
+      ra.diam = T->diam.as<double>(); ra.near_factor = o->near_field_factor; ra.area = a.area; ra.orig = a.orig;
+      ra.F = a.F; ra.q = wq;
+    }
+    cudaMemsetAsync(wq.ctr, 0, sizeof(unsigned long long) * kCtrCount, s->stream);
+    // chunks: each claims tiles while its queues have room, then traces and resolves them
+    unsigned long long prev = 0;
+    for (int chunk = 0;; ++chunk) {
+      e = mixed ? launch_gen_mixed(x, s->sm_count, s->stream) : launch_gen_fp64(a, s->sm_count, s->stream);
+      n_kernels += 1;
+      if (e != cudaSuccess) return cuda_err(e, "pair generation kernel launch");
+      if (!occ) break;  // without rays one launch integrates every tile
+      if (mixed) {
+        ta.nodes_in_smem = trace_smem_bytes(true, m->n_nodes) <= 72 * 1024;
+        if ((e = launch_trace(ta, true, s->sm_count, s->stream)) != cudaSuccess) return cuda_err(e, "FP32 trace launch");
+        n_kernels += 1;
+      }
+      ta.nodes_in_smem = trace_smem_bytes(false, m->n_nodes) <= 72 * 1024;
+      if ((e = launch_trace(ta, false, s->sm_count, s->stream)) != cudaSuccess) return cuda_err(e, "trace launch");
+      if ((e = launch_resolve(ra, mixed, s->sm_count, s->stream)) != cudaSuccess) return cuda_err(e, "resolve launch");
+      n_kernels += 2;
+      unsigned long long claimed = 0;
+      e = cudaMemcpyAsync(&claimed, wq.ctr + kCtrTile, sizeof claimed, cudaMemcpyDeviceToHost, s->stream);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+      if (e != cudaSuccess) return cuda_err(e, "pair pipeline");
+      if ((rc = read_err(s))) return rc;
+      if (claimed >= (unsigned long long)a.n_tiles) break;
+      if (claimed == prev) return set_err(RVF_ENOMEM, "pair pipeline made no progress: ray queue too small for one tile");
+      prev = claimed;
+      // keep the tile counter; clear the queues
+      cudaMemsetAsync(wq.ctr + 1, 0, sizeof(unsigned long long) * (kCtrCount - 1), s->stream);
+    }
     S.ms_pairs = t.stop();
     if ((rc = read_err(s))) return rc;
     // Duffy integrals overwrite the singular Quad8 pairs (Duffy for
