@@ -7,13 +7,16 @@
 // once, one ray per lane:
 //   * interior phase: each lane walks its own ray through the pre-order tree
 //     (slab test, descend to node+1 on a pass, jump to the miss link on a
-//     miss) until it reaches a leaf whose box it passes, or the end;
-//   * leaf phase: the primitives of all pending leaves of the warp are dealt
-//     out to the 32 lanes (a lane may test another lane's ray, read from the
-//     warp's shared-memory ray bank), so a leaf of 8 triangles costs one
+//     miss), collecting the leaves whose boxes it passes, until the end
+//     (up to kLeafSlots of them per round, so that lanes which reach a leaf
+//     early keep walking while the others catch up);
+//   * leaf phase: the primitives of all collected leaves of the warp are
+//     dealt out to the 32 lanes (a lane may test another lane's ray, read from
+//     the warp's shared-memory ray bank), so a leaf of 8 triangles costs one
 //     primitive test per lane instead of eight on one lane.
-// The set of (ray, triangle) tests is exactly the set the reference's walk
-// performs up to its first hit, so the any-hit answer is the reference's.
+// The (ray, triangle) tests are the reference walk's tests up to its first
+// hit plus at most the rest of that round's collected leaves, so the any-hit
+// answer is the reference's.
 #pragma once
 
 #include "device_mixed.cuh"
@@ -23,16 +26,25 @@ namespace rvf {
 // Per-warp shared-memory scratch: the ray bank with the leaf-phase work
 // lists (RayBank) and, for the fused kernel, the compaction buffers.  3D FP64 rays use o/d/tmax; 2-D segments store
 // their two end points in o (x, y) and d (x, y); FP32 rays use the *f arrays.
+constexpr int kLeafSlots = 4;  // passed leaves a lane collects per round
+
 struct RayBank {
-  double o[3][32];
-  double d[3][32];
-  double tmax[32];
-  float of[3][32];
-  float df[3][32];
-  float tmaxf[32];
-  float deltaf[32];
+  union {
+    struct {
+      double o[3][32];
+      double d[3][32];
+      double tmax[32];
+    } r64;  // FP64 rays; 2-D segments keep their end points in o (x, y) and d (x, y)
+    struct {
+      float o[3][32];
+      float d[3][32];
+      float tmax[32];
+      float delta[32];
+    } r32;
+  };
   int32_t gi[32], gj[32];
-  uint8_t owner[256];     // leaf phase: owning lane of each (ray, primitive) item
+  int32_t first[kLeafSlots][32];          // collected leaves: first primitive
+  uint16_t item[32 * kLeafSlots * 8];     // leaf phase: (lane, leaf slot, offset) per test
   uint8_t hit[32];
   uint8_t unsure[32];
 };
@@ -118,9 +130,11 @@ __device__ __forceinline__ int trace_batch(bool have, const Node* __restrict__ n
   int k = 0;
   bool done = !have;
   bool unsure = false;
-  for (int round = 0;; ++round) {
-    int la = 0, lc = 0;
-    while (!done && lc == 0) {
+  for (;;) {
+    // interior phase: walk until kLeafSlots passed leaves are collected or the walk ends
+    int nl = 0, total_own = 0;
+    uint32_t counts = 0;  // 4 bits per collected leaf
+    while (!done && nl < kLeafSlots) {
       const Node nd = nodes[k];
       ++cnt.nodes;
       const int s = pol.node(nd);
@@ -131,43 +145,47 @@ __device__ __forceinline__ int trace_batch(bool have, const Node* __restrict__ n
         ++cnt.unsure_slab;
         done = true;
       } else if (s == kHit && count > 0) {
-        la = first;
-        lc = count;
+        ws.first[nl][lane] = first;
+        counts |= (uint32_t)count << (4 * nl);
+        total_own += count;
+        ++nl;
         k = pol.miss(nd);
       } else {
         k = (s == kHit) ? k + 1 : pol.miss(nd);
       }
-      if (lc == 0 && k >= n_nodes) done = true;
+      if (k >= n_nodes) done = true;
     }
-    // leaf phase: deal the pending (ray, primitive) tests out to the lanes
-    int incl = lc;
+    // leaf phase: deal the collected (ray, primitive) tests out to the lanes
+    int incl = total_own;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
       const int v = __shfl_up_sync(kFull, incl, o);
       if (lane >= o) incl += v;
     }
     const int total = __shfl_sync(kFull, incl, 31);
-    if (total == 0) break;
-    const int excl = incl - lc;
-    for (int u = 0; u < lc; ++u) ws.owner[excl + u] = (uint8_t)lane;
+    if (total == 0) {
+      if (!__any_sync(kFull, !done)) break;
+      continue;
+    }
+    int pos = incl - total_own;
+    for (int sl = 0; sl < nl; ++sl) {
+      const int c = (int)((counts >> (4 * sl)) & 15u);
+      for (int u = 0; u < c; ++u) ws.item[pos++] = (uint16_t)((lane << 5) | (sl << 3) | u);
+    }
     __syncwarp();
     for (int base = 0; base < total; base += 32) {
       const int t = base + lane;
-      const int o = (t < total) ? (int)ws.owner[t] : 0;
-      const int oa = __shfl_sync(kFull, la, o);
-      const int oe = __shfl_sync(kFull, excl, o);
       if (t < total) {
-        const int r = pol.prim(ws, o, oa + (t - oe), cnt);
+        const int it = ws.item[t];
+        const int o = it >> 5;
+        const int r = pol.prim(ws, o, ws.first[(it >> 3) & 3][o] + (it & 7), cnt);
         if (r == kHit) ws.hit[o] = 1;
         else if (r == kUnsure) ws.unsure[o] = 1;
       }
-      __syncwarp();
-    }
-    if (lc > 0) {
-      if (ws.hit[lane]) done = true;
-      else if (k >= n_nodes) done = true;
     }
     __syncwarp();
+    if (ws.hit[lane]) done = true;
+    if (!__any_sync(kFull, !done)) break;
   }
   __syncwarp();
   const bool hit = ws.hit[lane] != 0;
@@ -185,10 +203,10 @@ struct PolD3 {
   __device__ __forceinline__ void store(RayBank& ws, int lane, int32_t gi, int32_t gj) const {
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-      ws.o[c][lane] = R.o[c];
-      ws.d[c][lane] = R.d[c];
+      ws.r64.o[c][lane] = R.o[c];
+      ws.r64.d[c][lane] = R.d[c];
     }
-    ws.tmax[lane] = R.tmax;
+    ws.r64.tmax[lane] = R.tmax;
     ws.gi[lane] = gi;
     ws.gj[lane] = gj;
   }
@@ -205,10 +223,10 @@ struct PolD3 {
     RayD Q;
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-      Q.o[c] = ws.o[c][o];
-      Q.d[c] = ws.d[c][o];
+      Q.o[c] = ws.r64.o[c][o];
+      Q.d[c] = ws.r64.d[c][o];
     }
-    Q.tmax = ws.tmax[o];
+    Q.tmax = ws.r64.tmax[o];
     return mt_d(tr, Q) ? kHit : kMiss;
   }
 };
@@ -219,10 +237,10 @@ struct PolD2 {
   double a[2], b[2];
   const SegD* segs;
   __device__ __forceinline__ void store(RayBank& ws, int lane, int32_t gi, int32_t gj) const {
-    ws.o[0][lane] = a[0];
-    ws.o[1][lane] = a[1];
-    ws.d[0][lane] = b[0];
-    ws.d[1][lane] = b[1];
+    ws.r64.o[0][lane] = a[0];
+    ws.r64.o[1][lane] = a[1];
+    ws.r64.d[0][lane] = b[0];
+    ws.r64.d[1][lane] = b[1];
     ws.gi[lane] = gi;
     ws.gj[lane] = gj;
   }
@@ -240,7 +258,7 @@ struct PolD2 {
     const SegD sg = segs[k];
     if (sg.group == ws.gi[o] || sg.group == ws.gj[o]) return kMiss;
     ++cnt.prims;
-    const double xa[2] = {ws.o[0][o], ws.o[1][o]}, xb[2] = {ws.d[0][o], ws.d[1][o]};
+    const double xa[2] = {ws.r64.o[0][o], ws.r64.o[1][o]}, xb[2] = {ws.r64.d[0][o], ws.r64.d[1][o]};
     return seg_blocks(sg, xa, xb) ? kHit : kMiss;
   }
 };
@@ -252,11 +270,11 @@ struct PolF3 {
   __device__ __forceinline__ void store(RayBank& ws, int lane, int32_t gi, int32_t gj) const {
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-      ws.of[c][lane] = R.o[c];
-      ws.df[c][lane] = R.d[c];
+      ws.r32.o[c][lane] = R.o[c];
+      ws.r32.d[c][lane] = R.d[c];
     }
-    ws.tmaxf[lane] = R.tmax;
-    ws.deltaf[lane] = R.delta;
+    ws.r32.tmax[lane] = R.tmax;
+    ws.r32.delta[lane] = R.delta;
     ws.gi[lane] = gi;
     ws.gj[lane] = gj;
   }
@@ -273,11 +291,11 @@ struct PolF3 {
     RayF Q;
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-      Q.o[c] = ws.of[c][o];
-      Q.d[c] = ws.df[c][o];
+      Q.o[c] = ws.r32.o[c][o];
+      Q.d[c] = ws.r32.d[c][o];
     }
-    Q.tmax = ws.tmaxf[o];
-    Q.delta = ws.deltaf[o];
+    Q.tmax = ws.r32.tmax[o];
+    Q.delta = ws.r32.delta[o];
     const int r = mt_f(tr, Q);
     if (r == kUnsure) ++cnt.unsure_prim;
     return r;
