@@ -355,6 +355,7 @@ int ensure_tables(Session* s, rvf_mesh* m, int nquad, Tables** out) {
   if ((rc = T->nrm.alloc(s, sizeof(double) * 3 * std::max<int64_t>(N, 1)))) return rc;
   if ((rc = T->cen.alloc(s, sizeof(double) * 3 * std::max<int64_t>(N, 1)))) return rc;
   if ((rc = T->diam.alloc(s, sizeof(double) * std::max<int64_t>(N, 1)))) return rc;
+  if ((rc = T->rad.alloc(s, sizeof(double) * std::max<int64_t>(N, 1)))) return rc;
   cudaMemsetAsync(T->tab.ptr, 0, T->tab.bytes, s->stream);
   cudaMemsetAsync(s->err.ptr, 0, sizeof(int), s->stream);
   PrepArgs a{};
@@ -377,6 +378,7 @@ int ensure_tables(Session* s, rvf_mesh* m, int nquad, Tables** out) {
   a.nrm = (double*)T->nrm.ptr;
   a.cen = (double*)T->cen.ptr;
   a.diam = (double*)T->diam.ptr;
+  a.rad = (double*)T->rad.ptr;
   a.err = (int*)s->err.ptr;
   cudaError_t e = launch_prep(a, s->stream);
   if (e != cudaSuccess) return cuda_err(e, "prep kernel launch");

@@ -59,6 +59,7 @@ struct PrepArgs {
   double* nrm;     // 3N
   double* cen;     // 3N
   double* diam;    // N
+  double* rad;     // N: largest distance of a quadrature point from the centroid (or null)
   int* err;
 };
 
@@ -75,6 +76,9 @@ struct PairArgs {
   const double* nrm;
   const int32_t* group;
   const int32_t* orig;  // internal -> caller's element index (null: identity)
+  const double* cen;    // pair culling: element centroids and point radii (or null)
+  const double* rad;
+  double cull_margin;
   double* F;        // N x N column-major, caller's element order
   // occlusion (n_nodes == 0: none)
   const NodeD* nodes;
@@ -126,6 +130,8 @@ struct MixedArgs {
   const double* cen;
   const double* diam;
   double near_factor;
+  const double* rad;
+  double cull_margin;
   const int32_t* group;
   const int32_t* orig;
   double* F;

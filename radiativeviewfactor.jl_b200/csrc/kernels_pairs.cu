@@ -78,6 +78,16 @@ __global__ void k_prep(PrepArgs a) {
       dm = fmax(dm, sqrt(dx * dx + dy * dy + dz * dz));
     }
   a.diam[e] = dm;
+  if (a.rad) {
+    double r2max = 0.0;
+    for (int p = 0; p < np; ++p) {
+      const double dx = base[(0 * a.pmax + p) * kTile] - a.cen[3 * e + 0];
+      const double dy = base[(1 * a.pmax + p) * kTile] - a.cen[3 * e + 1];
+      const double dz = base[(2 * a.pmax + p) * kTile] - a.cen[3 * e + 2];
+      r2max = fmax(r2max, dx * dx + dy * dy + dz * dz);
+    }
+    a.rad[e] = sqrt(r2max) * (1.0 + 1e-12);
+  }
 }
 
 // ---------------------------------------------------------------------------

@@ -118,6 +118,30 @@ __device__ __forceinline__ int64_t claim_tile(const WaveQ& q, int64_t n_tiles, b
   return t;
 }
 
+// True when every segment between a point of element i and a point of
+// element j certainly misses the box: each such segment stays within
+// R = max(rad_i, rad_j) of the centroid segment (convexity), so it suffices
+// that the centroid segment misses the box grown by R plus a margin that
+// dwarfs every rounding error of the reference's slab test.  2-D uses x, y.
+template <bool DIM3>
+__device__ __forceinline__ bool pair_misses_box(const double* ci, const double* cj, double R, const NodeD& nd) {
+  double te = 0.0, tx = 1.0;
+#pragma unroll
+  for (int c = 0; c < (DIM3 ? 3 : 2); ++c) {
+    const double lo = nd.lo[c] - R, hi = nd.hi[c] + R;
+    const double d = cj[c] - ci[c];
+    if (d == 0.0) {
+      if (ci[c] < lo || ci[c] > hi) return true;
+      continue;
+    }
+    const double inv = 1.0 / d;
+    const double t1 = (lo - ci[c]) * inv, t2 = (hi - ci[c]) * inv;
+    te = fmax(te, fmin(t1, t2));
+    tx = fmin(tx, fmax(t1, t2));
+  }
+  return te > tx;
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------------------
@@ -204,6 +228,10 @@ __global__ void __launch_bounds__(256, 2) k_gen_fp64(PairArgs a) {
       uint8_t* logp = (a.ray_log && valid)
                           ? a.ray_log + ((uint64_t)(sw ? oj : oi) * N + (sw ? oi : oj)) * a.log_pm * a.log_pm
                           : nullptr;
+      // pairs whose rays all certainly miss the root box need no ray at all
+      const bool cullp = OCC && npj > 0 && a.rad &&
+                         pair_misses_box<DIM3>(a.cen + 3 * i, a.cen + 3 * j, fmax(a.rad[i], a.rad[j]) + a.cull_margin,
+                                               nodes[0]);
       double acc = 0.0;
       int64_t slot = -1;
       int nst = 0;
@@ -240,7 +268,9 @@ __global__ void __launch_bounds__(256, 2) k_gen_fp64(PairArgs a) {
           if (OCC) {
             bool cast, defer = false;
             const NodeD& root = nodes[0];
-            if (DIM3) {
+            if (cullp) {
+              cast = (K > 0.0) && (!DIM3 || sqrt(r2) > 1e-15);  // make_ray's cast rule
+            } else if (DIM3) {
               RayD R;
               cast = (K > 0.0) && (sw ? make_ray(xj, -rx, -ry, -rz, r2, R) : make_ray(xi, rx, ry, rz, r2, R));
               if (cast) defer = slab_d(root, R);
@@ -302,7 +332,8 @@ __global__ void __launch_bounds__(256, 2) k_gen_fp64(PairArgs a) {
 template <bool OCC>
 __device__ __noinline__ void gen_mixed64(const MixedArgs& a, const NodeD* nodes, const double* it64,
                                          const double* jb64, int p, int q, bool need64, bool exactK_in, bool graze,
-                                         bool sw, double contrib32, uint8_t* logp, bool& defer64, double& accd,
+                                         bool sw, bool cullp, double contrib32, uint8_t* logp, bool& defer64,
+                                         double& accd,
                                          uint32_t& n_rays, uint32_t& n_rays64, uint32_t& n_graze) {
   const int pm = a.pmax;
   double xi[3], ni[3];
@@ -324,9 +355,13 @@ __device__ __noinline__ void gen_mixed64(const MixedArgs& a, const NodeD* nodes,
   bool cast64 = false;
   defer64 = false;
   if (OCC && need64 && (!exactK || K64 > 0.0)) {
-    RayD R64;
-    cast64 = sw ? make_ray(xj, -rx64, -ry64, -rz64, r264, R64) : make_ray(xi, rx64, ry64, rz64, r264, R64);
-    if (cast64) defer64 = slab_d(nodes[0], R64);
+    if (cullp) {
+      cast64 = sqrt(r264) > 1e-15;  // make_ray's cast rule; the ray certainly misses the root
+    } else {
+      RayD R64;
+      cast64 = sw ? make_ray(xj, -rx64, -ry64, -rz64, r264, R64) : make_ray(xi, rx64, ry64, rz64, r264, R64);
+      if (cast64) defer64 = slab_d(nodes[0], R64);
+    }
     if (cast64 && !defer64 && logp) logp[sw ? q * a.log_pm + p : p * a.log_pm + q] = 1;
   }
   n_rays64 += cast64 ? 1 : 0;
@@ -426,6 +461,9 @@ __global__ void __launch_bounds__(256, 2) k_gen_mixed(MixedArgs a) {
                   an2 = (float)(ci2 + (sw ? dc2 : 0.0));
       const float* ibf = iblk + li;
       const double* it64 = a.tab + bi * kComp * pm * kTile + li;
+      const bool cullp = OCC && npj > 0 && a.rad &&
+                         pair_misses_box<true>(a.cen + 3 * i, a.cen + 3 * j, fmax(a.rad[i], a.rad[j]) + a.cull_margin,
+                                               a.nodes[0]);
       uint8_t* logp = (a.ray_log && valid)
                           ? a.ray_log + ((uint64_t)(sw ? oj : oi) * N + (sw ? oi : oj)) * a.log_pm * a.log_pm
                           : nullptr;
@@ -457,7 +495,9 @@ __global__ void __launch_bounds__(256, 2) k_gen_mixed(MixedArgs a) {
           const bool cast32 = far && !graze && K32 > 0.0f;
           bool badray = false, defer32 = false;
           n_pp += lq ? 1 : 0;
-          if (OCC && cast32) {
+          if (OCC && cast32 && cullp) {
+            if (logp) logp[sw ? q * a.log_pm + p : p * a.log_pm + q] = 1;
+          } else if (OCC && cast32) {
             RayF R;
             const float xo[3] = {an0 + (sw ? oq0 : op0), an1 + (sw ? oq1 : op1), an2 + (sw ? oq2 : op2)};
             const bool rok =
@@ -474,7 +514,7 @@ __global__ void __launch_bounds__(256, 2) k_gen_mixed(MixedArgs a) {
           const bool need64 = lq && (near || graze || badray);
           bool defer64 = false;
           if (__any_sync(kFull, need64))
-            gen_mixed64<OCC>(a, a.nodes, it64, jb64, p, q, need64, near || graze, graze, sw,
+            gen_mixed64<OCC>(a, a.nodes, it64, jb64, p, q, need64, near || graze, graze, sw, cullp,
                              (double)(wq * (wp * K32)), logp, defer64, accd, n_rays, n_rays64, n_graze);
           if (OCC) {
             slot_alloc(Q, (defer32 || defer64) && slot < 0, slot, &s_slots);

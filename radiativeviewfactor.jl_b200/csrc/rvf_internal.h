@@ -44,7 +44,7 @@ int upload(Session* s, DevBuf& b, const void* src, size_t n);
 
 struct Tables {
   int nquad = 0, pmax = 0;
-  DevBuf rules, tab, area, np, flat, nrm, cen, diam;  // internal element order
+  DevBuf rules, tab, area, np, flat, nrm, cen, diam, rad;  // internal element order
   DevBuf area_orig;                                   // areas in the caller's element order
   DevBuf tabf;  // FP32 table, built on the first mixed-precision solve
 };

@@ -422,6 +422,9 @@ int rvf_solve(rvf_session* s, rvf_mesh* m, const rvf_options* o, double* F_elem,
   a.nrm = T->nrm.as<double>();
   a.group = m->group.as<int32_t>();
   a.orig = m->orig.as<int32_t>();
+  a.cen = T->cen.as<double>();
+  a.rad = T->rad.as<double>();
+  a.cull_margin = std::ldexp(m->extent, -30);
   a.F = m->F.as<double>();
   a.nodes = occ ? m->nodes.as<NodeD>() : nullptr;
   a.n_nodes = occ ? m->n_nodes : 0;
@@ -451,6 +454,7 @@ int rvf_solve(rvf_session* s, rvf_mesh* m, const rvf_options* o, double* F_elem,
       x.N = N; x.nT = a.nT; x.n_tiles = a.n_tiles; x.pmax = a.pmax;
       x.tab = a.tab; x.tabf = T->tabf.as<float>(); x.np = a.np; x.area = a.area; x.flat = a.flat; x.nrm = a.nrm;
       x.cen = T->cen.as<double>(); x.diam = T->diam.as<double>(); x.near_factor = o->near_field_factor;
+      x.rad = a.rad; x.cull_margin = a.cull_margin;
       x.group = a.group; x.orig = a.orig; x.F = a.F;
       x.nodes = a.nodes; x.n_nodes = a.n_nodes;
       x.nodesf = occ ? m->nodesf.as<NodeF>() : nullptr;
