@@ -39,6 +39,19 @@ OBSTRUCTION = [7]
 FLOP_POINT_PAIR = 23
 FLOP_SLAB = 12
 FLOP_TRI = 51
+# Reference-order traversal counts of the bench workloads: node (box) tests
+# and triangle tests of the reference's stackless walk (src/GPUBVH.jl:202-285)
+# ray by ray, from the oracle's instrumented FP64 traversal
+# (oracle.pyoracle.solve_plain(Mesh(md, [7]), 3) counters [1..3]).  Every
+# cast ray's first box test (the root) runs in the generation kernel, so the
+# traversal kernels' algorithmic work is 12 (node_visits - n_rays) + 51 prim_tests.
+REF_COUNTS = {
+    "medium": {"n_rays": 975146106, "node_visits": 5688464541, "prim_tests": 3647097481},
+}
+# DRAM bytes per traced ray of the traversal kernels (dram__bytes_read.sum +
+# dram__bytes_write.sum of one ncu capture on the medium workload divided by
+# the rays it traced; the capture is summarized under profiles/).
+TRAFFIC_PER_TRACED_RAY = {"mixed": None, "fp64": None}
 
 
 def load_pkg():
@@ -210,14 +223,35 @@ def timed_solves(dm, opts, steps, warmup, flush, ws, local):
     return stats, clk.summary()
 
 
-def roofline(stats, peak, bound, kernel):
+def roofline(stats, peak, bound, kernel, prec, size):
+    """Roofline of the dominant kernel, the traversal (FP32 + FP64 re-traversal
+    in mixed mode): algorithmic flop per step / CUDA-event time of the kernel."""
     s0 = stats[-1]
-    pair_ms = statistics.mean(s["ms_pairs"] for s in stats)
-    flops = FLOP_POINT_PAIR * s0["n_point_pairs"] + FLOP_SLAB * s0["node_visits"] + FLOP_TRI * s0["prim_tests"]
-    achieved = flops / (pair_ms / 1e3) / 1e12
+    trace_ms = statistics.mean(s["ms_trace"] + s["ms_trace_fp64"] for s in stats)
+    chunks = max(1, int(s0["n_chunks"]))
+    ref = REF_COUNTS.get(size)
+    if ref:
+        flops = FLOP_SLAB * (ref["node_visits"] - ref["n_rays"]) + FLOP_TRI * ref["prim_tests"]
+        src = "reference-order box and triangle tests (oracle traversal of this workload)"
+    else:
+        flops = FLOP_SLAB * (s0["node_visits"] - s0["n_rays_traced"]) + FLOP_TRI * s0["prim_tests"]
+        src = "box and triangle tests as executed (no reference-order counts for this size)"
+    achieved = flops / (trace_ms / 1e3) / 1e12
+    tpr = TRAFFIC_PER_TRACED_RAY.get(prec)
+    traffic = tpr * s0["n_rays_traced"] / chunks if tpr else None
     return {"bound": bound, "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
-            "traffic": None, "peak_source": "measured by rvf_fma_peak (FMA microbenchmark) in this run",
-            "kernel": kernel, "kernel_ms": pair_ms, "algorithmic_flop_per_launch": flops}
+            "traffic": traffic, "peak_source": "measured by rvf_fma_peak (FMA microbenchmark) in this run",
+            "kernel": kernel, "kernel_ms_per_launch": trace_ms / chunks, "launches_per_step": chunks,
+            "algorithmic_flop_per_launch": flops / chunks, "work_counts": src,
+            "traffic_source": "ncu capture of the medium workload scaled by traced rays" if tpr else None}
+
+
+def phases(stats):
+    keys = ("ms_gen", "ms_trace", "ms_trace_fp64", "ms_resolve", "ms_prep", "ms_reduce")
+    d = {k: statistics.mean(s[k] for s in stats) for k in keys}
+    d["n_chunks"] = int(stats[-1]["n_chunks"])
+    d["n_rays_traced"] = int(stats[-1]["n_rays_traced"])
+    return d
 
 
 def run_ours(args):
@@ -263,9 +297,9 @@ def run_ours(args):
     peak32 = _abi.fma_peak(local, False)
     H = runs[head]
     if head == "mixed":
-        roof = roofline(H["stats"], peak32, "fp32_fma", "k_pairs_mixed<OCC>")
+        roof = roofline(H["stats"], peak32, "fp32_fma", "k_trace32 (+ k_trace64 re-traversal)", "mixed", args.size)
     else:
-        roof = roofline(H["stats"], peak64, "fp64_fma", "k_pairs_fp64<DIM3,OCC>")
+        roof = roofline(H["stats"], peak64, "fp64_fma", "k_trace64<DIM3=1>", "fp64", args.size)
 
     # ---- e2e: through the C ABI with host buffers ----
     e2e = None
@@ -311,11 +345,14 @@ def run_ours(args):
             "gpu_launches": int(sum(s["gpu_kernels"] for s in H["stats"])),
             "roofline": roof,
             "clocks": H["clocks"],
+            "phases": phases(H["stats"]),
             "counts": {k: s0[k] for k in ("n_point_pairs", "n_rays", "n_rays_fp64", "n_pairs_fp64", "node_visits",
-                                          "prim_tests")}}
+                                          "prim_tests", "n_rays_traced")}}
     if len(precisions) == 2:
         line["fp64"] = {"value": runs["fp64"]["value"], "ms_per_step": runs["fp64"]["ms"],
-                        "roofline": roofline(runs["fp64"]["stats"], peak64, "fp64_fma", "k_pairs_fp64<DIM3,OCC>"),
+                        "roofline": roofline(runs["fp64"]["stats"], peak64, "fp64_fma", "k_trace64<DIM3=1>", "fp64",
+                                             args.size),
+                        "phases": phases(runs["fp64"]["stats"]),
                         "clocks": runs["fp64"]["clocks"]}
         line["mixed_over_fp64"] = runs["mixed"]["value"] / runs["fp64"]["value"]
         line["accuracy"] = accuracy

@@ -32,7 +32,7 @@
 extern "C" {
 #endif
 
-#define RVF_ABI_VERSION 1
+#define RVF_ABI_VERSION 2
 
 /* status codes */
 #define RVF_OK 0
@@ -126,6 +126,20 @@ typedef struct {
   int64_t n_pairs_fp64;   /* mixed mode: pairs integrated in FP64 (near field / grazing) */
   int64_t n_duffy_pairs;  /* vertex- or edge-sharing Quad8 pairs */
   double max_row_sum_dev; /* max_i |sum_j F_ij - 1| */
+  int64_t n_node_visits;  /* BVH box tests, as executed */
+  int64_t n_prim_tests;   /* ray-primitive tests, as executed */
+  int64_t n_kernels;      /* kernels of this library launched by the call */
+  int64_t n_graze_fp64;   /* mixed: grazing point pairs evaluated in FP64 */
+  int64_t n_unsure_rays;  /* mixed: FP32 rays with an uncertain decision (traced again in FP64) */
+  int64_t n_unsure_slab;  /* ... uncertain at a box test */
+  int64_t n_unsure_prim;  /* ... uncertain at a triangle test */
+  int64_t n_unsure_dir;   /* mixed: rays with a direction component below 1e-4 (FP64 from the start) */
+  int64_t n_rays_traced;  /* rays that passed the root box and went through the traversal queues */
+  int64_t n_chunks;       /* queue refills of the pair pipeline */
+  double ms_gen;          /* pair pipeline phases (CUDA events on the solve stream, summed over chunks): */
+  double ms_trace;        /*   traversal (FP32 in mixed mode) */
+  double ms_trace_fp64;   /*   mixed mode: FP64 traversal of the uncertain and FP64 rays */
+  double ms_resolve;      /*   visible terms of the traced rays */
   int64_t reserved[8];
 } rvf_stats;
 

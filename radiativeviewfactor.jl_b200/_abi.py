@@ -53,18 +53,24 @@ class Stats(C.Structure):
                 ("ms_duffy", C.c_double), ("ms_reduce", C.c_double), ("ms_download", C.c_double),
                 ("ms_total", C.c_double), ("n_pairs", C.c_int64), ("n_point_pairs", C.c_int64),
                 ("n_rays", C.c_int64), ("n_rays_fp64", C.c_int64), ("n_pairs_fp64", C.c_int64),
-                ("n_duffy_pairs", C.c_int64), ("max_row_sum_dev", C.c_double), ("reserved", C.c_int64 * 8)]
+                ("n_duffy_pairs", C.c_int64), ("max_row_sum_dev", C.c_double),
+                ("n_node_visits", C.c_int64), ("n_prim_tests", C.c_int64), ("n_kernels", C.c_int64),
+                ("n_graze_fp64", C.c_int64), ("n_unsure_rays", C.c_int64), ("n_unsure_slab", C.c_int64),
+                ("n_unsure_prim", C.c_int64), ("n_unsure_dir", C.c_int64), ("n_rays_traced", C.c_int64),
+                ("n_chunks", C.c_int64), ("ms_gen", C.c_double), ("ms_trace", C.c_double),
+                ("ms_trace_fp64", C.c_double), ("ms_resolve", C.c_double), ("reserved", C.c_int64 * 8)]
 
     def as_dict(self):
         d = {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
-        d["node_visits"] = int(self.reserved[0])
-        d["prim_tests"] = int(self.reserved[1])
-        d["gpu_kernels"] = int(self.reserved[2])
-        d["graze_point_pairs"] = int(self.reserved[3])
-        d["unsure_rays"] = int(self.reserved[4])
-        d["unsure_slab"] = int(self.reserved[5])
-        d["unsure_prim"] = int(self.reserved[6])
-        d["unsure_direction"] = int(self.reserved[7])
+        # short names used by the bench line
+        d["node_visits"] = int(self.n_node_visits)
+        d["prim_tests"] = int(self.n_prim_tests)
+        d["gpu_kernels"] = int(self.n_kernels)
+        d["graze_point_pairs"] = int(self.n_graze_fp64)
+        d["unsure_rays"] = int(self.n_unsure_rays)
+        d["unsure_slab"] = int(self.n_unsure_slab)
+        d["unsure_prim"] = int(self.n_unsure_prim)
+        d["unsure_direction"] = int(self.n_unsure_dir)
         return d
 
 

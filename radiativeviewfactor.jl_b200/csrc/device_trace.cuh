@@ -26,9 +26,12 @@ namespace rvf {
 // Per-warp shared-memory scratch: the ray bank with the leaf-phase work
 // lists (RayBank) and, for the fused kernel, the compaction buffers.  3D FP64 rays use o/d/tmax; 2-D segments store
 // their two end points in o (x, y) and d (x, y); FP32 rays use the *f arrays.
-constexpr int kLeafSlots = 4;  // passed leaves a lane collects per round
+constexpr int kLeafSlots = 4;     // passed leaves a lane collects per round (FP64 traversal)
+constexpr int kLeafSlotsF = 4;    // same, FP32 traversal (more slots cost more occupancy than they save)
 
-struct RayBank {
+// Per-warp ray bank and leaf-phase work lists for L collected leaves per lane.
+template <int L>
+struct RayBankT {
   union {
     struct {
       double o[3][32];
@@ -43,16 +46,57 @@ struct RayBank {
     } r32;
   };
   int32_t gi[32], gj[32];
-  int32_t first[kLeafSlots][32];          // collected leaves: first primitive
-  uint16_t item[32 * kLeafSlots * 8];     // leaf phase: (lane, leaf slot, offset) per test
+  int32_t first[L][32];          // collected leaves: first primitive
+  uint16_t item[32 * L * 8];     // leaf phase: (lane, leaf slot, offset) per test
   uint8_t hit[32];
   uint8_t unsure[32];
 };
+using RayBank = RayBankT<kLeafSlots>;
+using RayBankF = RayBankT<kLeafSlotsF>;
 
 struct WarpScratch {
   RayBank bank;
   double contrib[2][64];  // [0] FP64 / main buffer, [1] FP32 buffer (mixed)
   uint32_t meta[2][64];
+};
+
+// ---------------------------------------------------------------------------
+// Node sources for the traversal.  In shared memory the 16-byte chunks of
+// each node are XOR-swizzled: lanes of a warp walk different nodes, and with
+// the plain layout chunk c of every 64-byte node falls into one of only two
+// of the eight 16-byte bank groups (one of four for 32-byte nodes), so a
+// warp's node load needs up to 4x the ideal shared-memory wavefronts.
+// Chunk c of node k is stored at chunk 4k + (c ^ ((k >> 1) & 3)) (FP64) or
+// 2k + (c ^ ((k >> 2) & 1)) (FP32), which spreads any chunk over all eight
+// groups as k varies.
+// ---------------------------------------------------------------------------
+template <typename Node>
+struct GlobalNodes {
+  const Node* p;
+  __device__ __forceinline__ Node operator()(int k) const { return p[k]; }
+};
+
+template <typename Node>
+struct SwizNodes {
+  static constexpr int C = sizeof(Node) / 16;  // 16-byte chunks per node (4 or 2)
+  const int4* p;
+  __device__ static __forceinline__ int slot(int k, int c) {
+    return C == 4 ? 4 * k + (c ^ ((k >> 1) & 3)) : 2 * k + (c ^ ((k >> 2) & 1));
+  }
+  __device__ __forceinline__ Node operator()(int k) const {
+    union {
+      int4 v[C];
+      Node n;
+    } u;
+#pragma unroll
+    for (int c = 0; c < C; ++c) u.v[c] = p[slot(k, c)];
+    return u.n;
+  }
+  // block-cooperative copy of n nodes from global memory into dst
+  __device__ static void fill(int4* dst, const Node* src, int n) {
+    const int4* s4 = reinterpret_cast<const int4*>(src);
+    for (int t = threadIdx.x; t < n * C; t += blockDim.x) dst[slot(t / C, t % C)] = s4[t];
+  }
 };
 
 // buffer entry: owner lane (5 bits), swapped (1 bit), source point p (6 bits),
@@ -115,14 +159,16 @@ __device__ __forceinline__ void buf_collect(const WarpScratch& ws, int b, int n,
 // ---------------------------------------------------------------------------
 // Generic batch traversal.  Pol provides
 //   node(const Node&) -> int   kHit / kMiss / kUnsure for the lane's own ray
+// (nodes(k) returns node k: GlobalNodes or SwizNodes)
 //   leaf(const Node&, int& first, int& count)
 //   prim(ws, owner, k) -> int  kHit / kMiss / kUnsure for owner's ray
 // Returns kHit (blocked), kMiss (visible) or kUnsure (FP32 only: some
 // decision of the walk was not certain and no certain hit was found).
 // ---------------------------------------------------------------------------
-template <typename Node, typename Pol>
-__device__ __forceinline__ int trace_batch(bool have, const Node* __restrict__ nodes, int n_nodes, RayBank& ws,
-                                           Pol& pol, TravCount& cnt) {
+template <typename Src, typename Pol, int L>
+__device__ __forceinline__ int trace_batch(bool have, const Src& nodes, int n_nodes, RayBankT<L>& ws, Pol& pol,
+                                           TravCount& cnt) {
+  static_assert(L <= 8, "leaf slot index is 3 bits");
   const int lane = threadIdx.x & 31;
   ws.hit[lane] = 0;
   ws.unsure[lane] = 0;
@@ -134,8 +180,8 @@ __device__ __forceinline__ int trace_batch(bool have, const Node* __restrict__ n
     // interior phase: walk until kLeafSlots passed leaves are collected or the walk ends
     int nl = 0, total_own = 0;
     uint32_t counts = 0;  // 4 bits per collected leaf
-    while (!done && nl < kLeafSlots) {
-      const Node nd = nodes[k];
+    while (!done && nl < L) {
+      const auto nd = nodes(k);
       ++cnt.nodes;
       const int s = pol.node(nd);
       int first, count;
@@ -170,15 +216,15 @@ __device__ __forceinline__ int trace_batch(bool have, const Node* __restrict__ n
     int pos = incl - total_own;
     for (int sl = 0; sl < nl; ++sl) {
       const int c = (int)((counts >> (4 * sl)) & 15u);
-      for (int u = 0; u < c; ++u) ws.item[pos++] = (uint16_t)((lane << 5) | (sl << 3) | u);
+      for (int u = 0; u < c; ++u) ws.item[pos++] = (uint16_t)((lane << 6) | (sl << 3) | u);
     }
     __syncwarp();
     for (int base = 0; base < total; base += 32) {
       const int t = base + lane;
       if (t < total) {
         const int it = ws.item[t];
-        const int o = it >> 5;
-        const int r = pol.prim(ws, o, ws.first[(it >> 3) & 3][o] + (it & 7), cnt);
+        const int o = it >> 6;
+        const int r = pol.prim(ws, o, ws.first[(it >> 3) & 7][o] + (it & 7), cnt);
         if (r == kHit) ws.hit[o] = 1;
         else if (r == kUnsure) ws.unsure[o] = 1;
       }
@@ -200,7 +246,8 @@ __device__ __forceinline__ int trace_batch(bool have, const Node* __restrict__ n
 struct PolD3 {
   RayD R;
   const TriD* tris;
-  __device__ __forceinline__ void store(RayBank& ws, int lane, int32_t gi, int32_t gj) const {
+  template <typename B>
+  __device__ __forceinline__ void store(B& ws, int lane, int32_t gi, int32_t gj) const {
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       ws.r64.o[c][lane] = R.o[c];
@@ -216,7 +263,8 @@ struct PolD3 {
     count = nd.b;
   }
   __device__ __forceinline__ int miss(const NodeD& nd) const { return nd.miss; }
-  __device__ __forceinline__ int prim(const RayBank& ws, int o, int k, TravCount& cnt) const {
+  template <typename B>
+  __device__ __forceinline__ int prim(const B& ws, int o, int k, TravCount& cnt) const {
     const TriD tr = tris[k];
     if (tr.group == ws.gi[o] || tr.group == ws.gj[o]) return kMiss;
     ++cnt.prims;
@@ -236,7 +284,8 @@ struct PolD3 {
 struct PolD2 {
   double a[2], b[2];
   const SegD* segs;
-  __device__ __forceinline__ void store(RayBank& ws, int lane, int32_t gi, int32_t gj) const {
+  template <typename B>
+  __device__ __forceinline__ void store(B& ws, int lane, int32_t gi, int32_t gj) const {
     ws.r64.o[0][lane] = a[0];
     ws.r64.o[1][lane] = a[1];
     ws.r64.d[0][lane] = b[0];
@@ -254,7 +303,8 @@ struct PolD2 {
     count = nd.b;
   }
   __device__ __forceinline__ int miss(const NodeD& nd) const { return nd.miss; }
-  __device__ __forceinline__ int prim(const RayBank& ws, int o, int k, TravCount& cnt) const {
+  template <typename B>
+  __device__ __forceinline__ int prim(const B& ws, int o, int k, TravCount& cnt) const {
     const SegD sg = segs[k];
     if (sg.group == ws.gi[o] || sg.group == ws.gj[o]) return kMiss;
     ++cnt.prims;
@@ -267,7 +317,8 @@ struct PolD2 {
 struct PolF3 {
   RayF R;
   const TriF* tris;
-  __device__ __forceinline__ void store(RayBank& ws, int lane, int32_t gi, int32_t gj) const {
+  template <typename B>
+  __device__ __forceinline__ void store(B& ws, int lane, int32_t gi, int32_t gj) const {
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       ws.r32.o[c][lane] = R.o[c];
@@ -284,7 +335,8 @@ struct PolF3 {
     count = nd.ab & 15;
   }
   __device__ __forceinline__ int miss(const NodeF& nd) const { return nd.miss; }
-  __device__ __forceinline__ int prim(const RayBank& ws, int o, int k, TravCount& cnt) const {
+  template <typename B>
+  __device__ __forceinline__ int prim(const B& ws, int o, int k, TravCount& cnt) const {
     const TriF tr = tris[k];
     if (tr.group == ws.gi[o] || tr.group == ws.gj[o]) return kMiss;
     ++cnt.prims;

@@ -140,7 +140,7 @@ __device__ __noinline__ void flush_fp64(const PairArgs& a, WarpScratch& ws, cons
       else make_ray(xi, rx, ry, rz, r2, pol.R);
       pol.store(ws.bank, lane, gi, gL);
     }
-    r = trace_batch(have, nodes, a.n_nodes, ws.bank, pol, tc);
+    r = trace_batch(have, GlobalNodes<NodeD>{nodes}, a.n_nodes, ws.bank, pol, tc);
   } else {
     PolD2 pol;
     pol.segs = a.segs;
@@ -149,7 +149,7 @@ __device__ __noinline__ void flush_fp64(const PairArgs& a, WarpScratch& ws, cons
     pol.b[0] = esw ? xi[0] : xj[0];
     pol.b[1] = esw ? xi[1] : xj[1];
     if (have) pol.store(ws.bank, lane, gi, gL);
-    r = trace_batch(have, nodes, a.n_nodes, ws.bank, pol, tc);
+    r = trace_batch(have, GlobalNodes<NodeD>{nodes}, a.n_nodes, ws.bank, pol, tc);
   }
   if (have && a.ray_log) {
     uint8_t* lp = a.ray_log + ((uint64_t)(esw ? oL : oi) * a.N + (esw ? oi : oL)) * a.log_pm * a.log_pm;

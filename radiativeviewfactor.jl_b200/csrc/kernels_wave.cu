@@ -148,7 +148,7 @@ __device__ __forceinline__ bool pair_misses_box(const double* ci, const double* 
 // 1. Generation, FP64 (surfaces and curves).
 // ---------------------------------------------------------------------------
 template <bool DIM3, bool OCC>
-__global__ void __launch_bounds__(256, 2) k_gen_fp64(PairArgs a) {
+__global__ void __launch_bounds__(256, 3) k_gen_fp64(PairArgs a) {
   extern __shared__ __align__(128) unsigned char smem[];
   const int pm = a.pmax;
   double* iblk = reinterpret_cast<double*>(smem);
@@ -285,10 +285,12 @@ __global__ void __launch_bounds__(256, 2) k_gen_fp64(PairArgs a) {
             }
             n_rays += cast ? 1 : 0;
             if (logp && cast && !defer) logp[sw ? q * a.log_pm + p : p * a.log_pm + q] = 1;
-            slot_alloc(Q, defer && slot < 0, slot, &s_slots);
-            stage_push(stage, nst, defer, rec_make(slot, sw, p, q));
-            if (nst >= 32) stage_flush(stage, nst, 32, Q.rec64, Q.ctr + kCtrRec64, &s_used);
-            if (defer) K = 0.0;
+            if (__any_sync(kFull, defer)) {
+              slot_alloc(Q, defer && slot < 0, slot, &s_slots);
+              stage_push(stage, nst, defer, rec_make(slot, sw, p, q));
+              if (nst >= 32) stage_flush(stage, nst, 32, Q.rec64, Q.ctr + kCtrRec64, &s_used);
+              if (defer) K = 0.0;
+            }
           }
           inner = fma(wi, K, inner);
         }
@@ -516,7 +518,7 @@ __global__ void __launch_bounds__(256, 2) k_gen_mixed(MixedArgs a) {
           if (__any_sync(kFull, need64))
             gen_mixed64<OCC>(a, a.nodes, it64, jb64, p, q, need64, near || graze, graze, sw, cullp,
                              (double)(wq * (wp * K32)), logp, defer64, accd, n_rays, n_rays64, n_graze);
-          if (OCC) {
+          if (OCC && __any_sync(kFull, defer32 || defer64)) {
             slot_alloc(Q, (defer32 || defer64) && slot < 0, slot, &s_slots);
             stage_push(st64, n64, defer64, rec_make(slot, sw, p, q));
             if (n64 >= 32) stage_flush(st64, n64, 32, Q.rec64, Q.ctr + kCtrRec64, &s_used);
@@ -584,13 +586,7 @@ __global__ void __launch_bounds__(256, 3) k_trace64(TraceArgs a) {
   RayBank* wsa = reinterpret_cast<RayBank*>(snodes + (a.nodes_in_smem ? a.n_nodes : 0));
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   RayBank& ws = wsa[warp];
-  const NodeD* nodes = a.nodes;
-  if (a.nodes_in_smem) {
-    const int4* src = reinterpret_cast<const int4*>(a.nodes);
-    int4* dst = reinterpret_cast<int4*>(snodes);
-    for (int k = threadIdx.x; k < a.n_nodes * 4; k += blockDim.x) dst[k] = src[k];
-    nodes = snodes;
-  }
+  if (a.nodes_in_smem) SwizNodes<NodeD>::fill(reinterpret_cast<int4*>(snodes), a.nodes, a.n_nodes);
   __syncthreads();
   const WaveQ& Q = a.q;
   const int pm = a.pmax;
@@ -630,7 +626,8 @@ __global__ void __launch_bounds__(256, 3) k_trace64(TraceArgs a) {
         else make_ray(xi, rx, ry, rz, r2, pol.R);
         pol.store(ws, lane, gi, gj);
       }
-      res = trace_batch(have, nodes, a.n_nodes, ws, pol, tc);
+      res = a.nodes_in_smem ? trace_batch(have, SwizNodes<NodeD>{reinterpret_cast<const int4*>(snodes)}, a.n_nodes, ws, pol, tc)
+                            : trace_batch(have, GlobalNodes<NodeD>{a.nodes}, a.n_nodes, ws, pol, tc);
     } else {
       PolD2 pol;
       pol.segs = a.segs;
@@ -639,7 +636,8 @@ __global__ void __launch_bounds__(256, 3) k_trace64(TraceArgs a) {
       pol.b[0] = sw ? xi[0] : xj[0];
       pol.b[1] = sw ? xi[1] : xj[1];
       if (have) pol.store(ws, lane, gi, gj);
-      res = trace_batch(have, nodes, a.n_nodes, ws, pol, tc);
+      res = a.nodes_in_smem ? trace_batch(have, SwizNodes<NodeD>{reinterpret_cast<const int4*>(snodes)}, a.n_nodes, ws, pol, tc)
+                            : trace_batch(have, GlobalNodes<NodeD>{a.nodes}, a.n_nodes, ws, pol, tc);
     }
     if (have && res != kHit) set_visible(Q, slot, pm, p, q);
     if (have && a.ray_log) log_ray(a, i, j, sw, p, q, res == kHit ? 2 : 1);
@@ -654,16 +652,10 @@ __global__ void __launch_bounds__(256, 3) k_trace64(TraceArgs a) {
 __global__ void __launch_bounds__(256, 4) k_trace32(TraceArgs a) {
   extern __shared__ __align__(128) unsigned char smem[];
   NodeF* snodes = reinterpret_cast<NodeF*>(smem);
-  RayBank* wsa = reinterpret_cast<RayBank*>(snodes + (a.nodes_in_smem ? a.n_nodes : 0));
+  RayBankF* wsa = reinterpret_cast<RayBankF*>(snodes + (a.nodes_in_smem ? a.n_nodes : 0));
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  RayBank& ws = wsa[warp];
-  const NodeF* nodesf = a.nodesf;
-  if (a.nodes_in_smem) {
-    const int4* src = reinterpret_cast<const int4*>(a.nodesf);
-    int4* dst = reinterpret_cast<int4*>(snodes);
-    for (int k = threadIdx.x; k < a.n_nodes * 2; k += blockDim.x) dst[k] = src[k];
-    nodesf = snodes;
-  }
+  RayBankF& ws = wsa[warp];
+  if (a.nodes_in_smem) SwizNodes<NodeF>::fill(reinterpret_cast<int4*>(snodes), a.nodesf, a.n_nodes);
   __syncthreads();
   const WaveQ& Q = a.q;
   const int pm = a.pmax;
@@ -704,7 +696,9 @@ __global__ void __launch_bounds__(256, 4) k_trace32(TraceArgs a) {
       else make_ray_f(xo, rx, ry, rz, r2, a.delta, pol.R);
       pol.store(ws, lane, a.group[i], a.group[j]);
     }
-    const int res = trace_batch(have, nodesf, a.n_nodes, ws, pol, tc);
+    const int res = a.nodes_in_smem
+                        ? trace_batch(have, SwizNodes<NodeF>{reinterpret_cast<const int4*>(snodes)}, a.n_nodes, ws, pol, tc)
+                        : trace_batch(have, GlobalNodes<NodeF>{a.nodesf}, a.n_nodes, ws, pol, tc);
     if (have && res == kMiss) set_visible(Q, slot, pm, p, q);
     if (have && a.ray_log && res != kUnsure) log_ray(a, i, j, sw, p, q, res == kHit ? 2 : 1);
     // uncertain rays go to the FP64 queue
@@ -848,7 +842,7 @@ size_t gen_smem_bytes(bool mixed, int pmax, int n_nodes_smem, bool occ) {
 }
 
 size_t trace_smem_bytes(bool fp32, int n_nodes_smem) {
-  return (size_t)n_nodes_smem * (fp32 ? sizeof(NodeF) : sizeof(NodeD)) + 8 * sizeof(RayBank);
+  return (size_t)n_nodes_smem * (fp32 ? sizeof(NodeF) : sizeof(NodeD)) + 8 * (fp32 ? sizeof(RayBankF) : sizeof(RayBank));
 }
 
 template <typename F>

@@ -263,6 +263,8 @@ int rvf_session_create(const rvf_session_opts* opts, rvf_session** out) {
   s->smem_optin = p.sharedMemPerBlockOptin;
   if ((e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking)) != cudaSuccess)
     return cuda_err(e, "cudaStreamCreate");
+  for (cudaEvent_t& v : s->ev)
+    if ((e = cudaEventCreate(&v)) != cudaSuccess) return cuda_err(e, "cudaEventCreate");
   size_t fr = 0, tot = 0;
   cudaMemGetInfo(&fr, &tot);
   s->budget = (opts && opts->hbm_budget_bytes) ? opts->hbm_budget_bytes : (size_t)(0.9 * (double)fr);
@@ -286,6 +288,8 @@ int rvf_session_destroy(rvf_session* s) {
     s->tile_counter.free_();
     s->counters.free_();
     s->wq_ctr.free_(); s->wq_rec64.free_(); s->wq_rec32.free_(); s->wq_slots.free_(); s->wq_vis.free_();
+    for (cudaEvent_t v : s->ev)
+      if (v) cudaEventDestroy(v);
     cudaStreamDestroy(s->stream);
   }
   delete s;
@@ -484,25 +488,54 @@ int rvf_solve(rvf_session* s, rvf_mesh* m, const rvf_options* o, double* F_elem,
     cudaMemsetAsync(wq.ctr, 0, sizeof(unsigned long long) * kCtrCount, s->stream);
     // chunks: each claims tiles while its queues have room, then traces and resolves them
     unsigned long long prev = 0;
+    cudaEvent_t* ev = s->ev;
     for (int chunk = 0;; ++chunk) {
+      cudaEventRecord(ev[0], s->stream);
       e = mixed ? launch_gen_mixed(x, s->sm_count, s->stream) : launch_gen_fp64(a, s->sm_count, s->stream);
       n_kernels += 1;
       if (e != cudaSuccess) return cuda_err(e, "pair generation kernel launch");
-      if (!occ) break;  // without rays one launch integrates every tile
+      cudaEventRecord(ev[1], s->stream);
+      S.n_chunks += 1;
+      if (!occ) {  // without rays one launch integrates every tile
+        cudaEventSynchronize(ev[1]);
+        float g = 0.f;
+        cudaEventElapsedTime(&g, ev[0], ev[1]);
+        S.ms_gen += g;
+        break;
+      }
       if (mixed) {
-        ta.nodes_in_smem = trace_smem_bytes(true, m->n_nodes) <= 72 * 1024;
+        ta.nodes_in_smem = trace_smem_bytes(true, m->n_nodes) <= 80 * 1024;
         if ((e = launch_trace(ta, true, s->sm_count, s->stream)) != cudaSuccess) return cuda_err(e, "FP32 trace launch");
         n_kernels += 1;
       }
+      cudaEventRecord(ev[2], s->stream);
       ta.nodes_in_smem = trace_smem_bytes(false, m->n_nodes) <= 72 * 1024;
       if ((e = launch_trace(ta, false, s->sm_count, s->stream)) != cudaSuccess) return cuda_err(e, "trace launch");
+      cudaEventRecord(ev[3], s->stream);
       if ((e = launch_resolve(ra, mixed, s->sm_count, s->stream)) != cudaSuccess) return cuda_err(e, "resolve launch");
+      cudaEventRecord(ev[4], s->stream);
       n_kernels += 2;
-      unsigned long long claimed = 0;
-      e = cudaMemcpyAsync(&claimed, wq.ctr + kCtrTile, sizeof claimed, cudaMemcpyDeviceToHost, s->stream);
+      unsigned long long cc[kCtrCount] = {};
+      e = cudaMemcpyAsync(cc, wq.ctr, sizeof cc, cudaMemcpyDeviceToHost, s->stream);
       if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
       if (e != cudaSuccess) return cuda_err(e, "pair pipeline");
       if ((rc = read_err(s))) return rc;
+      float t01 = 0.f, t12 = 0.f, t23 = 0.f, t34 = 0.f;
+      cudaEventElapsedTime(&t01, ev[0], ev[1]);
+      cudaEventElapsedTime(&t12, ev[1], ev[2]);
+      cudaEventElapsedTime(&t23, ev[2], ev[3]);
+      cudaEventElapsedTime(&t34, ev[3], ev[4]);
+      S.ms_gen += t01;
+      if (mixed) {
+        S.ms_trace += t12;
+        S.ms_trace_fp64 += t23;
+        S.n_rays_traced += (int64_t)cc[kCtrRec32];
+      } else {
+        S.ms_trace += t23;
+        S.n_rays_traced += (int64_t)cc[kCtrRec64];
+      }
+      S.ms_resolve += t34;
+      const unsigned long long claimed = cc[kCtrTile];
       if (claimed >= (unsigned long long)a.n_tiles) break;
       if (claimed == prev) return set_err(RVF_ENOMEM, "pair pipeline made no progress: ray queue too small for one tile");
       prev = claimed;
@@ -576,14 +609,14 @@ int rvf_solve(rvf_session* s, rvf_mesh* m, const rvf_options* o, double* F_elem,
     S.n_rays = (int64_t)c[1];
     S.n_rays_fp64 = mixed ? (int64_t)c[4] : (int64_t)c[1];
     S.n_pairs_fp64 = mixed ? (int64_t)c[5] : S.n_pairs;
-    S.reserved[0] = (int64_t)c[2];
-    S.reserved[1] = (int64_t)c[3];
-    S.reserved[2] = n_kernels;
-    S.reserved[3] = mixed ? (int64_t)c[6] : 0;  // grazing point pairs re-evaluated in FP64
-    S.reserved[4] = mixed ? (int64_t)c[7] : 0;  // FP32 rays with an uncertain decision
-    S.reserved[5] = mixed ? (int64_t)c[8] : 0;  // ... of which at a slab test
-    S.reserved[6] = mixed ? (int64_t)c[9] : 0;  // ... of which at a triangle test
-    S.reserved[7] = mixed ? (int64_t)c[10] : 0; // rays with a direction component below 1e-4
+    S.n_node_visits = (int64_t)c[2];
+    S.n_prim_tests = (int64_t)c[3];
+    S.n_kernels = n_kernels;
+    S.n_graze_fp64 = mixed ? (int64_t)c[6] : 0;
+    S.n_unsure_rays = mixed ? (int64_t)c[7] : 0;
+    S.n_unsure_slab = mixed ? (int64_t)c[8] : 0;
+    S.n_unsure_prim = mixed ? (int64_t)c[9] : 0;
+    S.n_unsure_dir = mixed ? (int64_t)c[10] : 0;
     if (N > 0 && m->G > 0) {
       std::vector<double> rs(N);
       cudaMemcpy(rs.data(), m->rowsum.ptr, sizeof(double) * N, cudaMemcpyDeviceToHost);

@@ -40,7 +40,7 @@ def test_exports_every_declared_symbol(lib, rvf):
 def test_version_and_defaults(lib, rvf):
     from rvf_b200 import _abi
     assert b"sm_100a" in lib.rvf_version()
-    assert lib.rvf_abi_version() == 1
+    assert lib.rvf_abi_version() == 2
     o = _abi.default_options()
     assert o.nquad == 4 and o.n_samples == 10000 and o.method == 0 and o.precision == 0
     assert o.near_field_factor == 2.0
