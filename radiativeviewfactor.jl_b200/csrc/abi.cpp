@@ -240,6 +240,9 @@ int mesh_upload(Session* s, const rvf_mesh_desc* d, rvf_mesh** out) {
       if (n.b > 8) return set_err(RVF_EINVAL, "internal: BVH leaf holds more than 8 primitives");
       n.miss = h.miss == 0 ? M : (int32_t)(h.miss - 1);
       n.pad = 0;
+      // every walk of the tree moves forward: miss links and first children lie ahead
+      if (n.miss <= k || n.miss > M || (n.b == 0 && k + 1 >= M))
+        return set_err(RVF_EINVAL, "internal: BVH node %d has a link that does not point forward", k);
     }
     m->n_nodes = M;
     m->h_nodes = nodes;

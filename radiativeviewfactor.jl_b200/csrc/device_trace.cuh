@@ -197,6 +197,7 @@ __device__ __forceinline__ int trace_batch(bool have, const Src& nodes, int n_no
         ++nl;
         k = pol.miss(nd);
       } else {
+        // miss links point forward (checked when the tree is uploaded), so k grows
         k = (s == kHit) ? k + 1 : pol.miss(nd);
       }
       if (k >= n_nodes) done = true;

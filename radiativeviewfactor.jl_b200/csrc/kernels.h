@@ -12,8 +12,8 @@ namespace rvf {
 // Wavefront pipeline state (kernels_wave.cu).
 enum : int {
   kCtrTile = 0,    // tile claims
-  kCtrResv = 1,    // reserved queue records
-  kCtrResvS = 2,   // reserved pending-pair slots
+  kCtrResv = 1,    // reserved queue records (low 38 bits) and pending-pair slots (high bits)
+  kCtrSpare = 2,
   kCtrRec64 = 3,   // records in the FP64 queue
   kCtrRec32 = 4,   // records in the FP32 queue
   kCtrSlots = 5,   // pending-pair slots in use
@@ -22,10 +22,11 @@ enum : int {
   kCtrCount = 8
 };
 
-// A pair with queued rays: internal element indices and the sum of its
-// immediately decided terms.
+// A pair with queued rays: its request (mesh) within the launch, internal
+// element indices and the sum of its immediately decided terms.
 struct PendSlot {
   int32_t i, j;
+  int32_t req, pad;
   double acc;
 };
 
@@ -92,6 +93,7 @@ struct PairArgs {
   uint8_t* ray_log;              // device, or null
   int log_pm;
   WaveQ q;                       // wavefront queues (the fused kernel ignores them)
+  int64_t tile0;                 // batched generation: first tile of this request in the launch
 };
 
 struct RedArgs {
@@ -148,6 +150,7 @@ struct MixedArgs {
   uint8_t* ray_log;
   int log_pm;
   WaveQ q;
+  int64_t tile0;
 };
 
 struct TraceArgs {
@@ -188,12 +191,61 @@ struct ResolveArgs {
   WaveQ q;
 };
 
+// One launch of the pair pipeline over the tiles of one or more requests
+// (meshes): global tile t belongs to request r when tile_base[r] <= t <
+// tile_base[r+1], and is tile t - tile_base[r] + tile0 of that request.
+// The launch blocks live in device memory so that a captured CUDA graph can
+// be replayed with new contents.
+constexpr int kMaxBatch = 64;  // requests per launch
+
+struct GenBatch {
+  const PairArgs* reqs;    // FP64 generation
+  const MixedArgs* mreqs;  // mixed generation
+  const int64_t* tile_base;
+  int n_req;
+  int pmax_max;            // shared-memory layout and queue reservation
+  int64_t total_tiles;
+  bool nodes_in_smem;      // one request only: its BVH nodes are staged in shared memory
+  const void* smem_nodes;  // NodeD (FP64) or NodeF (mixed) of that request
+  int n_nodes_smem;
+  WaveQ q;
+  unsigned long long* counters;
+  int* err;
+};
+
+struct TraceBatch {
+  const TraceArgs* reqs;
+  int n_req;
+  // one request only: its BVH staged in shared memory, per traversal precision
+  bool nodes64_in_smem, nodes32_in_smem;
+  const NodeD* smem_nodes64;
+  const NodeF* smem_nodes32;
+  int n_nodes_smem;
+  WaveQ q;
+  unsigned long long* counters;
+};
+
+struct ResolveBatch {
+  const ResolveArgs* reqs;
+  int n_req;
+  WaveQ q;
+};
+
+// Kernel shapes of one launch class (fixed within a captured graph).
+struct WaveShape {
+  bool mixed, dim3, occ;
+  int pmax_max;
+  bool gen_nodes_smem, trace64_nodes_smem, trace32_nodes_smem;
+  int n_nodes_smem;
+};
+
 size_t gen_smem_bytes(bool mixed, int pmax, int n_nodes_smem, bool occ);
 size_t trace_smem_bytes(bool fp32, int n_nodes_smem);
-cudaError_t launch_gen_fp64(const PairArgs& a, int sm_count, cudaStream_t st);
-cudaError_t launch_gen_mixed(const MixedArgs& a, int sm_count, cudaStream_t st);
-cudaError_t launch_trace(const TraceArgs& a, bool fp32, int sm_count, cudaStream_t st);
-cudaError_t launch_resolve(const ResolveArgs& a, bool mixed, int sm_count, cudaStream_t st);
+// Generation, traversal and resolve of one chunk; the batch structs are
+// device pointers.
+cudaError_t launch_gen(const WaveShape& sh, const GenBatch* g, int sm_count, cudaStream_t st);
+cudaError_t launch_trace(const WaveShape& sh, const TraceBatch* t, bool fp32, int sm_count, cudaStream_t st);
+cudaError_t launch_resolve(const WaveShape& sh, const ResolveBatch* r, int sm_count, cudaStream_t st);
 
 // A Quad8 pair sharing corner nodes (src/DuffyKernel.jl:95-115), i < j in the
 // caller's order (the reference integrates with elem_i = the lower index).

@@ -94,25 +94,43 @@ __device__ __forceinline__ void slot_alloc(const WaveQ& q, bool need, int64_t& s
   }
 }
 
+// Queue reservations: records in the low 38 bits, pending-pair slots above,
+// in one counter, so that a claim checks and takes both capacities at once.
+__device__ __forceinline__ unsigned long long resv_pack(unsigned long long recs, unsigned long long slots) {
+  return recs | (slots << 38);
+}
+
+// Gives back part of a reservation (never more than was taken).
+__device__ __forceinline__ void resv_release(const WaveQ& q, unsigned long long recs, unsigned long long slots) {
+  atomicAdd(q.ctr + kCtrResv, neg(resv_pack(recs, slots)));
+}
+
 // Block-level tile claim with worst-case queue reservation.  Returns the
-// tile, or -1 when the chunk is full or every tile is claimed.
+// tile, or -1 when the chunk's queues have no room for another tile or every
+// tile is claimed.  The reservation is a compare-and-swap that only succeeds
+// when both capacities hold, so concurrent claims never over-reserve; the
+// retry loop is bounded (a block that keeps losing the race ends its chunk).
 __device__ __forceinline__ int64_t claim_tile(const WaveQ& q, int64_t n_tiles, bool occ,
                                               unsigned long long need, unsigned long long need_s) {
   if (occ) {
-    const unsigned long long r = atomicAdd(q.ctr + kCtrResv, need);
-    const unsigned long long rs = atomicAdd(q.ctr + kCtrResvS, need_s);
-    if (r + need > (unsigned long long)q.cap || rs + need_s > (unsigned long long)q.scap) {
-      atomicAdd(q.ctr + kCtrResv, neg(need));
-      atomicAdd(q.ctr + kCtrResvS, neg(need_s));
-      return -1;
+    unsigned long long* c = q.ctr + kCtrResv;
+    unsigned long long cur = *(volatile unsigned long long*)c;
+    bool ok = false;
+    for (int it = 0; it < 4096; ++it) {
+      const unsigned long long recs = cur & ((1ull << 38) - 1), slots = cur >> 38;
+      if (recs + need > (unsigned long long)q.cap || slots + need_s > (unsigned long long)q.scap) break;
+      const unsigned long long prev = atomicCAS(c, cur, cur + resv_pack(need, need_s));
+      if (prev == cur) {
+        ok = true;
+        break;
+      }
+      cur = prev;
     }
+    if (!ok) return -1;
   }
   const int64_t t = (int64_t)atomicAdd(q.ctr + kCtrTile, 1ull);
   if (t >= n_tiles) {
-    if (occ) {
-      atomicAdd(q.ctr + kCtrResv, neg(need));
-      atomicAdd(q.ctr + kCtrResvS, neg(need_s));
-    }
+    if (occ) resv_release(q, need, need_s);
     return -1;
   }
   return t;
@@ -142,64 +160,81 @@ __device__ __forceinline__ bool pair_misses_box(const double* ci, const double* 
   return te > tx;
 }
 
+// request r of the launch with tile_base[r] <= t < tile_base[r+1]
+__device__ __forceinline__ int find_req(const int64_t* tile_base, int n_req, int64_t t) {
+  int lo = 0, hi = n_req - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (tile_base[mid] <= t) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------------------
 // 1. Generation, FP64 (surfaces and curves).
 // ---------------------------------------------------------------------------
 template <bool DIM3, bool OCC>
-__global__ void __launch_bounds__(256, 3) k_gen_fp64(PairArgs a) {
+__global__ void __launch_bounds__(256, 3) k_gen_fp64(const GenBatch* __restrict__ Lp) {
   extern __shared__ __align__(128) unsigned char smem[];
-  const int pm = a.pmax;
+  const GenBatch& L = *Lp;
+  const int pmL = L.pmax_max;
   double* iblk = reinterpret_cast<double*>(smem);
-  NodeD* snodes = reinterpret_cast<NodeD*>(iblk + kComp * pm * kTile);
-  uint64_t* stage_all = reinterpret_cast<uint64_t*>(snodes + (a.nodes_in_smem ? a.n_nodes : 0));
+  NodeD* snodes = reinterpret_cast<NodeD*>(iblk + kComp * pmL * kTile);
+  uint64_t* stage_all = reinterpret_cast<uint64_t*>(snodes + (L.nodes_in_smem ? L.n_nodes_smem : 0));
   uint64_t* bar = stage_all + (OCC ? 8 * 64 : 0);
   __shared__ int64_t s_tile;
+  __shared__ int s_req;
   __shared__ unsigned long long s_used, s_slots;
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   uint64_t* stage = stage_all + warp * 64;
-  const NodeD* nodes = a.nodes;
-  if (OCC && a.nodes_in_smem) {
-    const int4* src = reinterpret_cast<const int4*>(a.nodes);
+  if (OCC && L.nodes_in_smem) {
+    const int4* src = reinterpret_cast<const int4*>(L.smem_nodes);
     int4* dst = reinterpret_cast<int4*>(snodes);
-    for (int k = threadIdx.x; k < a.n_nodes * 4; k += blockDim.x) dst[k] = src[k];
-    nodes = snodes;
+    for (int k = threadIdx.x; k < L.n_nodes_smem * 4; k += blockDim.x) dst[k] = src[k];
   }
   if (threadIdx.x == 0) mbar_init(bar, 1);
   __syncthreads();
 
-  const WaveQ& Q = a.q;
-  const unsigned long long need = (unsigned long long)kTile * kTile * pm * pm, need_s = kTile * kTile;
-  const uint32_t blk_bytes = (uint32_t)(kComp * pm * kTile * sizeof(double));
+  const WaveQ& Q = L.q;
+  const unsigned long long need = (unsigned long long)kTile * kTile * pmL * pmL, need_s = kTile * kTile;
   uint32_t phase = 0;
   uint32_t n_rays = 0, n_pp = 0;
   for (;;) {
     if (threadIdx.x == 0) {
-      s_tile = claim_tile(Q, a.n_tiles, OCC, need, need_s);
+      const int64_t g = claim_tile(Q, L.total_tiles, OCC, need, need_s);
       s_used = 0;
       s_slots = 0;
-      if (s_tile >= 0) {
+      s_tile = -1;
+      if (g >= 0) {
+        const int r = find_req(L.tile_base, L.n_req, g);
+        const PairArgs& a = L.reqs[r];
+        s_req = r;
+        s_tile = g - L.tile_base[r] + a.tile0;
         int64_t bi, bj;
         tile_coords(s_tile, a.nT, bi, bj);
+        const uint32_t blk_bytes = (uint32_t)(kComp * a.pmax * kTile * sizeof(double));
         mbar_expect_tx(bar, blk_bytes);
-        bulk_g2s(iblk, a.tab + bi * kComp * pm * kTile, blk_bytes, bar);
+        bulk_g2s(iblk, a.tab + bi * kComp * a.pmax * kTile, blk_bytes, bar);
       }
     }
     __syncthreads();
     const int64_t t = s_tile;
     if (t < 0) break;
+    const int req = s_req;
+    const PairArgs& a = L.reqs[req];
+    const int pm = a.pmax;
+    const NodeD* nodes = L.nodes_in_smem ? snodes : a.nodes;
     int64_t bi, bj;
     tile_coords(t, a.nT, bi, bj);
     const bool ok = mbar_wait_bounded(bar, phase);
     if (__syncthreads_or(!ok)) {
       if (threadIdx.x == 0) {
-        atomicOr(a.err, kErrWaitTimeout);
-        if (OCC) {  // give the whole reservation back
-          atomicAdd(Q.ctr + kCtrResv, neg(need));
-          atomicAdd(Q.ctr + kCtrResvS, neg(need_s));
-        }
+        atomicOr(L.err, kErrWaitTimeout);
+        if (OCC) resv_release(Q, need, need_s);  // give the whole reservation back
       }
       break;
     }
@@ -301,6 +336,8 @@ __global__ void __launch_bounds__(256, 3) k_gen_fp64(PairArgs a) {
         PendSlot ps;
         ps.i = (int32_t)i;
         ps.j = (int32_t)j;
+        ps.req = req;
+        ps.pad = 0;
         ps.acc = acc;
         Q.slots[slot] = ps;
       } else if (valid) {
@@ -312,15 +349,12 @@ __global__ void __launch_bounds__(256, 3) k_gen_fp64(PairArgs a) {
       }
     }
     __syncthreads();
-    if (OCC && threadIdx.x == 0) {  // keep only what the tile used
-      atomicAdd(Q.ctr + kCtrResv, neg(need - s_used));
-      atomicAdd(Q.ctr + kCtrResvS, neg(need_s - s_slots));
-    }
+    if (OCC && threadIdx.x == 0) resv_release(Q, need - s_used, need_s - s_slots);  // keep what the tile used
   }
   const uint64_t s_rays = warp_sum_u64(n_rays), s_pp = warp_sum_u64(n_pp);
-  if (lane == 0 && a.counters) {
-    atomicAdd(a.counters + 0, s_pp);
-    atomicAdd(a.counters + 1, s_rays);
+  if (lane == 0 && L.counters) {
+    atomicAdd(L.counters + 0, s_pp);
+    atomicAdd(L.counters + 1, s_rays);
   }
 }
 
@@ -372,59 +406,65 @@ __device__ __noinline__ void gen_mixed64(const MixedArgs& a, const NodeD* nodes,
 }
 
 template <bool OCC>
-__global__ void __launch_bounds__(256, 2) k_gen_mixed(MixedArgs a) {
+__global__ void __launch_bounds__(256, 2) k_gen_mixed(const GenBatch* __restrict__ Lp) {
   extern __shared__ __align__(128) unsigned char smem[];
-  const int pm = a.pmax;
+  const GenBatch& L = *Lp;
+  const int pmL = L.pmax_max;
   float* iblk = reinterpret_cast<float*>(smem);
-  NodeF* snodes = reinterpret_cast<NodeF*>(smem + (size_t)kComp * pm * kTile * sizeof(float));
-  uint64_t* stage_all = reinterpret_cast<uint64_t*>(snodes + (a.nodesf_in_smem ? a.n_nodes : 0));
+  NodeF* snodes = reinterpret_cast<NodeF*>(smem + (size_t)kComp * pmL * kTile * sizeof(float));
+  uint64_t* stage_all = reinterpret_cast<uint64_t*>(snodes + (L.nodes_in_smem ? L.n_nodes_smem : 0));
   uint64_t* bar = stage_all + (OCC ? 8 * 128 : 0);
   __shared__ int64_t s_tile;
+  __shared__ int s_req;
   __shared__ unsigned long long s_used, s_slots;
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   uint64_t* st64 = stage_all + warp * 128;
   uint64_t* st32 = st64 + 64;
-  const NodeF* nodesf = a.nodesf;
-  if (OCC && a.nodesf_in_smem) {
-    const int4* src = reinterpret_cast<const int4*>(a.nodesf);
+  if (OCC && L.nodes_in_smem) {
+    const int4* src = reinterpret_cast<const int4*>(L.smem_nodes);
     int4* dst = reinterpret_cast<int4*>(snodes);
-    for (int k = threadIdx.x; k < a.n_nodes * 2; k += blockDim.x) dst[k] = src[k];
-    nodesf = snodes;
+    for (int k = threadIdx.x; k < L.n_nodes_smem * 2; k += blockDim.x) dst[k] = src[k];
   }
   if (threadIdx.x == 0) mbar_init(bar, 1);
   __syncthreads();
 
-  const WaveQ& Q = a.q;
-  const unsigned long long need = (unsigned long long)kTile * kTile * pm * pm, need_s = kTile * kTile;
-  const uint32_t blk_bytes = (uint32_t)(kComp * pm * kTile * sizeof(float));
+  const WaveQ& Q = L.q;
+  const unsigned long long need = (unsigned long long)kTile * kTile * pmL * pmL, need_s = kTile * kTile;
   uint32_t phase = 0;
   uint32_t n_pp = 0, n_rays = 0, n_rays64 = 0, n_near = 0, n_graze = 0, n_baddir = 0;
   for (;;) {
     if (threadIdx.x == 0) {
-      s_tile = claim_tile(Q, a.n_tiles, OCC, need, need_s);
+      const int64_t g = claim_tile(Q, L.total_tiles, OCC, need, need_s);
       s_used = 0;
       s_slots = 0;
-      if (s_tile >= 0) {
+      s_tile = -1;
+      if (g >= 0) {
+        const int r = find_req(L.tile_base, L.n_req, g);
+        const MixedArgs& a = L.mreqs[r];
+        s_req = r;
+        s_tile = g - L.tile_base[r] + a.tile0;
         int64_t bi, bj;
         tile_coords(s_tile, a.nT, bi, bj);
+        const uint32_t blk_bytes = (uint32_t)(kComp * a.pmax * kTile * sizeof(float));
         mbar_expect_tx(bar, blk_bytes);
-        bulk_g2s(iblk, a.tabf + bi * kComp * pm * kTile, blk_bytes, bar);
+        bulk_g2s(iblk, a.tabf + bi * kComp * a.pmax * kTile, blk_bytes, bar);
       }
     }
     __syncthreads();
     const int64_t t = s_tile;
     if (t < 0) break;
+    const int req = s_req;
+    const MixedArgs& a = L.mreqs[req];
+    const int pm = a.pmax;
+    const NodeF* nodesf = L.nodes_in_smem ? snodes : a.nodesf;
     int64_t bi, bj;
     tile_coords(t, a.nT, bi, bj);
     const bool ok = mbar_wait_bounded(bar, phase);
     if (__syncthreads_or(!ok)) {
       if (threadIdx.x == 0) {
-        atomicOr(a.err, kErrWaitTimeout);
-        if (OCC) {
-          atomicAdd(Q.ctr + kCtrResv, neg(need));
-          atomicAdd(Q.ctr + kCtrResvS, neg(need_s));
-        }
+        atomicOr(L.err, kErrWaitTimeout);
+        if (OCC) resv_release(Q, need, need_s);
       }
       break;
     }
@@ -538,6 +578,8 @@ __global__ void __launch_bounds__(256, 2) k_gen_mixed(MixedArgs a) {
         PendSlot ps;
         ps.i = (int32_t)i;
         ps.j = (int32_t)j;
+        ps.req = req;
+        ps.pad = 0;
         ps.acc = raw;
         Q.slots[slot] = ps;
       } else if (valid) {
@@ -548,20 +590,17 @@ __global__ void __launch_bounds__(256, 2) k_gen_mixed(MixedArgs a) {
       }
     }
     __syncthreads();
-    if (OCC && threadIdx.x == 0) {
-      atomicAdd(Q.ctr + kCtrResv, neg(need - s_used));
-      atomicAdd(Q.ctr + kCtrResvS, neg(need_s - s_slots));
-    }
+    if (OCC && threadIdx.x == 0) resv_release(Q, need - s_used, need_s - s_slots);
   }
   const uint64_t s_pp = warp_sum_u64(n_pp), s_rays = warp_sum_u64(n_rays), s_r64 = warp_sum_u64(n_rays64),
                  s_near = warp_sum_u64(n_near), s_graze = warp_sum_u64(n_graze), s_bad = warp_sum_u64(n_baddir);
-  if (lane == 0 && a.counters) {
-    atomicAdd(a.counters + 0, s_pp);
-    atomicAdd(a.counters + 1, s_rays);
-    atomicAdd(a.counters + 4, s_r64);
-    atomicAdd(a.counters + 5, s_near);
-    atomicAdd(a.counters + 6, s_graze);
-    atomicAdd(a.counters + 10, s_bad);
+  if (lane == 0 && L.counters) {
+    atomicAdd(L.counters + 0, s_pp);
+    atomicAdd(L.counters + 1, s_rays);
+    atomicAdd(L.counters + 4, s_r64);
+    atomicAdd(L.counters + 5, s_near);
+    atomicAdd(L.counters + 6, s_graze);
+    atomicAdd(L.counters + 10, s_bad);
   }
 }
 
@@ -579,17 +618,38 @@ __device__ __forceinline__ void set_visible(const WaveQ& Q, int64_t slot, int pm
   atomicOr(reinterpret_cast<unsigned long long*>(Q.vis + slot * Q.vis_words + (b >> 6)), 1ull << (b & 63));
 }
 
+// A queued ray: its record, its pair and its request.
+struct QRay {
+  int64_t slot, i, j;
+  int p, q, req;
+  bool sw;
+};
+
+__device__ __forceinline__ QRay read_ray(const WaveQ& Q, uint64_t r) {
+  QRay x;
+  x.slot = rec_slot(r);
+  x.sw = rec_sw(r);
+  x.p = rec_p(r);
+  x.q = rec_q(r);
+  const PendSlot ps = Q.slots[x.slot];
+  x.i = ps.i;
+  x.j = ps.j;
+  x.req = ps.req;
+  return x;
+}
+
 template <bool DIM3>
-__global__ void __launch_bounds__(256, 3) k_trace64(TraceArgs a) {
+__global__ void __launch_bounds__(256, 3) k_trace64(const TraceBatch* __restrict__ Lp) {
   extern __shared__ __align__(128) unsigned char smem[];
+  const TraceBatch& L = *Lp;
   NodeD* snodes = reinterpret_cast<NodeD*>(smem);
-  RayBank* wsa = reinterpret_cast<RayBank*>(snodes + (a.nodes_in_smem ? a.n_nodes : 0));
+  const bool in_smem = L.nodes64_in_smem;
+  RayBank* wsa = reinterpret_cast<RayBank*>(snodes + (in_smem ? L.n_nodes_smem : 0));
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   RayBank& ws = wsa[warp];
-  if (a.nodes_in_smem) SwizNodes<NodeD>::fill(reinterpret_cast<int4*>(snodes), a.nodes, a.n_nodes);
+  if (in_smem) SwizNodes<NodeD>::fill(reinterpret_cast<int4*>(snodes), L.smem_nodes64, L.n_nodes_smem);
   __syncthreads();
-  const WaveQ& Q = a.q;
-  const int pm = a.pmax;
+  const WaveQ& Q = L.q;
   const unsigned long long n = *(volatile unsigned long long*)(Q.ctr + kCtrRec64);
   TravCount tc;
   for (;;) {
@@ -598,23 +658,17 @@ __global__ void __launch_bounds__(256, 3) k_trace64(TraceArgs a) {
     base = __shfl_sync(kFull, base, 0);
     if (base >= n) break;
     const bool have = base + lane < n;
-    const uint64_t r = have ? Q.rec64[base + lane] : 0ull;
-    const int64_t slot = rec_slot(r);
-    const bool sw = rec_sw(r);
-    const int p = rec_p(r), q = rec_q(r);
-    int64_t i = 0, j = 0;
-    if (have) {
-      const PendSlot ps = Q.slots[slot];
-      i = ps.i;
-      j = ps.j;
-    }
+    const QRay x = have ? read_ray(Q, Q.rec64[base + lane]) : QRay{0, 0, 0, 0, 0, 0, false};
+    const TraceArgs& a = L.reqs[x.req];
+    const int pm = a.pmax;
     double xi[3], xj[3];
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-      xi[c] = have ? a.tab[tab_at(i, c, p, pm)] : 0.0;
-      xj[c] = have ? a.tab[tab_at(j, c, q, pm)] : 0.0;
+      xi[c] = have ? a.tab[tab_at(x.i, c, x.p, pm)] : 0.0;
+      xj[c] = have ? a.tab[tab_at(x.j, c, x.q, pm)] : 0.0;
     }
-    const int32_t gi = have ? a.group[i] : 0, gj = have ? a.group[j] : 0;
+    const int32_t gi = have ? a.group[x.i] : 0, gj = have ? a.group[x.j] : 0;
+    const int n_nodes = have ? a.n_nodes : 0;
     int res;
     if (DIM3) {
       PolD3 pol;
@@ -622,43 +676,44 @@ __global__ void __launch_bounds__(256, 3) k_trace64(TraceArgs a) {
       const double rx = xj[0] - xi[0], ry = xj[1] - xi[1], rz = xj[2] - xi[2];
       const double r2 = (rx * rx + ry * ry) + rz * rz;
       if (have) {
-        if (sw) make_ray(xj, -rx, -ry, -rz, r2, pol.R);
+        if (x.sw) make_ray(xj, -rx, -ry, -rz, r2, pol.R);
         else make_ray(xi, rx, ry, rz, r2, pol.R);
         pol.store(ws, lane, gi, gj);
       }
-      res = a.nodes_in_smem ? trace_batch(have, SwizNodes<NodeD>{reinterpret_cast<const int4*>(snodes)}, a.n_nodes, ws, pol, tc)
-                            : trace_batch(have, GlobalNodes<NodeD>{a.nodes}, a.n_nodes, ws, pol, tc);
+      res = in_smem ? trace_batch(have, SwizNodes<NodeD>{reinterpret_cast<const int4*>(snodes)}, n_nodes, ws, pol, tc)
+                            : trace_batch(have, GlobalNodes<NodeD>{a.nodes}, n_nodes, ws, pol, tc);
     } else {
       PolD2 pol;
       pol.segs = a.segs;
-      pol.a[0] = sw ? xj[0] : xi[0];
-      pol.a[1] = sw ? xj[1] : xi[1];
-      pol.b[0] = sw ? xi[0] : xj[0];
-      pol.b[1] = sw ? xi[1] : xj[1];
+      pol.a[0] = x.sw ? xj[0] : xi[0];
+      pol.a[1] = x.sw ? xj[1] : xi[1];
+      pol.b[0] = x.sw ? xi[0] : xj[0];
+      pol.b[1] = x.sw ? xi[1] : xj[1];
       if (have) pol.store(ws, lane, gi, gj);
-      res = a.nodes_in_smem ? trace_batch(have, SwizNodes<NodeD>{reinterpret_cast<const int4*>(snodes)}, a.n_nodes, ws, pol, tc)
-                            : trace_batch(have, GlobalNodes<NodeD>{a.nodes}, a.n_nodes, ws, pol, tc);
+      res = in_smem ? trace_batch(have, SwizNodes<NodeD>{reinterpret_cast<const int4*>(snodes)}, n_nodes, ws, pol, tc)
+                            : trace_batch(have, GlobalNodes<NodeD>{a.nodes}, n_nodes, ws, pol, tc);
     }
-    if (have && res != kHit) set_visible(Q, slot, pm, p, q);
-    if (have && a.ray_log) log_ray(a, i, j, sw, p, q, res == kHit ? 2 : 1);
+    if (have && res != kHit) set_visible(Q, x.slot, pm, x.p, x.q);
+    if (have && a.ray_log) log_ray(a, x.i, x.j, x.sw, x.p, x.q, res == kHit ? 2 : 1);
   }
   const uint64_t s_nodes = warp_sum_u64(tc.nodes), s_prims = warp_sum_u64(tc.prims);
-  if (lane == 0 && a.counters) {
-    atomicAdd(a.counters + 2, s_nodes);
-    atomicAdd(a.counters + 3, s_prims);
+  if (lane == 0 && L.counters) {
+    atomicAdd(L.counters + 2, s_nodes);
+    atomicAdd(L.counters + 3, s_prims);
   }
 }
 
-__global__ void __launch_bounds__(256, 4) k_trace32(TraceArgs a) {
+__global__ void __launch_bounds__(256, 4) k_trace32(const TraceBatch* __restrict__ Lp) {
   extern __shared__ __align__(128) unsigned char smem[];
+  const TraceBatch& L = *Lp;
   NodeF* snodes = reinterpret_cast<NodeF*>(smem);
-  RayBankF* wsa = reinterpret_cast<RayBankF*>(snodes + (a.nodes_in_smem ? a.n_nodes : 0));
+  const bool in_smem = L.nodes32_in_smem;
+  RayBankF* wsa = reinterpret_cast<RayBankF*>(snodes + (in_smem ? L.n_nodes_smem : 0));
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   RayBankF& ws = wsa[warp];
-  if (a.nodes_in_smem) SwizNodes<NodeF>::fill(reinterpret_cast<int4*>(snodes), a.nodesf, a.n_nodes);
+  if (in_smem) SwizNodes<NodeF>::fill(reinterpret_cast<int4*>(snodes), L.smem_nodes32, L.n_nodes_smem);
   __syncthreads();
-  const WaveQ& Q = a.q;
-  const int pm = a.pmax;
+  const WaveQ& Q = L.q;
   const unsigned long long n = *(volatile unsigned long long*)(Q.ctr + kCtrRec32);
   TravCount tc;
   uint32_t n_unsure = 0;
@@ -668,27 +723,25 @@ __global__ void __launch_bounds__(256, 4) k_trace32(TraceArgs a) {
     base = __shfl_sync(kFull, base, 0);
     if (base >= n) break;
     const bool have = base + lane < n;
-    const uint64_t r = have ? Q.rec32[base + lane] : 0ull;
-    const int64_t slot = rec_slot(r);
-    const bool sw = rec_sw(r);
-    const int p = rec_p(r), q = rec_q(r);
-    int64_t i = 0, j = 0;
-    if (have) {
-      const PendSlot ps = Q.slots[slot];
-      i = ps.i;
-      j = ps.j;
-    }
+    const uint64_t rec = have ? Q.rec32[base + lane] : 0ull;
+    const QRay x = have ? read_ray(Q, rec) : QRay{0, 0, 0, 0, 0, 0, false};
+    const TraceArgs& a = L.reqs[x.req];
+    const int pm = a.pmax;
     PolF3 pol;
     pol.tris = a.trisf;
     if (have) {
       // the generation's FP32 ray, operation for operation
+      const int64_t i = x.i, j = x.j;
+      const bool sw = x.sw;
       const double ci0 = a.cen[3 * i], ci1 = a.cen[3 * i + 1], ci2 = a.cen[3 * i + 2];
       const double dc0 = a.cen[3 * j] - ci0, dc1 = a.cen[3 * j + 1] - ci1, dc2 = a.cen[3 * j + 2] - ci2;
       const float d0 = (float)dc0, d1 = (float)dc1, d2 = (float)dc2;
       const float an0 = (float)(ci0 + (sw ? dc0 : 0.0)), an1 = (float)(ci1 + (sw ? dc1 : 0.0)),
                   an2 = (float)(ci2 + (sw ? dc2 : 0.0));
-      const float op0 = a.tabf[tab_at(i, 0, p, pm)], op1 = a.tabf[tab_at(i, 1, p, pm)], op2 = a.tabf[tab_at(i, 2, p, pm)];
-      const float oq0 = a.tabf[tab_at(j, 0, q, pm)], oq1 = a.tabf[tab_at(j, 1, q, pm)], oq2 = a.tabf[tab_at(j, 2, q, pm)];
+      const float op0 = a.tabf[tab_at(i, 0, x.p, pm)], op1 = a.tabf[tab_at(i, 1, x.p, pm)],
+                  op2 = a.tabf[tab_at(i, 2, x.p, pm)];
+      const float oq0 = a.tabf[tab_at(j, 0, x.q, pm)], oq1 = a.tabf[tab_at(j, 1, x.q, pm)],
+                  oq2 = a.tabf[tab_at(j, 2, x.q, pm)];
       const float rx = d0 + (oq0 - op0), ry = d1 + (oq1 - op1), rz = d2 + (oq2 - op2);
       const float r2 = fmaf(rx, rx, fmaf(ry, ry, rz * rz));
       const float xo[3] = {an0 + (sw ? oq0 : op0), an1 + (sw ? oq1 : op1), an2 + (sw ? oq2 : op2)};
@@ -696,11 +749,12 @@ __global__ void __launch_bounds__(256, 4) k_trace32(TraceArgs a) {
       else make_ray_f(xo, rx, ry, rz, r2, a.delta, pol.R);
       pol.store(ws, lane, a.group[i], a.group[j]);
     }
-    const int res = a.nodes_in_smem
-                        ? trace_batch(have, SwizNodes<NodeF>{reinterpret_cast<const int4*>(snodes)}, a.n_nodes, ws, pol, tc)
-                        : trace_batch(have, GlobalNodes<NodeF>{a.nodesf}, a.n_nodes, ws, pol, tc);
-    if (have && res == kMiss) set_visible(Q, slot, pm, p, q);
-    if (have && a.ray_log && res != kUnsure) log_ray(a, i, j, sw, p, q, res == kHit ? 2 : 1);
+    const int n_nodes = have ? a.n_nodes : 0;
+    const int res = in_smem
+                        ? trace_batch(have, SwizNodes<NodeF>{reinterpret_cast<const int4*>(snodes)}, n_nodes, ws, pol, tc)
+                        : trace_batch(have, GlobalNodes<NodeF>{a.nodesf}, n_nodes, ws, pol, tc);
+    if (have && res == kMiss) set_visible(Q, x.slot, pm, x.p, x.q);
+    if (have && a.ray_log && res != kUnsure) log_ray(a, x.i, x.j, x.sw, x.p, x.q, res == kHit ? 2 : 1);
     // uncertain rays go to the FP64 queue
     const bool uns = have && res == kUnsure;
     const uint32_t m = __ballot_sync(kFull, uns);
@@ -708,20 +762,20 @@ __global__ void __launch_bounds__(256, 4) k_trace32(TraceArgs a) {
       unsigned long long b64 = 0;
       if (lane == 0) b64 = atomicAdd(Q.ctr + kCtrRec64, (unsigned long long)__popc(m));
       b64 = __shfl_sync(kFull, b64, 0);
-      if (uns) Q.rec64[b64 + __popc(m & lanemask_lt())] = r;
+      if (uns) Q.rec64[b64 + __popc(m & lanemask_lt())] = rec;
     }
     n_unsure += uns ? 1 : 0;
   }
   const uint64_t s_nodes = warp_sum_u64(tc.nodes), s_prims = warp_sum_u64(tc.prims),
                  s_us = warp_sum_u64(tc.unsure_slab), s_up = warp_sum_u64(tc.unsure_prim),
                  s_un = warp_sum_u64(n_unsure);
-  if (lane == 0 && a.counters) {
-    atomicAdd(a.counters + 2, s_nodes);
-    atomicAdd(a.counters + 3, s_prims);
-    atomicAdd(a.counters + 4, s_un);
-    atomicAdd(a.counters + 7, s_un);
-    atomicAdd(a.counters + 8, s_us);
-    atomicAdd(a.counters + 9, s_up);
+  if (lane == 0 && L.counters) {
+    atomicAdd(L.counters + 2, s_nodes);
+    atomicAdd(L.counters + 3, s_prims);
+    atomicAdd(L.counters + 4, s_un);
+    atomicAdd(L.counters + 7, s_un);
+    atomicAdd(L.counters + 8, s_us);
+    atomicAdd(L.counters + 9, s_up);
   }
 }
 
@@ -729,13 +783,14 @@ __global__ void __launch_bounds__(256, 4) k_trace32(TraceArgs a) {
 // 3. Resolve: one thread per pending pair.
 // ---------------------------------------------------------------------------
 template <bool DIM3>
-__global__ void __launch_bounds__(256) k_resolve64(ResolveArgs a) {
-  const WaveQ& Q = a.q;
+__global__ void __launch_bounds__(256) k_resolve64(const ResolveBatch* __restrict__ Lp) {
+  const WaveQ& Q = Lp->q;
   const unsigned long long ns = *(volatile unsigned long long*)(Q.ctr + kCtrSlots);
-  const int pm = a.pmax;
   for (unsigned long long s = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; s < ns;
        s += (unsigned long long)gridDim.x * blockDim.x) {
     const PendSlot ps = Q.slots[s];
+    const ResolveArgs& a = Lp->reqs[ps.req];
+    const int pm = a.pmax;
     const int64_t i = ps.i, j = ps.j;
     double raw = ps.acc;
     for (int w = 0; w < Q.vis_words; ++w) {
@@ -765,13 +820,14 @@ __global__ void __launch_bounds__(256) k_resolve64(ResolveArgs a) {
   }
 }
 
-__global__ void __launch_bounds__(256) k_resolve_mixed(ResolveArgs a) {
-  const WaveQ& Q = a.q;
+__global__ void __launch_bounds__(256) k_resolve_mixed(const ResolveBatch* __restrict__ Lp) {
+  const WaveQ& Q = Lp->q;
   const unsigned long long ns = *(volatile unsigned long long*)(Q.ctr + kCtrSlots);
-  const int pm = a.pmax;
   for (unsigned long long s = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; s < ns;
        s += (unsigned long long)gridDim.x * blockDim.x) {
     const PendSlot ps = Q.slots[s];
+    const ResolveArgs& a = Lp->reqs[ps.req];
+    const int pm = a.pmax;
     const int64_t i = ps.i, j = ps.j;
     double raw = ps.acc;
     // the generation's near-field and FP32 quantities, operation for operation
@@ -858,55 +914,39 @@ static int grid_for(F fn, size_t smem, int sm_count, int cap) {
   return sm_count * per_sm;
 }
 
-cudaError_t launch_gen_fp64(const PairArgs& a, int sm_count, cudaStream_t st) {
-  const bool occ = a.n_nodes > 0;
-  const size_t smem = gen_smem_bytes(false, a.pmax, a.nodes_in_smem ? a.n_nodes : 0, occ);
+cudaError_t launch_gen(const WaveShape& sh, const GenBatch* g, int sm_count, cudaStream_t st) {
+  const size_t smem = gen_smem_bytes(sh.mixed, sh.pmax_max, sh.gen_nodes_smem ? sh.n_nodes_smem : 0, sh.occ);
   auto launch = [&](auto fn) -> cudaError_t {
     cudaError_t e = set_smem(fn, smem);
     if (e != cudaSuccess) return e;
-    int64_t grid = grid_for(fn, smem, sm_count, 4);
-    if (grid > a.n_tiles) grid = a.n_tiles;
-    if (grid < 1) grid = 1;
-    fn<<<(unsigned)grid, 256, smem, st>>>(a);
+    const int grid = grid_for(fn, smem, sm_count, 4);
+    fn<<<(unsigned)grid, 256, smem, st>>>(g);
     return cudaGetLastError();
   };
-  if (a.dim3) return occ ? launch(k_gen_fp64<true, true>) : launch(k_gen_fp64<true, false>);
-  return occ ? launch(k_gen_fp64<false, true>) : launch(k_gen_fp64<false, false>);
+  if (sh.mixed) return sh.occ ? launch(k_gen_mixed<true>) : launch(k_gen_mixed<false>);
+  if (sh.dim3) return sh.occ ? launch(k_gen_fp64<true, true>) : launch(k_gen_fp64<true, false>);
+  return sh.occ ? launch(k_gen_fp64<false, true>) : launch(k_gen_fp64<false, false>);
 }
 
-cudaError_t launch_gen_mixed(const MixedArgs& a, int sm_count, cudaStream_t st) {
-  const bool occ = a.n_nodes > 0;
-  const size_t smem = gen_smem_bytes(true, a.pmax, a.nodesf_in_smem ? a.n_nodes : 0, occ);
-  auto launch = [&](auto fn) -> cudaError_t {
-    cudaError_t e = set_smem(fn, smem);
-    if (e != cudaSuccess) return e;
-    int64_t grid = grid_for(fn, smem, sm_count, 4);
-    if (grid > a.n_tiles) grid = a.n_tiles;
-    if (grid < 1) grid = 1;
-    fn<<<(unsigned)grid, 256, smem, st>>>(a);
-    return cudaGetLastError();
-  };
-  return occ ? launch(k_gen_mixed<true>) : launch(k_gen_mixed<false>);
-}
-
-cudaError_t launch_trace(const TraceArgs& a, bool fp32, int sm_count, cudaStream_t st) {
-  const size_t smem = trace_smem_bytes(fp32, a.nodes_in_smem ? a.n_nodes : 0);
+cudaError_t launch_trace(const WaveShape& sh, const TraceBatch* t, bool fp32, int sm_count, cudaStream_t st) {
+  const bool in_smem = fp32 ? sh.trace32_nodes_smem : sh.trace64_nodes_smem;
+  const size_t smem = trace_smem_bytes(fp32, in_smem ? sh.n_nodes_smem : 0);
   auto launch = [&](auto fn) -> cudaError_t {
     cudaError_t e = set_smem(fn, smem);
     if (e != cudaSuccess) return e;
     const int grid = grid_for(fn, smem, sm_count, 8);
-    fn<<<(unsigned)grid, 256, smem, st>>>(a);
+    fn<<<(unsigned)grid, 256, smem, st>>>(t);
     return cudaGetLastError();
   };
   if (fp32) return launch(k_trace32);
-  return a.dim3 ? launch(k_trace64<true>) : launch(k_trace64<false>);
+  return sh.dim3 ? launch(k_trace64<true>) : launch(k_trace64<false>);
 }
 
-cudaError_t launch_resolve(const ResolveArgs& a, bool mixed, int sm_count, cudaStream_t st) {
+cudaError_t launch_resolve(const WaveShape& sh, const ResolveBatch* r, int sm_count, cudaStream_t st) {
   const int grid = sm_count * 8;
-  if (mixed) k_resolve_mixed<<<grid, 256, 0, st>>>(a);
-  else if (a.dim3) k_resolve64<true><<<grid, 256, 0, st>>>(a);
-  else k_resolve64<false><<<grid, 256, 0, st>>>(a);
+  if (sh.mixed) k_resolve_mixed<<<grid, 256, 0, st>>>(r);
+  else if (sh.dim3) k_resolve64<true><<<grid, 256, 0, st>>>(r);
+  else k_resolve64<false><<<grid, 256, 0, st>>>(r);
   return cudaGetLastError();
 }
 

@@ -61,8 +61,12 @@ struct rvf_session {
   rvf::DevBuf err;           // int
   rvf::DevBuf tile_counter;  // u64
   rvf::DevBuf counters;      // u64 x 8
-  // wavefront pair pipeline (kernels_wave.cu)
+  // wavefront pair pipeline (kernels_wave.cu, wave_host.cpp): queues,
+  // device launch blocks, pinned counter readback, graphs per launch shape
   rvf::DevBuf wq_ctr, wq_rec64, wq_rec32, wq_slots, wq_vis;
+  rvf::DevBuf wl_pair, wl_mixed, wl_trace, wl_resolve, wl_tilebase, wl_gen, wl_tb, wl_rb;
+  unsigned long long* h_ctr = nullptr;
+  std::map<uint64_t, cudaGraphExec_t> graphs;
   std::set<rvf_mesh*> meshes;
   cudaEvent_t ev[8] = {};
 };

@@ -9,6 +9,7 @@
 
 #include "../../include/rvf_b200.h"
 #include "kernels.h"
+#include "wave_host.h"
 #include "rvf_internal.h"
 
 using namespace rvf;
@@ -91,54 +92,6 @@ int run_reduce(Session* s, rvf_mesh* m, const double* area) {
   r.Agroup = m->Agroup.as<double>();
   cudaError_t e = launch_reduce(r, s->stream);
   return e == cudaSuccess ? RVF_OK : cuda_err(e, "reduction kernels");
-}
-
-// Ray queues of the wavefront pipeline, kept by the session and grown on
-// demand.  Capacity: every point pair of every tile when that is small,
-// otherwise up to 2^29 records per queue (4 GiB) within the HBM budget, and
-// never below a few tiles' worst case.
-int ensure_wave(Session* s, bool two_queues, bool occ, int pmax, int64_t n_tiles, WaveQ& q) {
-  int rc = 0;
-  if (!s->wq_ctr.ptr && (rc = s->wq_ctr.alloc(s, sizeof(unsigned long long) * kCtrCount))) return rc;
-  q = WaveQ{};
-  q.ctr = s->wq_ctr.as<unsigned long long>();
-  q.vis_words = (pmax * pmax + 63) / 64;
-  if (!occ) return 0;
-  const int64_t per_tile = (int64_t)kTile * kTile * pmax * pmax;
-  const int64_t want = std::min<int64_t>(n_tiles * per_tile, (int64_t)1 << 29);
-  const int64_t floor_recs = std::min<int64_t>(n_tiles * per_tile, 4 * per_tile);
-  const int64_t want_s = std::min<int64_t>(n_tiles * kTile * kTile, (int64_t)1 << 25);
-  const int64_t floor_s = std::min<int64_t>(n_tiles * kTile * kTile, 4 * kTile * kTile);
-  const int nq = two_queues ? 2 : 1;
-  const size_t slot_bytes = sizeof(PendSlot) + sizeof(unsigned long long) * q.vis_words;
-  auto have = [&](int64_t recs, int64_t slots) {
-    return s->wq_rec64.bytes >= sizeof(uint64_t) * recs && (!two_queues || s->wq_rec32.bytes >= sizeof(uint64_t) * recs) &&
-           s->wq_slots.bytes >= sizeof(PendSlot) * slots &&
-           s->wq_vis.bytes >= sizeof(unsigned long long) * q.vis_words * slots;
-  };
-  int64_t recs = want, slots = want_s;
-  if (!have(recs, slots)) {
-    // release and size against the budget left
-    s->wq_rec64.free_(); s->wq_rec32.free_(); s->wq_slots.free_(); s->wq_vis.free_();
-    const size_t left = s->budget > s->used ? s->budget - s->used : 0;
-    while ((size_t)(recs * 8 * nq) + (size_t)slots * slot_bytes > left / 2 && (recs > floor_recs || slots > floor_s)) {
-      recs = std::max<int64_t>(floor_recs, recs / 2);
-      slots = std::max<int64_t>(floor_s, slots / 2);
-    }
-    if ((rc = s->wq_rec64.alloc(s, sizeof(uint64_t) * recs))) return rc;
-    if (two_queues && (rc = s->wq_rec32.alloc(s, sizeof(uint64_t) * recs))) return rc;
-    if ((rc = s->wq_slots.alloc(s, sizeof(PendSlot) * slots))) return rc;
-    if ((rc = s->wq_vis.alloc(s, sizeof(unsigned long long) * q.vis_words * slots))) return rc;
-  }
-  q.rec64 = s->wq_rec64.as<uint64_t>();
-  q.rec32 = two_queues ? s->wq_rec32.as<uint64_t>() : nullptr;
-  q.cap = (int64_t)(s->wq_rec64.bytes / sizeof(uint64_t));
-  if (two_queues) q.cap = std::min<int64_t>(q.cap, (int64_t)(s->wq_rec32.bytes / sizeof(uint64_t)));
-  q.slots = s->wq_slots.as<PendSlot>();
-  q.vis = s->wq_vis.as<unsigned long long>();
-  q.scap = std::min<int64_t>((int64_t)(s->wq_slots.bytes / sizeof(PendSlot)),
-                             (int64_t)(s->wq_vis.bytes / (sizeof(unsigned long long) * q.vis_words)));
-  return 0;
 }
 
 // Quad8 pairs that share corner nodes, in the reference's classification
@@ -288,6 +241,13 @@ int rvf_session_destroy(rvf_session* s) {
     s->tile_counter.free_();
     s->counters.free_();
     s->wq_ctr.free_(); s->wq_rec64.free_(); s->wq_rec32.free_(); s->wq_slots.free_(); s->wq_vis.free_();
+    for (rvf::DevBuf* b : {&s->wl_pair, &s->wl_mixed, &s->wl_trace, &s->wl_resolve, &s->wl_tilebase, &s->wl_gen,
+                           &s->wl_tb, &s->wl_rb})
+      b->free_();
+    for (auto& kv : s->graphs) cudaGraphExecDestroy(kv.second);
+    s->graphs.clear();
+    if (s->h_ctr) cudaFreeHost(s->h_ctr);
+    s->h_ctr = nullptr;
     for (cudaEvent_t v : s->ev)
       if (v) cudaEventDestroy(v);
     cudaStreamDestroy(s->stream);
@@ -413,134 +373,28 @@ int rvf_solve(rvf_session* s, rvf_mesh* m, const rvf_options* o, double* F_elem,
       if ((rc = read_err(s))) return rc;
     }
   } else {
-  PairArgs a{};
-  a.N = N;
-  a.nT = (N + kTile - 1) / kTile;
-  a.n_tiles = a.nT * (a.nT + 1) / 2;
-  a.pmax = T->pmax;
-  a.dim3 = (m->dim == 2);
-  a.tab = T->tab.as<double>();
-  a.np = T->np.as<int8_t>();
-  a.area = T->area.as<double>();
-  a.flat = T->flat.as<uint8_t>();
-  a.nrm = T->nrm.as<double>();
-  a.group = m->group.as<int32_t>();
-  a.orig = m->orig.as<int32_t>();
-  a.cen = T->cen.as<double>();
-  a.rad = T->rad.as<double>();
-  a.cull_margin = std::ldexp(m->extent, -30);
-  a.F = m->F.as<double>();
-  a.nodes = occ ? m->nodes.as<NodeD>() : nullptr;
-  a.n_nodes = occ ? m->n_nodes : 0;
-  const size_t smem_cap = std::min<size_t>(s->smem_optin, 110 * 1024);
-  a.nodes_in_smem = occ && gen_smem_bytes(false, T->pmax, m->n_nodes, occ) <= smem_cap;
-  a.tris = occ ? (o->geometric_soup ? m->tris_geo.as<TriD>() : m->tris_ref.as<TriD>()) : nullptr;
-  a.segs = occ ? m->segs.as<SegD>() : nullptr;
-  a.tile_counter = s->tile_counter.as<unsigned long long>();
-  a.counters = s->counters.as<unsigned long long>();
-  a.err = s->err.as<int>();
-  a.ray_log = o->ray_log ? log.as<uint8_t>() : nullptr;
-  a.log_pm = o->ray_log_pm;
   if (N > 0) {
     if (N == 1) {
       cudaMemsetAsync(m->F.ptr, 0, sizeof(double), s->stream);
     }
     cudaError_t e = cudaSuccess;
-    MixedArgs x{};
-    if (mixed) {
-      if (!T->tabf.ptr) {
-        if ((rc = T->tabf.alloc(s, sizeof(float) * a.nT * kComp * T->pmax * kTile))) return rc;
-        cudaMemsetAsync(T->tabf.ptr, 0, T->tabf.bytes, s->stream);
-        PrepF32Args pf{N, T->pmax, T->tab.as<double>(), T->tabf.as<float>(), T->np.as<int8_t>(), T->cen.as<double>()};
-        if ((e = launch_prep_f32(pf, s->stream)) != cudaSuccess) return cuda_err(e, "FP32 table kernel launch");
-        n_kernels += 1;
-      }
-      x.N = N; x.nT = a.nT; x.n_tiles = a.n_tiles; x.pmax = a.pmax;
-      x.tab = a.tab; x.tabf = T->tabf.as<float>(); x.np = a.np; x.area = a.area; x.flat = a.flat; x.nrm = a.nrm;
-      x.cen = T->cen.as<double>(); x.diam = T->diam.as<double>(); x.near_factor = o->near_field_factor;
-      x.rad = a.rad; x.cull_margin = a.cull_margin;
-      x.group = a.group; x.orig = a.orig; x.F = a.F;
-      x.nodes = a.nodes; x.n_nodes = a.n_nodes;
-      x.nodesf = occ ? m->nodesf.as<NodeF>() : nullptr;
-      x.nodesf_in_smem = occ && gen_smem_bytes(true, T->pmax, m->n_nodes, occ) <= smem_cap;
-      x.tris = a.tris;
-      x.trisf = occ ? (o->geometric_soup ? m->trisf_geo.as<TriF>() : m->trisf_ref.as<TriF>()) : nullptr;
-      x.delta = (float)std::ldexp(m->extent, -20);
-      x.tile_counter = a.tile_counter; x.counters = a.counters; x.err = a.err;
-      x.ray_log = a.ray_log; x.log_pm = a.log_pm;
-    }
+    WaveReq w;
+    if ((rc = wave_prepare(s, m, T, o, o->ray_log ? log.as<uint8_t>() : nullptr, w, &n_kernels))) return rc;
     EvTimer t(s->stream);
-    WaveQ wq{};
-    if ((rc = ensure_wave(s, mixed && occ, occ, T->pmax, a.n_tiles, wq))) return rc;
-    a.q = wq;
-    x.q = wq;
-    TraceArgs ta{};
-    ResolveArgs ra{};
-    if (occ) {
-      ta.N = N; ta.pmax = a.pmax; ta.dim3 = a.dim3; ta.tab = a.tab; ta.tabf = x.tabf; ta.cen = T->cen.as<double>();
-      ta.group = a.group; ta.orig = a.orig; ta.nodes = a.nodes; ta.nodesf = x.nodesf; ta.n_nodes = a.n_nodes;
-      ta.tris = a.tris; ta.trisf = x.trisf; ta.segs = a.segs; ta.delta = x.delta; ta.q = wq;
-      ta.counters = a.counters; ta.ray_log = a.ray_log; ta.log_pm = a.log_pm;
-      ra.N = N; ra.pmax = a.pmax; ra.dim3 = a.dim3; ra.tab = a.tab; ra.tabf = x.tabf; ra.cen = T->cen.as<double>();
-      ra.diam = T->diam.as<double>(); ra.near_factor = o->near_field_factor; ra.area = a.area; ra.orig = a.orig;
-      ra.F = a.F; ra.q = wq;
-    }
-    cudaMemsetAsync(wq.ctr, 0, sizeof(unsigned long long) * kCtrCount, s->stream);
-    // chunks: each claims tiles while its queues have room, then traces and resolves them
-    unsigned long long prev = 0;
-    cudaEvent_t* ev = s->ev;
-    for (int chunk = 0;; ++chunk) {
-      cudaEventRecord(ev[0], s->stream);
-      e = mixed ? launch_gen_mixed(x, s->sm_count, s->stream) : launch_gen_fp64(a, s->sm_count, s->stream);
-      n_kernels += 1;
-      if (e != cudaSuccess) return cuda_err(e, "pair generation kernel launch");
-      cudaEventRecord(ev[1], s->stream);
-      S.n_chunks += 1;
-      if (!occ) {  // without rays one launch integrates every tile
-        cudaEventSynchronize(ev[1]);
-        float g = 0.f;
-        cudaEventElapsedTime(&g, ev[0], ev[1]);
-        S.ms_gen += g;
-        break;
-      }
-      if (mixed) {
-        ta.nodes_in_smem = trace_smem_bytes(true, m->n_nodes) <= 80 * 1024;
-        if ((e = launch_trace(ta, true, s->sm_count, s->stream)) != cudaSuccess) return cuda_err(e, "FP32 trace launch");
-        n_kernels += 1;
-      }
-      cudaEventRecord(ev[2], s->stream);
-      ta.nodes_in_smem = trace_smem_bytes(false, m->n_nodes) <= 72 * 1024;
-      if ((e = launch_trace(ta, false, s->sm_count, s->stream)) != cudaSuccess) return cuda_err(e, "trace launch");
-      cudaEventRecord(ev[3], s->stream);
-      if ((e = launch_resolve(ra, mixed, s->sm_count, s->stream)) != cudaSuccess) return cuda_err(e, "resolve launch");
-      cudaEventRecord(ev[4], s->stream);
-      n_kernels += 2;
-      unsigned long long cc[kCtrCount] = {};
-      e = cudaMemcpyAsync(cc, wq.ctr, sizeof cc, cudaMemcpyDeviceToHost, s->stream);
-      if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
-      if (e != cudaSuccess) return cuda_err(e, "pair pipeline");
+    WaveReq* one = &w;
+    while (!w.done()) {  // chunks: each claims tiles while the ray queues have room
+      ChunkInfo ci;
+      const int64_t before = w.claimed;
+      if ((rc = wave_chunk(s, &one, 1, false, &ci))) return rc;
       if ((rc = read_err(s))) return rc;
-      float t01 = 0.f, t12 = 0.f, t23 = 0.f, t34 = 0.f;
-      cudaEventElapsedTime(&t01, ev[0], ev[1]);
-      cudaEventElapsedTime(&t12, ev[1], ev[2]);
-      cudaEventElapsedTime(&t23, ev[2], ev[3]);
-      cudaEventElapsedTime(&t34, ev[3], ev[4]);
-      S.ms_gen += t01;
-      if (mixed) {
-        S.ms_trace += t12;
-        S.ms_trace_fp64 += t23;
-        S.n_rays_traced += (int64_t)cc[kCtrRec32];
-      } else {
-        S.ms_trace += t23;
-        S.n_rays_traced += (int64_t)cc[kCtrRec64];
-      }
-      S.ms_resolve += t34;
-      const unsigned long long claimed = cc[kCtrTile];
-      if (claimed >= (unsigned long long)a.n_tiles) break;
-      if (claimed == prev) return set_err(RVF_ENOMEM, "pair pipeline made no progress: ray queue too small for one tile");
-      prev = claimed;
-      // keep the tile counter; clear the queues
-      cudaMemsetAsync(wq.ctr + 1, 0, sizeof(unsigned long long) * (kCtrCount - 1), s->stream);
+      n_kernels += ci.kernels;
+      S.n_chunks += 1;
+      S.ms_gen += ci.ms_gen;
+      S.ms_trace += ci.ms_trace;
+      S.ms_trace_fp64 += ci.ms_trace_fp64;
+      S.ms_resolve += ci.ms_resolve;
+      S.n_rays_traced += ci.rays_traced;
+      if (w.claimed == before) return set_err(RVF_ENOMEM, "pair pipeline made no progress: ray queue too small for one tile");
     }
     S.ms_pairs = t.stop();
     if ((rc = read_err(s))) return rc;
@@ -558,10 +412,10 @@ int rvf_solve(rvf_session* s, rvf_mesh* m, const rvf_options* o, double* F_elem,
       d.enodes = m->enodes.as<int32_t>();
       d.area_orig = T->area_orig.as<double>();
       d.F = m->F.as<double>();
-      d.nodes = a.nodes;
-      d.n_nodes = a.n_nodes;
-      d.tris = a.tris;
-      d.counters = a.counters;
+      d.nodes = w.pa.nodes;
+      d.n_nodes = w.pa.n_nodes;
+      d.tris = w.pa.tris;
+      d.counters = s->counters.as<unsigned long long>();
       if (d.n_pairs > 0) {
         if ((e = launch_duffy(d, s->stream)) != cudaSuccess) return cuda_err(e, "Duffy kernel launch");
         n_kernels += 1;

@@ -1,0 +1,43 @@
+// wave_host.h -- host side of the wavefront pair pipeline (wave_host.cpp).
+#pragma once
+
+#include "kernels.h"
+#include "rvf_internal.h"
+
+namespace rvf {
+
+// One request's kernel arguments and progress through its tiles.
+struct WaveReq {
+  PairArgs pa{};
+  MixedArgs ma{};
+  TraceArgs ta{};
+  ResolveArgs ra{};
+  bool mixed = false, occ = false, dim3 = true;
+  int pmax = 0;
+  int64_t n_tiles = 0;  // upper-triangle tiles of the mesh
+  int64_t claimed = 0;  // tiles integrated so far
+  const NodeD* nodes_d = nullptr;
+  const NodeF* nodes_f = nullptr;
+  bool done() const { return claimed >= n_tiles; }
+};
+
+struct ChunkInfo {
+  double ms_gen = 0, ms_trace = 0, ms_trace_fp64 = 0, ms_resolve = 0;  // CUDA events (eager launches only)
+  int64_t rays_traced = 0;
+  int kernels = 0;
+  bool graph = false;  // replayed from a captured graph
+};
+
+int ensure_wave(Session* s, bool two_queues, bool occ, int pmax, int64_t n_tiles, WaveQ& q);
+// Fills w from a mesh, its tables and the options (builds the FP32 table on
+// the first mixed-precision use).
+int wave_prepare(Session* s, rvf_mesh* m, Tables* T, const rvf_options* o, uint8_t* ray_log, WaveReq& w,
+                 int64_t* n_kernels);
+WaveShape wave_shape(Session* s, WaveReq* const* reqs, int n);
+// One chunk over n requests of one shape (mixed, dim3, occ equal): claims
+// tiles in request order while the queues have room, traces and resolves
+// them, and advances each request's progress.  use_graph replays a CUDA
+// graph captured per launch shape (eager launch when capture is refused).
+int wave_chunk(Session* s, WaveReq* const* reqs, int n, bool use_graph, ChunkInfo* info);
+
+}  // namespace rvf
