@@ -185,6 +185,87 @@ int rvf_fma_peak(int32_t device, int32_t fp64, double* tflops);
  * rvf_result_device: the mixed-precision F against the FP64 F). */
 int rvf_max_abs_diff(const double* a_dev, const double* b_dev, int64_t n, double* out);
 
+/* ---------------------------------------------------------------------------
+ * Serving: continuous batching of solves (the request loop a Julia service
+ * would run around _gpu_compute_hook, src/Assembly.jl:241-260; the
+ * reference itself solves one mesh per call, synchronously).
+ *
+ * rvf_submit copies the mesh and options and returns at once.  A worker
+ * thread admits requests in arrival order while their device footprint
+ * (F matrix, quadrature tables, BVH) fits the admission budget, keeps each
+ * admitted mesh's geometry, BVH and F on the device, and feeds every
+ * admitted quadrature request of one launch class (precision, surface or
+ * curve, occlusion) to the same batched launches: each chunk's generation
+ * kernel drains one device-side queue of tiles drawn from all of them, so
+ * requests that arrive while others run join at the next chunk and their work
+ * overlaps on the device.  Launches of a class replay a CUDA graph captured
+ * for its shape; the grid sizes are chosen by a short autotuning sweep on the
+ * first chunks of the class.  Monte Carlo requests run one at a time between
+ * chunks.  Results stay on the device until rvf_request_result copies them;
+ * rvf_release frees them and the admission budget.  Every request's result
+ * is bit-identical to rvf_solve of the same mesh and options.
+ * The server drives the session's stream: do not call rvf_solve on the same
+ * session while a server exists on it.
+ * ------------------------------------------------------------------------- */
+typedef struct rvf_server rvf_server;
+
+#define RVF_REQ_QUEUED 0
+#define RVF_REQ_RUNNING 1
+#define RVF_REQ_DONE 2
+#define RVF_REQ_FAILED 3
+#define RVF_REQ_CANCELED 4
+
+typedef struct {
+  uint64_t admit_bytes;  /* admission budget for the admitted requests' footprints (0 = 70% of the session budget) */
+  int32_t max_batch;     /* requests per batched launch, 1..64 (0 = 64) */
+  int32_t use_graphs;    /* 0 or 1: replay a CUDA graph per launch shape; -1: eager launches */
+  int32_t autotune;      /* 0 = default grids; 1 = sweep grid sizes on the first chunks of each launch class */
+  int32_t reserved[8];
+} rvf_server_opts;
+
+typedef struct {
+  int32_t state;             /* RVF_REQ_* */
+  int32_t status;            /* RVF_OK, or the error of a failed request */
+  int64_t n_elems;
+  uint64_t footprint_bytes;  /* device memory charged to the admission budget */
+  double t_submit_ms;        /* since the server was created */
+  double t_admit_ms;
+  double t_done_ms;
+  int64_t n_chunks;          /* batched chunks the request took part in */
+  int32_t reserved[8];
+} rvf_request_info;
+
+typedef struct {
+  int64_t submitted, completed, failed, canceled, in_flight;
+  double p50_ms, p99_ms, mean_ms;  /* latency submit -> done of the completed requests */
+  double wall_ms;                  /* first submit -> last completion */
+  int64_t pairs_done;              /* element pairs of the completed requests */
+  int64_t chunks;                  /* batched launches */
+  int64_t graph_replays;
+  int64_t batched_requests;        /* sum over chunks of the requests in the chunk */
+  uint64_t admitted_bytes_peak;
+  int32_t reserved[8];
+} rvf_server_stats;
+
+int rvf_server_create(rvf_session* s, const rvf_server_opts* o, rvf_server** out);
+/* Cancels the queued requests, finishes the running chunk, frees everything. */
+int rvf_server_destroy(rvf_server* sv);
+/* ray_log is not supported here (RVF_EINVAL). */
+int rvf_submit(rvf_server* sv, const rvf_mesh_desc* d, const rvf_options* o, int64_t* id);
+/* RVF_OK when done, RVF_EBUSY while queued or running, the request's error
+ * when it failed, RVF_ECANCELED when cancelled; info may be NULL. */
+int rvf_poll(rvf_server* sv, int64_t id, rvf_request_info* info);
+/* As rvf_poll, waiting up to timeout_ms (< 0: no limit); RVF_ETIMEDOUT when
+ * the request is still queued or running at the limit. */
+int rvf_wait(rvf_server* sv, int64_t id, int64_t timeout_ms, rvf_request_info* info);
+int rvf_cancel(rvf_server* sv, int64_t id);
+/* Host copies of a done request's result (any pointer may be NULL). */
+int rvf_request_result(rvf_server* sv, int64_t id, double* F_elem, double* A_elem, double* F_group,
+                       double* A_group, double* row_sums);
+/* Frees a finished request's device memory and its admission charge. */
+int rvf_release(rvf_server* sv, int64_t id);
+int rvf_server_stats_get(rvf_server* sv, rvf_server_stats* st);
+
 /* Plain FP64 assembly that allocates no memory (no counterpart in the
  * reference).  For callers that cannot call cudaMalloc -- code under an
  * allocator that owns all device memory, memory-capped services, hosts that

@@ -18,6 +18,7 @@ RVF_OK = 0
 STATUS_NAMES = {0: "RVF_OK", -1: "RVF_EINVAL", -2: "RVF_ENOMEM", -3: "RVF_EBUDGET", -4: "RVF_ECUDA",
                 -5: "RVF_ETIMEDOUT", -6: "RVF_ECANCELED", -7: "RVF_EUNSUPPORTED", -8: "RVF_ENODEV",
                 -9: "RVF_EBUSY", -10: "RVF_ECLOSED"}
+globals().update({name: code for code, name in STATUS_NAMES.items()})  # RVF_EINVAL, ...
 
 METHOD_QUADRATURE, METHOD_MONTE_CARLO = 0, 1
 PREC_FP64, PREC_MIXED = 0, 1
@@ -74,6 +75,30 @@ class Stats(C.Structure):
         return d
 
 
+class ServerOpts(C.Structure):
+    _fields_ = [("admit_bytes", C.c_uint64), ("max_batch", C.c_int32), ("use_graphs", C.c_int32),
+                ("autotune", C.c_int32), ("reserved", C.c_int32 * 8)]
+
+
+class RequestInfo(C.Structure):
+    _fields_ = [("state", C.c_int32), ("status", C.c_int32), ("n_elems", C.c_int64),
+                ("footprint_bytes", C.c_uint64), ("t_submit_ms", C.c_double), ("t_admit_ms", C.c_double),
+                ("t_done_ms", C.c_double), ("n_chunks", C.c_int64), ("reserved", C.c_int32 * 8)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("submitted", C.c_int64), ("completed", C.c_int64), ("failed", C.c_int64),
+                ("canceled", C.c_int64), ("in_flight", C.c_int64), ("p50_ms", C.c_double),
+                ("p99_ms", C.c_double), ("mean_ms", C.c_double), ("wall_ms", C.c_double),
+                ("pairs_done", C.c_int64), ("chunks", C.c_int64), ("graph_replays", C.c_int64),
+                ("batched_requests", C.c_int64), ("admitted_bytes_peak", C.c_uint64), ("reserved", C.c_int32 * 8)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+
+
+REQ_STATES = {0: "queued", 1: "running", 2: "done", 3: "failed", 4: "canceled"}
+
 # exported symbols and their signatures (checked by the CPU test-suite)
 SIGNATURES = {
     "rvf_version": (C.c_char_p, []),
@@ -97,6 +122,15 @@ SIGNATURES = {
     "rvf_max_abs_diff": (C.c_int, [_pd, _pd, C.c_int64, _pd]),
     "rvf_solve_fp64_noalloc": (C.c_int, [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64,
                                          C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "rvf_server_create": (C.c_int, [_p, C.POINTER(ServerOpts), C.POINTER(_p)]),
+    "rvf_server_destroy": (C.c_int, [_p]),
+    "rvf_submit": (C.c_int, [_p, C.POINTER(MeshDesc), C.POINTER(Options), C.POINTER(C.c_int64)]),
+    "rvf_poll": (C.c_int, [_p, C.c_int64, C.POINTER(RequestInfo)]),
+    "rvf_wait": (C.c_int, [_p, C.c_int64, C.c_int64, C.POINTER(RequestInfo)]),
+    "rvf_cancel": (C.c_int, [_p, C.c_int64]),
+    "rvf_request_result": (C.c_int, [_p, C.c_int64, _pd, _pd, _pd, _pd, _pd]),
+    "rvf_release": (C.c_int, [_p, C.c_int64]),
+    "rvf_server_stats_get": (C.c_int, [_p, C.POINTER(ServerStats)]),
 }
 
 
@@ -177,6 +211,32 @@ class Session:
         return {"sm_count": sm.value, "hbm_total": tot.value, "hbm_free": fr.value}
 
 
+def mesh_desc(desc_arrays: dict) -> MeshDesc:
+    """rvf_mesh_desc over the arrays of mesh_desc_arrays (kept alive by the caller)."""
+    d = MeshDesc()
+    d.mesh_dim = desc_arrays["mesh_dim"]
+    d.n_nodes = desc_arrays["coords"].shape[1]
+    d.coords = ptr(desc_arrays["coords"], C.c_double)
+    d.n_elems = desc_arrays["elem_family"].shape[0]
+    d.elem_family = ptr(desc_arrays["elem_family"], C.c_int8)
+    d.elem_node_idx = ptr(desc_arrays["elem_node_idx"], C.c_int32)
+    d.elem_group = ptr(desc_arrays["elem_group"], C.c_int32)
+    for f in range(6):
+        t = desc_arrays["nodes"][f]
+        d.nodes[f] = ptr(t, C.c_int32) if t.size else None
+        d.n_family[f] = t.shape[0]
+    soup = desc_arrays.get("obs_soup")
+    if soup is not None:
+        d.n_obs = soup.shape[0]
+        d.obs_nv = soup.shape[1]
+        d.obs_soup = ptr(soup, C.c_double)
+        d.obs_group = ptr(desc_arrays["obs_group"], C.c_int32)
+    tags = desc_arrays["group_tags"]
+    d.n_groups = tags.shape[0]
+    d.group_tags = ptr(tags, C.c_int32)
+    return d
+
+
 class DeviceMesh:
     """A mesh resident on the device (rvf_mesh)."""
 
@@ -184,27 +244,7 @@ class DeviceMesh:
         self.session = session
         self.lib = session.lib
         self._keep = desc_arrays  # the library copies, but keep inputs alive during the call
-        d = MeshDesc()
-        d.mesh_dim = desc_arrays["mesh_dim"]
-        d.n_nodes = desc_arrays["coords"].shape[1]
-        d.coords = ptr(desc_arrays["coords"], C.c_double)
-        d.n_elems = desc_arrays["elem_family"].shape[0]
-        d.elem_family = ptr(desc_arrays["elem_family"], C.c_int8)
-        d.elem_node_idx = ptr(desc_arrays["elem_node_idx"], C.c_int32)
-        d.elem_group = ptr(desc_arrays["elem_group"], C.c_int32)
-        for f in range(6):
-            t = desc_arrays["nodes"][f]
-            d.nodes[f] = ptr(t, C.c_int32) if t.size else None
-            d.n_family[f] = t.shape[0]
-        soup = desc_arrays.get("obs_soup")
-        if soup is not None:
-            d.n_obs = soup.shape[0]
-            d.obs_nv = soup.shape[1]
-            d.obs_soup = ptr(soup, C.c_double)
-            d.obs_group = ptr(desc_arrays["obs_group"], C.c_int32)
-        tags = desc_arrays["group_tags"]
-        d.n_groups = tags.shape[0]
-        d.group_tags = ptr(tags, C.c_int32)
+        d = mesh_desc(desc_arrays)
         h = _p()
         check(self.lib.rvf_mesh_upload(session.handle, C.byref(d), C.byref(h)), self.lib)
         self.handle = h
@@ -310,5 +350,73 @@ class PinnedArray:
     def __del__(self):
         try:
             self.free()
+        except Exception:
+            pass
+
+
+class Server:
+    """Continuous-batching request loop on a session (rvf_server): submit
+    solves as they arrive, poll / wait, copy results, release."""
+
+    def __init__(self, session: Session, admit_bytes: int = 0, max_batch: int = 0, use_graphs: bool = True,
+                 autotune: bool = True):
+        self.session = session
+        self.lib = session.lib
+        o = ServerOpts(admit_bytes=admit_bytes, max_batch=max_batch, use_graphs=0 if use_graphs else -1,
+                       autotune=0 if autotune else -1)
+        h = _p()
+        check(self.lib.rvf_server_create(session.handle, C.byref(o), C.byref(h)), self.lib)
+        self.handle = h
+        self.n_elems = {}
+
+    def submit(self, desc_arrays: dict, opts: Options) -> int:
+        d = mesh_desc(desc_arrays)
+        rid = C.c_int64()
+        check(self.lib.rvf_submit(self.handle, C.byref(d), C.byref(opts), C.byref(rid)), self.lib)
+        self.n_elems[rid.value] = (int(d.n_elems), int(d.n_groups))
+        return rid.value
+
+    def poll(self, rid: int):
+        """(state name, status, RequestInfo)."""
+        info = RequestInfo()
+        st = self.lib.rvf_poll(self.handle, rid, C.byref(info))
+        return REQ_STATES.get(info.state, info.state), st, info
+
+    def wait(self, rid: int, timeout_ms: int = -1) -> RequestInfo:
+        info = RequestInfo()
+        check(self.lib.rvf_wait(self.handle, rid, timeout_ms, C.byref(info)), self.lib)
+        return info
+
+    def cancel(self, rid: int):
+        check(self.lib.rvf_cancel(self.handle, rid), self.lib)
+
+    def result(self, rid: int, F=None, A=None, Fg=None, Ag=None, row_sums=None):
+        N, G = self.n_elems[rid]
+        F = np.empty((N, N), order="F") if F is None else F
+        A = np.empty(N) if A is None else A
+        Fg = np.empty((G, G), order="F") if Fg is None else Fg
+        Ag = np.empty(G) if Ag is None else Ag
+        check(self.lib.rvf_request_result(self.handle, rid, ptr(F, C.c_double), ptr(A, C.c_double),
+                                          ptr(Fg, C.c_double), ptr(Ag, C.c_double), ptr(row_sums, C.c_double)),
+              self.lib)
+        return F, A, Fg, Ag
+
+    def release(self, rid: int):
+        check(self.lib.rvf_release(self.handle, rid), self.lib)
+        self.n_elems.pop(rid, None)
+
+    def stats(self) -> dict:
+        st = ServerStats()
+        check(self.lib.rvf_server_stats_get(self.handle, C.byref(st)), self.lib)
+        return st.as_dict()
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self.lib.rvf_server_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
         except Exception:
             pass

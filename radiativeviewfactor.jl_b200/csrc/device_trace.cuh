@@ -46,6 +46,7 @@ struct RayBankT {
     } r32;
   };
   int32_t gi[32], gj[32];
+  const void* prims[32];         // each ray's primitive array (rays of one warp may come from different meshes)
   int32_t first[L][32];          // collected leaves: first primitive
   uint16_t item[32 * L * 8];     // leaf phase: (lane, leaf slot, offset) per test
   uint8_t hit[32];
@@ -257,6 +258,7 @@ struct PolD3 {
     ws.r64.tmax[lane] = R.tmax;
     ws.gi[lane] = gi;
     ws.gj[lane] = gj;
+    ws.prims[lane] = tris;
   }
   __device__ __forceinline__ int node(const NodeD& nd) const { return slab_d(nd, R) ? kHit : kMiss; }
   __device__ __forceinline__ void leaf(const NodeD& nd, int& first, int& count) const {
@@ -266,7 +268,7 @@ struct PolD3 {
   __device__ __forceinline__ int miss(const NodeD& nd) const { return nd.miss; }
   template <typename B>
   __device__ __forceinline__ int prim(const B& ws, int o, int k, TravCount& cnt) const {
-    const TriD tr = tris[k];
+    const TriD tr = static_cast<const TriD*>(ws.prims[o])[k];
     if (tr.group == ws.gi[o] || tr.group == ws.gj[o]) return kMiss;
     ++cnt.prims;
     RayD Q;
@@ -293,6 +295,7 @@ struct PolD2 {
     ws.r64.d[1][lane] = b[1];
     ws.gi[lane] = gi;
     ws.gj[lane] = gj;
+    ws.prims[lane] = segs;
   }
   __device__ __forceinline__ int node(const NodeD& nd) const {
     const double xlo = fmin(a[0], b[0]), xhi = fmax(a[0], b[0]);
@@ -306,7 +309,7 @@ struct PolD2 {
   __device__ __forceinline__ int miss(const NodeD& nd) const { return nd.miss; }
   template <typename B>
   __device__ __forceinline__ int prim(const B& ws, int o, int k, TravCount& cnt) const {
-    const SegD sg = segs[k];
+    const SegD sg = static_cast<const SegD*>(ws.prims[o])[k];
     if (sg.group == ws.gi[o] || sg.group == ws.gj[o]) return kMiss;
     ++cnt.prims;
     const double xa[2] = {ws.r64.o[0][o], ws.r64.o[1][o]}, xb[2] = {ws.r64.d[0][o], ws.r64.d[1][o]};
@@ -329,6 +332,7 @@ struct PolF3 {
     ws.r32.delta[lane] = R.delta;
     ws.gi[lane] = gi;
     ws.gj[lane] = gj;
+    ws.prims[lane] = tris;
   }
   __device__ __forceinline__ int node(const NodeF& nd) const { return slab_f(nd, R); }
   __device__ __forceinline__ void leaf(const NodeF& nd, int& first, int& count) const {
@@ -338,7 +342,7 @@ struct PolF3 {
   __device__ __forceinline__ int miss(const NodeF& nd) const { return nd.miss; }
   template <typename B>
   __device__ __forceinline__ int prim(const B& ws, int o, int k, TravCount& cnt) const {
-    const TriF tr = tris[k];
+    const TriF tr = static_cast<const TriF*>(ws.prims[o])[k];
     if (tr.group == ws.gi[o] || tr.group == ws.gj[o]) return kMiss;
     ++cnt.prims;
     RayF Q;

@@ -237,6 +237,7 @@ struct WaveShape {
   int pmax_max;
   bool gen_nodes_smem, trace64_nodes_smem, trace32_nodes_smem;
   int n_nodes_smem;
+  int gen_bps, trace_bps;  // blocks per SM of the generation / traversal grids (0 = occupancy limit)
 };
 
 size_t gen_smem_bytes(bool mixed, int pmax, int n_nodes_smem, bool occ);

@@ -919,7 +919,7 @@ cudaError_t launch_gen(const WaveShape& sh, const GenBatch* g, int sm_count, cud
   auto launch = [&](auto fn) -> cudaError_t {
     cudaError_t e = set_smem(fn, smem);
     if (e != cudaSuccess) return e;
-    const int grid = grid_for(fn, smem, sm_count, 4);
+    const int grid = grid_for(fn, smem, sm_count, sh.gen_bps > 0 ? sh.gen_bps : 4);
     fn<<<(unsigned)grid, 256, smem, st>>>(g);
     return cudaGetLastError();
   };
@@ -934,7 +934,7 @@ cudaError_t launch_trace(const WaveShape& sh, const TraceBatch* t, bool fp32, in
   auto launch = [&](auto fn) -> cudaError_t {
     cudaError_t e = set_smem(fn, smem);
     if (e != cudaSuccess) return e;
-    const int grid = grid_for(fn, smem, sm_count, 8);
+    const int grid = grid_for(fn, smem, sm_count, sh.trace_bps > 0 ? sh.trace_bps : 8);
     fn<<<(unsigned)grid, 256, smem, st>>>(t);
     return cudaGetLastError();
   };

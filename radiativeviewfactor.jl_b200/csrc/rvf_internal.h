@@ -112,4 +112,9 @@ struct rvf_mesh {
 namespace rvf {
 int mesh_upload(Session* s, const rvf_mesh_desc* d, rvf_mesh** out);
 int ensure_tables(Session* s, rvf_mesh* m, int nquad, Tables** out);
+// solve.cpp helpers shared with the serving loop (callers hold s->mu)
+int read_err(Session* s);
+int validate_options(const rvf_mesh* m, const rvf_options* o);
+int run_reduce(Session* s, rvf_mesh* m, const double* area);
+int ensure_duffy(Session* s, rvf_mesh* m, int nquad, const double** p01, const double** w01);
 }  // namespace rvf

@@ -37,6 +37,10 @@ struct EvTimer {
   }
 };
 
+}  // namespace
+
+namespace rvf {
+
 int read_err(Session* s) {
   int herr = 0;
   cudaError_t e = cudaMemcpyAsync(&herr, s->err.ptr, sizeof(int), cudaMemcpyDeviceToHost, s->stream);
@@ -168,7 +172,7 @@ int ensure_duffy(Session* s, rvf_mesh* m, int nquad, const double** p01, const d
   return RVF_OK;
 }
 
-}  // namespace
+}  // namespace rvf
 
 extern "C" {
 

@@ -176,7 +176,8 @@ int ensure_blocks(Session* s) {
 uint64_t shape_key(const WaveShape& sh) {
   return (uint64_t)sh.mixed | ((uint64_t)sh.dim3 << 1) | ((uint64_t)sh.occ << 2) | ((uint64_t)sh.gen_nodes_smem << 3) |
          ((uint64_t)sh.trace64_nodes_smem << 4) | ((uint64_t)sh.trace32_nodes_smem << 5) |
-         ((uint64_t)sh.pmax_max << 8) | ((uint64_t)sh.n_nodes_smem << 24);
+         ((uint64_t)sh.pmax_max << 8) | ((uint64_t)sh.gen_bps << 16) | ((uint64_t)sh.trace_bps << 20) |
+         ((uint64_t)sh.n_nodes_smem << 24);
 }
 
 // The chunk's device work: counters reset, generation, traversal(s), resolve
@@ -202,11 +203,13 @@ cudaError_t enqueue_chunk(Session* s, const WaveShape& sh, bool events) {
 
 }  // namespace
 
-int wave_chunk(Session* s, WaveReq* const* reqs, int n, bool use_graph, ChunkInfo* info) {
+int wave_chunk(Session* s, WaveReq* const* reqs, int n, bool use_graph, ChunkInfo* info, int gen_bps, int trace_bps) {
   if (n < 1 || n > kMaxBatch) return set_err(RVF_EINVAL, "batch of %d requests (1..%d)", n, kMaxBatch);
   int rc = 0;
   if ((rc = ensure_blocks(s))) return rc;
-  const WaveShape sh = wave_shape(s, reqs, n);
+  WaveShape sh = wave_shape(s, reqs, n);
+  sh.gen_bps = gen_bps;
+  sh.trace_bps = trace_bps;
   // tiles still to claim, per request, in launch order
   std::vector<int64_t> base(n + 1, 0);
   for (int r = 0; r < n; ++r) base[r + 1] = base[r] + (reqs[r]->n_tiles - reqs[r]->claimed);

@@ -38,6 +38,8 @@ WaveShape wave_shape(Session* s, WaveReq* const* reqs, int n);
 // tiles in request order while the queues have room, traces and resolves
 // them, and advances each request's progress.  use_graph replays a CUDA
 // graph captured per launch shape (eager launch when capture is refused).
-int wave_chunk(Session* s, WaveReq* const* reqs, int n, bool use_graph, ChunkInfo* info);
+// gen_bps / trace_bps: blocks per SM of the two grids (0 = occupancy limit).
+int wave_chunk(Session* s, WaveReq* const* reqs, int n, bool use_graph, ChunkInfo* info, int gen_bps = 0,
+               int trace_bps = 0);
 
 }  // namespace rvf

@@ -53,6 +53,37 @@ def test_struct_sizes_match_header(lib):
     assert ctypes.sizeof(_abi.MeshDesc) % 8 == 0
 
 
+def test_struct_layouts_match_compiled_header(tmp_path, rvf):
+    """sizeof / offsetof of every ABI struct, compiled from the header with
+    gcc, against the ctypes mirror."""
+    import shutil
+    import subprocess
+    from rvf_b200 import _abi
+    if not shutil.which("gcc"):
+        pytest.skip("gcc not available")
+    structs = {"rvf_session_opts": _abi.SessionOpts, "rvf_mesh_desc": _abi.MeshDesc, "rvf_options": _abi.Options,
+               "rvf_stats": _abi.Stats, "rvf_server_opts": _abi.ServerOpts, "rvf_request_info": _abi.RequestInfo,
+               "rvf_server_stats": _abi.ServerStats}
+    lines = ['#include <stdio.h>', '#include <stddef.h>', f'#include "{HEADER}"', 'int main(void) {']
+    for cname, ct in structs.items():
+        lines.append(f'  printf("{cname} size %zu\\n", sizeof({cname}));')
+        for fname, _ in ct._fields_:
+            lines.append(f'  printf("{cname} {fname} %zu\\n", offsetof({cname}, {fname}));')
+    lines.append("  return 0;\n}")
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", str(src), "-o", str(exe)], check=True)
+    got = {}
+    for ln in subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.splitlines():
+        c, f, v = ln.split()
+        got[(c, f)] = int(v)
+    for cname, ct in structs.items():
+        assert got[(cname, "size")] == ctypes.sizeof(ct), cname
+        for fname, _ in ct._fields_:
+            assert got[(cname, fname)] == getattr(ct, fname).offset, (cname, fname)
+
+
 def test_session_without_gpu_reports_enodev(lib, rvf):
     import torch
     if torch.cuda.is_available():
