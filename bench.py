@@ -254,6 +254,148 @@ def phases(stats):
     return d
 
 
+# ---------------------------------------------------------------------------
+# Serving stream (C5): seeded requests with Poisson arrivals through rvf_server
+# ---------------------------------------------------------------------------
+SERVE_SIZES = {
+    # requests, element count range (log-uniform), admission budget
+    "small": (32, 2000, 8000, 150 << 30),
+    "full": (512, 2000, 40000, 150 << 30),
+}
+
+
+def serve_requests(rvf, n_req, n_lo, n_hi, seed=5):
+    """Random geometry (plates / cube enclosure / cylinder), element count
+    log-uniform in [n_lo, n_hi], Tri3 / Quad4 / Quad8, nquad 2..5, 30% with
+    an obstruction box, 20% Monte Carlo (64 samples); quadrature requests in
+    mixed precision."""
+    import math
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    M = rvf.meshes
+    out = []
+    for k in range(n_req):
+        n = math.exp(rng.uniform(math.log(n_lo), math.log(n_hi)))
+        geo = rng.choice(["plates", "cube", "cylinder"])
+        fam = rng.choice(["tri3", "quad4", "quad"])
+        box = rng.uniform() < 0.3
+        mc = rng.uniform() < 0.2
+        nquad = int(rng.integers(2, 6))
+        obs = []
+        if geo == "cylinder":
+            nc = max(8, int(round(math.sqrt(n / 0.75) / 4)) * 4)
+            md = M.cylinder(nc=nc, na=nc // 2, cap_rings=max(2, nc // 8), seed=int(rng.integers(1 << 30)))
+            fam = "quad"
+            center = (0.0, 0.0, 0.5)
+        elif geo == "cube":
+            per = 12 if fam == "tri3" else 6
+            md = M.cube_enclosure(max(2, int(round(math.sqrt(n / per)))), family=fam, box=False,
+                                  seed=int(rng.integers(1 << 30)))
+            center = (0.5, 0.5, 0.5)
+        else:
+            per = 4 if fam == "tri3" else 2
+            md = M.parallel_plates(max(2, int(round(math.sqrt(n / per)))), fam)
+            center = (0.5, 0.5, 0.5)
+        if box:
+            md.group_tri_soup[99] = M.obstruction_box(center=center, edge=0.3, m=8)
+            obs = [99]
+        o = rvf.make_options(nquad, monte_carlo=bool(mc), n_samples=64, seed=int(rng.integers(1 << 62)),
+                             precision="fp64" if mc else "mixed")
+        out.append({"md": md, "obs": obs, "opts": o, "geo": str(geo), "family": fam, "nquad": nquad,
+                    "box": bool(box), "mc": bool(mc), "N": md.n_elems})
+    return out
+
+
+def run_serve(rvf, sess, size: str, local: int):
+    """p50/p99 latency and throughput of a Poisson request stream through the
+    serving loop, at ~80% of the measured one-at-a-time capacity; a sample of
+    the results is compared with plain FP64 one-at-a-time solves."""
+    import threading
+    import numpy as np
+    from rvf_b200 import _abi
+    n_req, n_lo, n_hi, admit = SERVE_SIZES[size]
+    reqs = serve_requests(rvf, n_req, n_lo, n_hi)
+    arrays = [rvf.mesh_desc_arrays(r["md"], r["obs"]) for r in reqs]
+    pairs = [r["N"] * (r["N"] - 1) // 2 for r in reqs]
+    # one-at-a-time capacity on a sample, same options (mixed) and plain FP64
+    sample = list(range(0, n_req, max(1, n_req // 8)))[:8]
+    t_mixed, t_fp64, dF = 0.0, 0.0, 0.0
+    for k in sample:
+        r = reqs[k]
+        N, G = r["N"], max(1, len(r["md"].group_tags))
+        dm = _abi.DeviceMesh(sess, arrays[k])
+        dm.solve(r["opts"])  # warm (tables, queues)
+        t0 = time.perf_counter()
+        dm.solve(r["opts"])
+        t_mixed += time.perf_counter() - t0
+        o64 = rvf.make_options(r["nquad"], monte_carlo=r["mc"], n_samples=64, seed=r["opts"].seed, precision="fp64")
+        t0 = time.perf_counter()
+        dm.solve(o64)
+        t_fp64 += time.perf_counter() - t0
+        dm.release()
+    mean_service = t_mixed / len(sample)
+    sample_pairs = sum(pairs[k] for k in sample)
+    lam = 0.8 / mean_service
+    rng = np.random.default_rng(7)
+    arrivals = np.cumsum(rng.exponential(1.0 / lam, size=n_req))
+    sv = _abi.Server(sess, admit_bytes=admit)
+    ids = [None] * n_req
+    err = []
+
+    def submitter():
+        t0 = time.perf_counter()
+        for k in range(n_req):
+            dt = arrivals[k] - (time.perf_counter() - t0)
+            if dt > 0:
+                time.sleep(dt)
+            ids[k] = sv.submit(arrays[k], reqs[k]["opts"])
+
+    th = threading.Thread(target=submitter)
+    t_start = time.perf_counter()
+    th.start()
+    th.join()
+    for k in range(n_req):
+        try:
+            sv.wait(ids[k], 3_600_000)
+        except _abi.RVFError as e:
+            err.append(str(e))
+    wall = time.perf_counter() - t_start
+    # a sample of the results against plain FP64 one-at-a-time solves
+    check = [k for k in sample if not reqs[k]["mc"]][:4]
+    for k in check:
+        N = reqs[k]["N"]
+        F = sv.result(ids[k])[0]
+        dm = _abi.DeviceMesh(sess, arrays[k])
+        F64 = np.empty((N, N), order="F")
+        dm.solve(rvf.make_options(reqs[k]["nquad"], seed=0, precision="fp64"), F64)
+        dm.release()
+        dF = max(dF, float(np.nanmax(np.abs(F - F64))))
+    st = sv.stats()
+    for k in range(n_req):
+        try:
+            sv.release(ids[k])
+        except _abi.RVFError:
+            pass
+    sv.close()
+    total_pairs = sum(pairs)
+    return {
+        "metric": "serve latency and throughput", "requests": n_req, "failed": len(err),
+        "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "mean_ms": st["mean_ms"],
+        "throughput_pairs_per_s": total_pairs / wall, "wall_s": wall,
+        "one_at_a_time_mixed_pairs_per_s": sample_pairs / t_mixed,
+        "one_at_a_time_fp64_pairs_per_s": sample_pairs / t_fp64,
+        "lambda_per_s": lam, "offered_load": 0.8,
+        "max_abs_dF_vs_fp64_solo": dF, "checked_requests": len(check),
+        "chunks": st["chunks"], "batched_requests": st["batched_requests"], "graph_replays": st["graph_replays"],
+        "admit_bytes": admit, "admitted_bytes_peak": st["admitted_bytes_peak"],
+        "config": {"stream": f"{n_req} seeded requests (seed 5), Poisson arrivals, N log-uniform {n_lo}-{n_hi}, "
+                             "plates / cube / cylinder, Tri3 / Quad4 / Quad8, nquad 2-5, 30% obstruction box, "
+                             "20% Monte Carlo (64 samples), quadrature in mixed precision",
+                   "mix": {"mc": sum(r["mc"] for r in reqs), "box": sum(r["box"] for r in reqs),
+                           "elements_total": sum(r["N"] for r in reqs)}},
+    }
+
+
 def run_ours(args):
     ws, rank, local = dist_setup()
     rvf = load_pkg()
@@ -358,6 +500,8 @@ def run_ours(args):
         line["accuracy"] = accuracy
     if rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(rvf, md, args.ref_seconds)
+    if rank == 0 and args.serve != "none":
+        line["serve"] = run_serve(rvf, sess, args.serve, local)
     if rank == 0:
         print(json.dumps(line), flush=True)
     del flush
@@ -380,6 +524,8 @@ def main():
     ap.add_argument("--e2e-warmup", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ref-seconds", type=float, default=15.0)
+    ap.add_argument("--serve", choices=["none", "small", "full"], default="small",
+                    help="serving stream reported beside the main line (small: 32 requests, 2k-8k elements)")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

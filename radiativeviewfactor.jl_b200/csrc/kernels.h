@@ -281,6 +281,8 @@ cudaError_t launch_duffy(const DuffyArgs& a, cudaStream_t st);
 
 struct McArgs {
   int64_t N, nT, n_tiles;
+  int64_t tile0, tile_count;  // this launch integrates tiles [tile0, tile0 + tile_count)
+  bool area_pass;             // also run the area rule (first launch of a solve)
   int n_samples;
   uint64_t seed;
   bool exclude;  // skip source / destination groups in the traversal

@@ -121,9 +121,10 @@ __global__ void __launch_bounds__(256) k_pairs_mc(McArgs a) {
   for (;;) {
     if (threadIdx.x == 0) s_tile = (int64_t)atomicAdd(a.tile_counter, 1ull);
     __syncthreads();
-    const int64_t t = s_tile;
+    const int64_t tl = s_tile;
     __syncthreads();
-    if (t >= a.n_tiles) break;
+    if (tl >= a.tile_count) break;
+    const int64_t t = a.tile0 + tl;
     int64_t bi, bj;
     tile_coords(t, a.nT, bi, bj);
     const int64_t j = bj * kTile + lane;
@@ -225,11 +226,14 @@ static cudaError_t launch_mc_t(const McArgs& a, int grid, cudaStream_t st) {
 
 cudaError_t launch_mc(const McArgs& a, int sm_count, cudaStream_t st) {
   if (a.N == 0) return cudaSuccess;
-  k_mc_area<<<(unsigned)((a.N + 127) / 128), 128, 0, st>>>(a);
-  cudaError_t e = cudaGetLastError();
-  if (e != cudaSuccess) return e;
+  if (a.area_pass) {
+    k_mc_area<<<(unsigned)((a.N + 127) / 128), 128, 0, st>>>(a);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
+  if (a.tile_count <= 0) return cudaSuccess;
   int64_t grid = (int64_t)sm_count * 3;
-  if (grid > a.n_tiles) grid = a.n_tiles;
+  if (grid > a.tile_count) grid = a.tile_count;
   if (grid < 1) grid = 1;
   const bool occ = a.n_nodes > 0;
   if (a.dim3) return occ ? launch_mc_t<true, true>(a, (int)grid, st) : launch_mc_t<true, false>(a, (int)grid, st);

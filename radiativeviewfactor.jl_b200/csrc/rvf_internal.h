@@ -14,6 +14,7 @@
 
 #include "../../include/rvf_b200.h"
 #include "rvf_host.h"
+#include "kernels.h"
 
 struct rvf_session;
 
@@ -117,4 +118,5 @@ int read_err(Session* s);
 int validate_options(const rvf_mesh* m, const rvf_options* o);
 int run_reduce(Session* s, rvf_mesh* m, const double* area);
 int ensure_duffy(Session* s, rvf_mesh* m, int nquad, const double** p01, const double** w01);
+void fill_mc_args(Session* s, rvf_mesh* m, const rvf_options* o, uint8_t* ray_log, McArgs& c);
 }  // namespace rvf

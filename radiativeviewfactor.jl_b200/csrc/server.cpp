@@ -83,6 +83,9 @@ struct Req {
   WaveReq w;
   double t_submit = 0, t_admit = -1, t_done = -1;
   int64_t n_chunks = 0;
+  // Monte Carlo progress (tiles of the upper triangle)
+  int64_t mc_tiles = 0, mc_claimed = 0;
+  bool mc_area_done = false;
 };
 
 // points per element of the quadrature rules (upper bound over the families present)
@@ -149,6 +152,13 @@ struct rvf_server {
 
 namespace {
 
+// Work offered to one launch: tens of milliseconds, so that arrivals join
+// and the oldest requests finish at short intervals (quadrature point pairs
+// of the mixed pipeline; Monte Carlo sample pairs, each of which evaluates
+// both elements' geometry).
+constexpr double kChunkPointPairs = 4e8;
+constexpr double kChunkSamplePairs = 1e8;
+
 const int kCand[][2] = {{0, 0}, {2, 0}, {0, 2}, {2, 2}};
 constexpr int kNCand = 4;
 
@@ -189,11 +199,20 @@ int admit_one(rvf_server* sv, Req* r) {
   int rc = rvf_mesh_upload(s, &r->mesh.d, &r->m);
   if (rc) return rc;
   r->mesh.drop();
-  if (!r->quad) return RVF_OK;
   std::lock_guard<std::mutex> lk(s->mu);
   cudaSetDevice(s->device);
   rvf_mesh* m = r->m;
   if ((rc = validate_options(m, &r->opts))) return rc;
+  if (!r->quad) {
+    const int64_t N = m->N, nT = (N + kTile - 1) / kTile;
+    if (m->mc_area.bytes < sizeof(double) * std::max<int64_t>(N, 1))
+      if ((rc = m->mc_area.alloc(s, sizeof(double) * std::max<int64_t>(N, 1)))) return rc;
+    if (m->F.bytes < sizeof(double) * N * N)
+      if ((rc = m->F.alloc(s, sizeof(double) * std::max<int64_t>(N * N, 1)))) return rc;
+    m->has_result = false;
+    r->mc_tiles = nT * (nT + 1) / 2;
+    return RVF_OK;
+  }
   if (r->opts.precision == RVF_PREC_MIXED && !(r->opts.near_field_factor >= 0.0))
     return set_err(RVF_EINVAL, "near_field_factor must be >= 0");
   if ((rc = ensure_tables(s, m, r->opts.nquad, &r->T))) return rc;
@@ -282,7 +301,7 @@ void run_chunk(rvf_server* sv, std::vector<Req*>& batch) {
     std::lock_guard<std::mutex> lk(s->mu);
     cudaSetDevice(s->device);
     cudaMemsetAsync(s->err.ptr, 0, sizeof(int), s->stream);
-    rc = wave_chunk(s, w.data(), (int)w.size(), sv->o.use_graphs >= 0, &info, gen, trace);
+    rc = wave_chunk(s, w.data(), (int)w.size(), sv->o.use_graphs >= 0, &info, gen, trace, kChunkPointPairs);
     if (!rc) rc = read_err(s);
   }
   const double ms = std::chrono::duration<double, std::milli>(Clock::now() - c0).count();
@@ -350,14 +369,49 @@ void run_chunk(rvf_server* sv, std::vector<Req*>& batch) {
   }
 }
 
-void run_mc(rvf_server* sv, Req* r) {
-  const int rc = rvf_solve(sv->s, r->m, &r->opts, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr);
+// One chunk of a Monte Carlo request (the area rule on its first chunk);
+// finishes the request after its last tile.
+void run_mc_chunk(rvf_server* sv, Req* r) {
+  Session* s = sv->s;
+  int rc = 0;
+  bool fin = false;
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    cudaSetDevice(s->device);
+    McArgs c{};
+    fill_mc_args(s, r->m, &r->opts, nullptr, c);
+    const double per = (double)kTile * kTile * std::max(1, r->opts.n_samples);
+    const int64_t budget = std::max<int64_t>(1, (int64_t)(kChunkSamplePairs / per));
+    c.tile0 = r->mc_claimed;
+    c.tile_count = std::min<int64_t>(r->mc_tiles - r->mc_claimed, budget);
+    c.area_pass = !r->mc_area_done;
+    cudaMemsetAsync(s->err.ptr, 0, sizeof(int), s->stream);
+    cudaMemsetAsync(s->tile_counter.ptr, 0, 8, s->stream);
+    cudaError_t e = launch_mc(c, s->sm_count, s->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+    rc = (e != cudaSuccess) ? cuda_err(e, "Monte Carlo chunk") : read_err(s);
+    if (!rc) {
+      r->mc_claimed += std::max<int64_t>(c.tile_count, 0);
+      r->mc_area_done = true;
+      if (r->mc_claimed >= r->mc_tiles) {
+        rc = run_reduce(s, r->m, r->m->mc_area.as<double>());
+        if (!rc && (e = cudaStreamSynchronize(s->stream)) != cudaSuccess) rc = cuda_err(e, "Monte Carlo finish");
+        if (!rc) {
+          r->m->has_result = true;
+          r->m->result_area = r->m->mc_area.as<double>();
+          fin = true;
+        }
+      }
+    }
+  }
   std::lock_guard<std::mutex> lk(sv->mu);
-  sv->active.erase(std::remove(sv->active.begin(), sv->active.end(), r), sv->active.end());
+  ++sv->chunks;
+  r->n_chunks += 1;
+  if (rc || fin) sv->active.erase(std::remove(sv->active.begin(), sv->active.end(), r), sv->active.end());
   if (rc) {
     finish(sv, r, RVF_REQ_FAILED, rc);
     drop_device(sv, r);
-  } else {
+  } else if (fin) {
     finish(sv, r, RVF_REQ_DONE, RVF_OK);
   }
 }
@@ -423,33 +477,29 @@ void worker_main(rvf_server* sv) {
         sv->active.push_back(r);
       }
     }
-    // next piece of work: a Monte Carlo request, else a chunk of the oldest request's class
+    // next piece of work: a chunk of the oldest admitted request -- Monte
+    // Carlo alone, quadrature together with every request of its class
     Req* mc = nullptr;
     std::vector<Req*> batch;
     {
       std::lock_guard<std::mutex> lk(sv->mu);
       const int maxb = (sv->o.max_batch >= 1 && sv->o.max_batch <= kMaxBatch) ? sv->o.max_batch : kMaxBatch;
+      const Req* head = nullptr;
       for (Req* r : sv->active)
-        if (!r->cancel && !r->quad) {
-          mc = r;
+        if (!r->cancel && (!r->quad || !r->w.done())) {
+          head = r;
           break;
         }
-      if (!mc) {
-        const Req* head = nullptr;
+      if (head && !head->quad) {
+        mc = const_cast<Req*>(head);
+      } else if (head) {
+        const uint64_t key = class_key(head);
         for (Req* r : sv->active)
-          if (!r->cancel && r->quad && !r->w.done()) {
-            head = r;
-            break;
-          }
-        if (head) {
-          const uint64_t key = class_key(head);
-          for (Req* r : sv->active)
-            if (!r->cancel && r->quad && !r->w.done() && class_key(r) == key && (int)batch.size() < maxb)
-              batch.push_back(r);
-        }
+          if (!r->cancel && r->quad && !r->w.done() && class_key(r) == key && (int)batch.size() < maxb)
+            batch.push_back(r);
       }
     }
-    if (mc) run_mc(sv, mc);
+    if (mc) run_mc_chunk(sv, mc);
     else if (!batch.empty()) run_chunk(sv, batch);
   }
 }

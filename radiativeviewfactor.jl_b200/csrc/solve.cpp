@@ -66,6 +66,38 @@ int validate_options(const rvf_mesh* m, const rvf_options* o) {
   return RVF_OK;
 }
 
+// Monte Carlo launch arguments of a whole solve (src/GPUMCKernels.jl:295-328).
+void fill_mc_args(Session* s, rvf_mesh* m, const rvf_options* o, uint8_t* ray_log, McArgs& c) {
+  const int64_t N = m->N;
+  const bool occ = o->occlusion && m->n_nodes > 0;
+  c = McArgs{};
+  c.N = N;
+  c.nT = (N + kTile - 1) / kTile;
+  c.n_tiles = c.nT * (c.nT + 1) / 2;
+  c.tile0 = 0;
+  c.tile_count = c.n_tiles;
+  c.area_pass = true;
+  c.n_samples = o->n_samples;
+  c.seed = o->seed;
+  c.exclude = o->mc_exclude_groups != 0 || m->dim == 1;
+  c.dim3 = (m->dim == 2);
+  c.coords = m->coords.as<double>();
+  c.enodes = m->enodes.as<int32_t>();
+  c.fam = m->fam.as<int8_t>();
+  c.group = m->group.as<int32_t>();
+  c.orig = m->orig.as<int32_t>();
+  c.inv = m->inv.as<int32_t>();
+  c.area_orig = m->mc_area.as<double>();
+  c.F = m->F.as<double>();
+  c.nodes = occ ? m->nodes.as<NodeD>() : nullptr;
+  c.n_nodes = occ ? m->n_nodes : 0;
+  c.tris = occ ? (o->geometric_soup ? m->tris_geo.as<TriD>() : m->tris_ref.as<TriD>()) : nullptr;
+  c.segs = occ ? m->segs.as<SegD>() : nullptr;
+  c.tile_counter = s->tile_counter.as<unsigned long long>();
+  c.counters = s->counters.as<unsigned long long>();
+  c.ray_log = ray_log;
+}
+
 int run_reduce(Session* s, rvf_mesh* m, const double* area) {
   const int64_t N = m->N;
   if (N == 0 || m->G == 0) return RVF_OK;
@@ -346,28 +378,7 @@ int rvf_solve(rvf_session* s, rvf_mesh* m, const rvf_options* o, double* F_elem,
   const bool occ = o->occlusion && m->n_nodes > 0;
   if (mc) {  // src/GPUMCKernels.jl:295-328
     McArgs c{};
-    c.N = N;
-    c.nT = (N + kTile - 1) / kTile;
-    c.n_tiles = c.nT * (c.nT + 1) / 2;
-    c.n_samples = o->n_samples;
-    c.seed = o->seed;
-    c.exclude = o->mc_exclude_groups != 0 || m->dim == 1;
-    c.dim3 = (m->dim == 2);
-    c.coords = m->coords.as<double>();
-    c.enodes = m->enodes.as<int32_t>();
-    c.fam = m->fam.as<int8_t>();
-    c.group = m->group.as<int32_t>();
-    c.orig = m->orig.as<int32_t>();
-    c.inv = m->inv.as<int32_t>();
-    c.area_orig = m->mc_area.as<double>();
-    c.F = m->F.as<double>();
-    c.nodes = occ ? m->nodes.as<NodeD>() : nullptr;
-    c.n_nodes = occ ? m->n_nodes : 0;
-    c.tris = occ ? (o->geometric_soup ? m->tris_geo.as<TriD>() : m->tris_ref.as<TriD>()) : nullptr;
-    c.segs = occ ? m->segs.as<SegD>() : nullptr;
-    c.tile_counter = s->tile_counter.as<unsigned long long>();
-    c.counters = s->counters.as<unsigned long long>();
-    c.ray_log = o->ray_log ? log.as<uint8_t>() : nullptr;
+    fill_mc_args(s, m, o, o->ray_log ? log.as<uint8_t>() : nullptr, c);
     if (N > 0) {
       EvTimer t(s->stream);
       cudaError_t e = launch_mc(c, s->sm_count, s->stream);

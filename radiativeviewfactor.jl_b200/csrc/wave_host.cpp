@@ -203,16 +203,32 @@ cudaError_t enqueue_chunk(Session* s, const WaveShape& sh, bool events) {
 
 }  // namespace
 
-int wave_chunk(Session* s, WaveReq* const* reqs, int n, bool use_graph, ChunkInfo* info, int gen_bps, int trace_bps) {
-  if (n < 1 || n > kMaxBatch) return set_err(RVF_EINVAL, "batch of %d requests (1..%d)", n, kMaxBatch);
+int wave_chunk(Session* s, WaveReq* const* reqs_in, int n_in, bool use_graph, ChunkInfo* info, int gen_bps,
+               int trace_bps, double pp_budget) {
+  if (n_in < 1 || n_in > kMaxBatch) return set_err(RVF_EINVAL, "batch of %d requests (1..%d)", n_in, kMaxBatch);
   int rc = 0;
   if ((rc = ensure_blocks(s))) return rc;
-  WaveShape sh = wave_shape(s, reqs, n);
+  // tiles offered to this launch, in request order: all that remain, or as
+  // many as the point-pair budget allows (the oldest requests first)
+  std::vector<WaveReq*> reqs;
+  std::vector<int64_t> offer;
+  double left = pp_budget > 0 ? pp_budget : 1e300;
+  for (int r = 0; r < n_in && left > 0; ++r) {
+    const int64_t rem = reqs_in[r]->n_tiles - reqs_in[r]->claimed;
+    if (rem <= 0) continue;
+    const double per = (double)kTile * kTile * reqs_in[r]->pmax * reqs_in[r]->pmax;
+    const int64_t take = (left >= per * (double)rem) ? rem : std::max<int64_t>(1, (int64_t)std::ceil(left / per));
+    reqs.push_back(reqs_in[r]);
+    offer.push_back(take);
+    left -= per * (double)take;
+  }
+  if (reqs.empty()) return RVF_OK;
+  const int n = (int)reqs.size();
+  WaveShape sh = wave_shape(s, reqs.data(), n);
   sh.gen_bps = gen_bps;
   sh.trace_bps = trace_bps;
-  // tiles still to claim, per request, in launch order
   std::vector<int64_t> base(n + 1, 0);
-  for (int r = 0; r < n; ++r) base[r + 1] = base[r] + (reqs[r]->n_tiles - reqs[r]->claimed);
+  for (int r = 0; r < n; ++r) base[r + 1] = base[r] + offer[r];
   WaveQ q{};
   if ((rc = ensure_wave(s, sh.mixed && sh.occ, sh.occ, sh.pmax_max, base[n], q))) return rc;
   std::vector<PairArgs> pa(n);

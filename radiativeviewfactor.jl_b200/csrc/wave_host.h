@@ -38,8 +38,10 @@ WaveShape wave_shape(Session* s, WaveReq* const* reqs, int n);
 // tiles in request order while the queues have room, traces and resolves
 // them, and advances each request's progress.  use_graph replays a CUDA
 // graph captured per launch shape (eager launch when capture is refused).
-// gen_bps / trace_bps: blocks per SM of the two grids (0 = occupancy limit).
+// gen_bps / trace_bps: blocks per SM of the two grids (0 = occupancy limit);
+// pp_budget > 0 caps the point pairs (worst case 32 x 32 x pmax^2 per tile)
+// offered to the launch, given to the requests in order.
 int wave_chunk(Session* s, WaveReq* const* reqs, int n, bool use_graph, ChunkInfo* info, int gen_bps = 0,
-               int trace_bps = 0);
+               int trace_bps = 0, double pp_budget = 0.0);
 
 }  // namespace rvf
