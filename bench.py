@@ -42,11 +42,12 @@ FLOP_TRI = 51
 # Reference-order traversal counts of the bench workloads: node (box) tests
 # and triangle tests of the reference's stackless walk (src/GPUBVH.jl:202-285)
 # ray by ray, from the oracle's instrumented FP64 traversal
-# (oracle.pyoracle.solve_plain(Mesh(md, [7]), 3) counters [1..3]).  Every
+# (oracle/ref_counts.py, which prints these numbers).  Every
 # cast ray's first box test (the root) runs in the generation kernel, so the
 # traversal kernels' algorithmic work is 12 (node_visits - n_rays) + 51 prim_tests.
 REF_COUNTS = {
     "medium": {"n_rays": 975146106, "node_visits": 5688464541, "prim_tests": 3647097481},
+    "full": {"n_rays": 38102400000, "node_visits": 222278703194, "prim_tests": 142516108216},
 }
 # DRAM bytes per traced ray of the traversal kernels (dram__bytes_read.sum +
 # dram__bytes_write.sum of one ncu capture on the medium workload divided by
@@ -65,15 +66,42 @@ def load_pkg():
     return mod
 
 
-def workload(rvf, size: str):
+class Workload:
+    """One bench configuration: mesh, obstruction groups and solve options."""
+
+    def __init__(self, md, desc, obs, nquad, method="quadrature", use_duffy=False, n_samples=64, seed=1,
+                 precisions=("fp64", "mixed")):
+        self.md, self.desc, self.obs, self.nquad = md, desc, list(obs), nquad
+        self.method, self.use_duffy, self.n_samples, self.seed = method, use_duffy, n_samples, seed
+        self.precisions = list(precisions)
+
+    def options(self, rvf, prec):
+        return rvf.make_options(self.nquad, monte_carlo=self.method == "mc", n_samples=self.n_samples,
+                                use_duffy=self.use_duffy, seed=self.seed, precision=prec)
+
+
+def workload(rvf, size: str) -> Workload:
+    M = rvf.meshes
     if size == "small":  # quick check of the same shape at m = 12
-        return rvf.meshes.cube_enclosure(12, box_m=4), "cube 12x12/face Tri3 (1,728 elements) + box"
+        return Workload(M.cube_enclosure(12, box_m=4), "cube 12x12/face Tri3 (1,728 elements) + box", OBSTRUCTION,
+                        NQUAD)
     if size == "medium":  # profiling size: F = 382 MB > L2, same box
-        return (rvf.meshes.cube_enclosure(24, jitter=0.3, seed=2, box=True, box_edge=0.3, box_m=12),
-                "cube 24x24/face jittered Tri3 (6,912 elements) + centred 0.3 box (1,728 tris), nquad=3")
-    return (rvf.meshes.cube_enclosure(60, jitter=0.3, seed=2, box=True, box_edge=0.3, box_m=12),
-            "closed cube 60x60/face jittered Tri3 (43,200 elements) + centred 0.3 box (1,728 tris), "
-            "Dunavant 7-pt (nquad=3), dense FP64 F")
+        return Workload(M.cube_enclosure(24, jitter=0.3, seed=2, box=True, box_edge=0.3, box_m=12),
+                        "cube 24x24/face jittered Tri3 (6,912 elements) + centred 0.3 box (1,728 tris), nquad=3",
+                        OBSTRUCTION, NQUAD)
+    if size == "c3":  # precision form with Duffy
+        return Workload(M.cylinder(nc=64, na=32, caps=True, cap_rings=8, jitter=0.01, seed=3),
+                        "open cylinder r=0.5 h=1, 64x32 Quad8 wall + two 64x8 Quad8 annular caps sharing the end "
+                        "rings (3,072 elements), +-1% radial jitter, use_duffy, nquad=5, no obstruction", [], 5,
+                        use_duffy=True)
+    if size == "c4":  # Monte Carlo 2-D
+        return Workload(M.cavity_2d(n_wall=800, n_circle=200, n_circles=4, seed=4),
+                        "1x1 cavity, 4 x 800 Line3 walls + 4 circles r=0.1 x 200 Line3 (4,000 elements), circles "
+                        "as obstruction, stratified Monte Carlo 64 samples (8x8), seed 4", [5, 6, 7, 8], 3,
+                        method="mc", n_samples=64, seed=4, precisions=("fp64",))
+    return Workload(M.cube_enclosure(60, jitter=0.3, seed=2, box=True, box_edge=0.3, box_m=12),
+                    "closed cube 60x60/face jittered Tri3 (43,200 elements) + centred 0.3 box (1,728 tris), "
+                    "Dunavant 7-pt (nquad=3), dense FP64 F", OBSTRUCTION, NQUAD)
 
 
 class Clocks:
@@ -155,32 +183,42 @@ def barrier(ws: int):
         dist.barrier()
 
 
-def cpu_baseline(rvf, md, seconds: float, offset: int = 0):
+def cpu_baseline(rvf, W: Workload, seconds: float, offset: int = 0):
     """The reference's CPU path (src/Assembly.jl:102-225, restated in
-    oracle/) on every `stride`-th row, all host threads; pairs/s."""
+    oracle/; Monte Carlo: the restated src/GPUMCKernels.jl streams) on every
+    `stride`-th row, all host threads; pairs/s."""
     if str(ROOT) not in sys.path:
         sys.path.insert(0, str(ROOT))
     from oracle import pyoracle as orc
-    m = orc.Mesh(md, OBSTRUCTION)
+    md = W.md
+    m = orc.Mesh(md, W.obs)
     N = md.n_elems
     cores = os.cpu_count() or 1
+
+    def run(begin, stride):
+        if W.method == "mc":
+            orc.solve_mc(m, W.n_samples, W.seed, row_begin=begin, row_stride=stride, threads=cores)
+        else:
+            orc.solve_cpu(m, W.nquad, use_duffy=W.use_duffy, row_begin=begin, row_stride=stride, threads=cores)
+
     # calibrate on 2 rows per thread
     probe = max(2 * cores, 8)
     stride0 = max(1, N // probe)
     t0 = time.perf_counter()
-    orc.solve_cpu(m, NQUAD, row_begin=offset % stride0, row_stride=stride0, threads=cores)
+    run(offset % stride0, stride0)
     dt = time.perf_counter() - t0
     pairs0 = sum(N - 1 - i for i in range(offset % stride0, N, stride0))
     rate = pairs0 / max(dt, 1e-9)
     stride = max(1, int(N * (N / 2) / max(rate * seconds, 1.0)))
     begin = offset % stride
     t0 = time.perf_counter()
-    orc.solve_cpu(m, NQUAD, row_begin=begin, row_stride=stride, threads=cores)
+    run(begin, stride)
     dt = time.perf_counter() - t0
     pairs = sum(N - 1 - i for i in range(begin, N, stride))
+    what = ("Monte Carlo streams of the GPU path" if W.method == "mc" else
+            "CPU path with one BVH per active obstruction subset" + (", Duffy pairs" if W.use_duffy else ""))
     return {"value": pairs / dt, "unit": UNIT, "cores": cores, "kind": "port",
-            "sample": f"rows {begin}::{stride} of {N} ({pairs:,} pairs, {dt:.1f} s), CPU path with one "
-                      f"BVH per active obstruction subset, OpenMP over rows"}
+            "sample": f"rows {begin}::{stride} of {N} ({pairs:,} pairs, {dt:.1f} s), {what}, OpenMP over rows"}
 
 
 def run_reference(args):
@@ -188,10 +226,11 @@ def run_reference(args):
     if rank != 0:
         return
     rvf = load_pkg()
-    md, desc = workload(rvf, args.size)
+    W = workload(rvf, args.size)
+    md, desc = W.md, W.desc
     samples = []
     for k in range(args.warmup + args.steps):
-        r = cpu_baseline(rvf, md, args.ref_seconds, offset=k * 7919)
+        r = cpu_baseline(rvf, W, args.ref_seconds, offset=k * 7919)
         if k >= args.warmup:
             samples.append(r)
     v = statistics.median(s["value"] for s in samples)
@@ -199,7 +238,7 @@ def run_reference(args):
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * (N * (N - 1) / 2) / v,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": desc, "n_elems": N, "nquad": NQUAD},
+            "config": {"workload": desc, "n_elems": N, "nquad": W.nquad},
             "cpu_baseline": {**samples[-1], "value": v},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -246,8 +285,41 @@ def roofline(stats, peak, bound, kernel, prec, size):
             "traffic_source": "ncu capture of the medium workload scaled by traced rays" if tpr else None}
 
 
+# Monte Carlo sample pair on Line3 curves: two element evaluations (45 flop
+# each), the 2-D kernel (26) and the accumulation (2); a 2-D segment test is
+# 14 flop, a box test 12.
+FLOP_MC_LINE3 = 45 + 45 + 26 + 2
+FLOP_SEG = 14
+
+
+def roof_for(W: Workload, stats, prec, size, peak64, peak32):
+    """Roofline of the workload's dominant kernel."""
+    peak, bound = (peak32, "fp32_fma") if prec == "mixed" else (peak64, "fp64_fma")
+    s0 = stats[-1]
+    if W.method == "mc":
+        ms = statistics.mean(s["ms_pairs"] for s in stats)
+        flops = FLOP_MC_LINE3 * s0["n_point_pairs"] + FLOP_SLAB * s0["node_visits"] + FLOP_SEG * s0["prim_tests"]
+        achieved = flops / (ms / 1e3) / 1e12
+        return {"bound": bound, "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                "traffic": None, "peak_source": "measured by rvf_fma_peak (FMA microbenchmark) in this run",
+                "kernel": "k_pairs_mc<DIM3=0,OCC=1> (+ k_mc_area)", "kernel_ms_per_launch": ms,
+                "launches_per_step": 1, "algorithmic_flop_per_launch": flops,
+                "work_counts": "sample pairs, box and segment tests as executed"}
+    if not W.obs:
+        ms = statistics.mean(s["ms_gen"] for s in stats)
+        flops = FLOP_POINT_PAIR * s0["n_point_pairs"]
+        achieved = flops / (ms / 1e3) / 1e12
+        return {"bound": bound, "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                "traffic": None, "peak_source": "measured by rvf_fma_peak (FMA microbenchmark) in this run",
+                "kernel": "k_gen_mixed<OCC=0>" if prec == "mixed" else "k_gen_fp64<DIM3=1,OCC=0>",
+                "kernel_ms_per_launch": ms, "launches_per_step": 1, "algorithmic_flop_per_launch": flops,
+                "work_counts": "23 flop per quadrature point pair (Duffy pairs run in k_duffy, timed in phases)"}
+    kernel = "k_trace32 (+ k_trace64 re-traversal)" if prec == "mixed" else "k_trace64<DIM3=1>"
+    return roofline(stats, peak, bound, kernel, prec, size)
+
+
 def phases(stats):
-    keys = ("ms_gen", "ms_trace", "ms_trace_fp64", "ms_resolve", "ms_prep", "ms_reduce")
+    keys = ("ms_gen", "ms_trace", "ms_trace_fp64", "ms_resolve", "ms_duffy", "ms_pairs", "ms_prep", "ms_reduce")
     d = {k: statistics.mean(s[k] for s in stats) for k in keys}
     d["n_chunks"] = int(stats[-1]["n_chunks"])
     d["n_rays_traced"] = int(stats[-1]["n_rays_traced"])
@@ -404,18 +476,21 @@ def run_ours(args):
     from rvf_b200 import _abi
     if not _abi.LIB_PATH.exists():
         raise SystemExit("librvf_b200.so is not built (run __graft_entry__.build())")
-    md, desc = workload(rvf, args.size)
+    W = workload(rvf, args.size)
+    md, desc = W.md, W.desc
     N = md.n_elems
     G = len(md.group_tags)
     pairs = N * (N - 1) // 2
     sess = _abi.Session(local)
-    arrays = rvf.mesh_desc_arrays(md, OBSTRUCTION)
+    arrays = rvf.mesh_desc_arrays(md, W.obs)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")
-    precisions = ["fp64", "mixed"] if args.precision == "both" else [args.precision]
+    precisions = W.precisions if args.precision == "both" else [p for p in W.precisions if p == args.precision]
+    if not precisions:
+        raise SystemExit(f"--precision {args.precision} is not available for --size {args.size}")
     head = precisions[-1]
     runs, meshes = {}, {}
     for prec in precisions:
-        opts = rvf.make_options(NQUAD, precision=prec, seed=1)
+        opts = W.options(rvf, prec)
         dm = _abi.DeviceMesh(sess, arrays)
         stats, clocks = timed_solves(dm, opts, args.steps, args.warmup, flush, ws, local)
         total_ms = allreduce_max(sum(s["ms_total"] for s in stats), ws)
@@ -438,15 +513,12 @@ def run_ours(args):
     peak64 = _abi.fma_peak(local, True)
     peak32 = _abi.fma_peak(local, False)
     H = runs[head]
-    if head == "mixed":
-        roof = roofline(H["stats"], peak32, "fp32_fma", "k_trace32 (+ k_trace64 re-traversal)", "mixed", args.size)
-    else:
-        roof = roofline(H["stats"], peak64, "fp64_fma", "k_trace64<DIM3=1>", "fp64", args.size)
+    roof = roof_for(W, H["stats"], head, args.size, peak64, peak32)
 
     # ---- e2e: through the C ABI with host buffers ----
     e2e = None
     if not args.no_e2e:
-        opts = rvf.make_options(NQUAD, precision=head, seed=1)
+        opts = W.options(rvf, head)
         h2d = sum(a.nbytes for k, a in arrays.items() if hasattr(a, "nbytes")) + sum(t.nbytes for t in arrays["nodes"])
         d2h = 8 * (N * N + N + G * G + G)
         try:
@@ -461,7 +533,7 @@ def run_ours(args):
         for k in range(args.e2e_warmup + args.e2e_steps):
             barrier(ws)
             t0 = time.perf_counter()
-            d = _abi.DeviceMesh(sess, rvf.mesh_desc_arrays(md, OBSTRUCTION))
+            d = _abi.DeviceMesh(sess, rvf.mesh_desc_arrays(md, W.obs))
             d.solve(opts, F, A, Fg, Ag)
             d.release()
             t1 = time.perf_counter()
@@ -479,7 +551,8 @@ def run_ours(args):
             "warmup": args.warmup, "ms_per_step": H["ms"], "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64" if head == "fp64" else "f32+f64",
             "data": "synthetic",
-            "config": {"workload": desc, "n_elems": N, "pairs_per_step": pairs, "nquad": NQUAD,
+            "config": {"workload": desc, "n_elems": N, "pairs_per_step": pairs, "nquad": W.nquad,
+                       "method": W.method, "use_duffy": W.use_duffy,
                        "precision": head, "parallelism": f"replicas x{ws} (independent meshes)",
                        "l2": "each step writes the dense F matrix (C2: 14.9 GB >> 126 MB L2); a 256 MB "
                              "buffer is also written between steps"},
@@ -492,14 +565,13 @@ def run_ours(args):
                                           "prim_tests", "n_rays_traced")}}
     if len(precisions) == 2:
         line["fp64"] = {"value": runs["fp64"]["value"], "ms_per_step": runs["fp64"]["ms"],
-                        "roofline": roofline(runs["fp64"]["stats"], peak64, "fp64_fma", "k_trace64<DIM3=1>", "fp64",
-                                             args.size),
+                        "roofline": roof_for(W, runs["fp64"]["stats"], "fp64", args.size, peak64, peak32),
                         "phases": phases(runs["fp64"]["stats"]),
                         "clocks": runs["fp64"]["clocks"]}
         line["mixed_over_fp64"] = runs["mixed"]["value"] / runs["fp64"]["value"]
         line["accuracy"] = accuracy
     if rank == 0 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(rvf, md, args.ref_seconds)
+        line["cpu_baseline"] = cpu_baseline(rvf, W, args.ref_seconds)
     if rank == 0 and args.serve != "none":
         line["serve"] = run_serve(rvf, sess, args.serve, local)
     if rank == 0:
@@ -518,7 +590,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--precision", choices=["fp64", "mixed", "both"], default="both")
-    ap.add_argument("--size", choices=["full", "medium", "small"], default="full")
+    ap.add_argument("--size", choices=["full", "medium", "small", "c3", "c4"], default="full",
+                    help="full: the headline workload (closed cube, 43,200 Tri3, occluded); c3: cylinder with "
+                         "Duffy pairs; c4: 2-D Monte Carlo cavity; medium / small: the headline shape at m = 24 / 12")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--e2e-warmup", type=int, default=1)
