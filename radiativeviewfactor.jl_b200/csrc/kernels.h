@@ -205,9 +205,6 @@ struct GenBatch {
   int n_req;
   int pmax_max;            // shared-memory layout and queue reservation
   int64_t total_tiles;
-  bool nodes_in_smem;      // one request only: its BVH nodes are staged in shared memory
-  const void* smem_nodes;  // NodeD (FP64) or NodeF (mixed) of that request
-  int n_nodes_smem;
   WaveQ q;
   unsigned long long* counters;
   int* err;
@@ -235,12 +232,12 @@ struct ResolveBatch {
 struct WaveShape {
   bool mixed, dim3, occ;
   int pmax_max;
-  bool gen_nodes_smem, trace64_nodes_smem, trace32_nodes_smem;
+  bool trace64_nodes_smem, trace32_nodes_smem;
   int n_nodes_smem;
   int gen_bps, trace_bps;  // blocks per SM of the generation / traversal grids (0 = occupancy limit)
 };
 
-size_t gen_smem_bytes(bool mixed, int pmax, int n_nodes_smem, bool occ);
+size_t gen_smem_bytes(bool mixed, int pmax, bool occ);
 size_t trace_smem_bytes(bool fp32, int n_nodes_smem);
 // Generation, traversal and resolve of one chunk; the batch structs are
 // device pointers.

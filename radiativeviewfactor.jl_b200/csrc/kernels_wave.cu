@@ -77,6 +77,46 @@ __device__ __forceinline__ void stage_flush(uint64_t* st, int& n, int k, uint64_
   __syncwarp();
 }
 
+// Per-lane runs of queue records.  Each lane collects the deferred rays of
+// its own pair in a ring of kRun records in shared memory (entry k of thread t
+// at ring[k * 256 + t]) and appends it to the queue as one contiguous run when
+// it is full and when the pair ends.  A traversal warp takes 32 consecutive
+// records, so its rays come from one or two pairs -- thin bundles whose walks
+// agree -- instead of one ray from each of 32 pairs.
+constexpr int kRun = 16;
+
+__device__ __forceinline__ void run_push(uint64_t* ring, int& nr, bool push, uint64_t rec) {
+  if (push) {
+    ring[nr * 256] = rec;
+    ++nr;
+  }
+}
+
+// Appends the full runs (all runs when `all`) of the warp's lanes, lane by
+// lane, with one counter update.  Warp-uniform call.
+__device__ __forceinline__ void run_flush(uint64_t* ring, int& nr, bool all, uint64_t* queue,
+                                          unsigned long long* count, unsigned long long* tile_used) {
+  const int lane = threadIdx.x & 31;
+  const int mine = (all || nr == kRun) ? nr : 0;
+  int incl = mine;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int v = __shfl_up_sync(kFull, incl, o);
+    if (lane >= o) incl += v;
+  }
+  const int total = __shfl_sync(kFull, incl, 31);
+  if (total == 0) return;
+  unsigned long long base = 0;
+  if (lane == 0) {
+    base = atomicAdd(count, (unsigned long long)total);
+    atomicAdd(tile_used, (unsigned long long)total);
+  }
+  base = __shfl_sync(kFull, base, 0);
+  uint64_t* dst = queue + base + (incl - mine);
+  for (int k = 0; k < mine; ++k) dst[k] = ring[k * 256];
+  if (mine > 0) nr = 0;
+}
+
 // Gives lanes with `need` a fresh pending-pair slot and clears its visibility words.
 __device__ __forceinline__ void slot_alloc(const WaveQ& q, bool need, int64_t& slot, unsigned long long* tile_slots) {
   const uint32_t m = __ballot_sync(kFull, need);
@@ -160,6 +200,12 @@ __device__ __forceinline__ bool pair_misses_box(const double* ci, const double* 
   return te > tx;
 }
 
+// bytes of one tile block of the quadrature table in shared memory (a
+// multiple of 128: kComp * pmax * 32 elements of 4 or 8 bytes)
+__host__ __device__ __forceinline__ size_t gen_tab_bytes(bool mixed, int pmax) {
+  return (size_t)kComp * pmax * kTile * (mixed ? sizeof(float) : sizeof(double));
+}
+
 // request r of the launch with tile_base[r] <= t < tile_base[r+1]
 __device__ __forceinline__ int find_req(const int64_t* tile_base, int n_req, int64_t t) {
   int lo = 0, hi = n_req - 1;
@@ -182,20 +228,14 @@ __global__ void __launch_bounds__(256, 3) k_gen_fp64(const GenBatch* __restrict_
   const GenBatch& L = *Lp;
   const int pmL = L.pmax_max;
   double* iblk = reinterpret_cast<double*>(smem);
-  NodeD* snodes = reinterpret_cast<NodeD*>(iblk + kComp * pmL * kTile);
-  uint64_t* stage_all = reinterpret_cast<uint64_t*>(snodes + (L.nodes_in_smem ? L.n_nodes_smem : 0));
-  uint64_t* bar = stage_all + (OCC ? 8 * 64 : 0);
+  uint64_t* ring = reinterpret_cast<uint64_t*>(iblk + kComp * pmL * kTile) + threadIdx.x;
+  uint64_t* bar = reinterpret_cast<uint64_t*>(iblk + kComp * pmL * kTile) + (OCC ? kRun * 256 : 0);
   __shared__ int64_t s_tile;
   __shared__ int s_req;
   __shared__ unsigned long long s_used, s_slots;
+  __shared__ NodeD s_root;  // the request's root box: the only node the generation tests
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  uint64_t* stage = stage_all + warp * 64;
-  if (OCC && L.nodes_in_smem) {
-    const int4* src = reinterpret_cast<const int4*>(L.smem_nodes);
-    int4* dst = reinterpret_cast<int4*>(snodes);
-    for (int k = threadIdx.x; k < L.n_nodes_smem * 4; k += blockDim.x) dst[k] = src[k];
-  }
   if (threadIdx.x == 0) mbar_init(bar, 1);
   __syncthreads();
 
@@ -214,6 +254,7 @@ __global__ void __launch_bounds__(256, 3) k_gen_fp64(const GenBatch* __restrict_
         const PairArgs& a = L.reqs[r];
         s_req = r;
         s_tile = g - L.tile_base[r] + a.tile0;
+        if (OCC) s_root = a.nodes[0];
         int64_t bi, bj;
         tile_coords(s_tile, a.nT, bi, bj);
         const uint32_t blk_bytes = (uint32_t)(kComp * a.pmax * kTile * sizeof(double));
@@ -227,7 +268,6 @@ __global__ void __launch_bounds__(256, 3) k_gen_fp64(const GenBatch* __restrict_
     const int req = s_req;
     const PairArgs& a = L.reqs[req];
     const int pm = a.pmax;
-    const NodeD* nodes = L.nodes_in_smem ? snodes : a.nodes;
     int64_t bi, bj;
     tile_coords(t, a.nT, bi, bj);
     const bool ok = mbar_wait_bounded(bar, phase);
@@ -266,10 +306,10 @@ __global__ void __launch_bounds__(256, 3) k_gen_fp64(const GenBatch* __restrict_
       // pairs whose rays all certainly miss the root box need no ray at all
       const bool cullp = OCC && npj > 0 && a.rad &&
                          pair_misses_box<DIM3>(a.cen + 3 * i, a.cen + 3 * j, fmax(a.rad[i], a.rad[j]) + a.cull_margin,
-                                               nodes[0]);
+                                               s_root);
       double acc = 0.0;
       int64_t slot = -1;
-      int nst = 0;
+      int nr = 0;
       for (int q = 0; q < qmax; ++q) {
         const bool lq = q < npj;
         double xj[3], nj[3], wj;
@@ -302,7 +342,7 @@ __global__ void __launch_bounds__(256, 3) k_gen_fp64(const GenBatch* __restrict_
           n_pp += lq ? 1 : 0;
           if (OCC) {
             bool cast, defer = false;
-            const NodeD& root = nodes[0];
+            const NodeD& root = s_root;
             if (cullp) {
               cast = (K > 0.0) && (!DIM3 || sqrt(r2) > 1e-15);  // make_ray's cast rule
             } else if (DIM3) {
@@ -322,8 +362,8 @@ __global__ void __launch_bounds__(256, 3) k_gen_fp64(const GenBatch* __restrict_
             if (logp && cast && !defer) logp[sw ? q * a.log_pm + p : p * a.log_pm + q] = 1;
             if (__any_sync(kFull, defer)) {
               slot_alloc(Q, defer && slot < 0, slot, &s_slots);
-              stage_push(stage, nst, defer, rec_make(slot, sw, p, q));
-              if (nst >= 32) stage_flush(stage, nst, 32, Q.rec64, Q.ctr + kCtrRec64, &s_used);
+              run_push(ring, nr, defer, rec_make(slot, sw, p, q));
+              if (__any_sync(kFull, nr == kRun)) run_flush(ring, nr, false, Q.rec64, Q.ctr + kCtrRec64, &s_used);
               if (defer) K = 0.0;
             }
           }
@@ -331,7 +371,7 @@ __global__ void __launch_bounds__(256, 3) k_gen_fp64(const GenBatch* __restrict_
         }
         acc = fma(wj, inner, acc);
       }
-      if (OCC && nst > 0) stage_flush(stage, nst, nst, Q.rec64, Q.ctr + kCtrRec64, &s_used);
+      if (OCC && __any_sync(kFull, nr > 0)) run_flush(ring, nr, true, Q.rec64, Q.ctr + kCtrRec64, &s_used);
       if (slot >= 0) {
         PendSlot ps;
         ps.i = (int32_t)i;
@@ -411,21 +451,19 @@ __global__ void __launch_bounds__(256, 2) k_gen_mixed(const GenBatch* __restrict
   const GenBatch& L = *Lp;
   const int pmL = L.pmax_max;
   float* iblk = reinterpret_cast<float*>(smem);
-  NodeF* snodes = reinterpret_cast<NodeF*>(smem + (size_t)kComp * pmL * kTile * sizeof(float));
-  uint64_t* stage_all = reinterpret_cast<uint64_t*>(snodes + (L.nodes_in_smem ? L.n_nodes_smem : 0));
-  uint64_t* bar = stage_all + (OCC ? 8 * 128 : 0);
+  // FP32 rays: per-lane runs; FP64 rays (near field, grazing, unusable
+  // directions, a few per cent): per-warp staging
+  uint64_t* stage_all = reinterpret_cast<uint64_t*>(smem + gen_tab_bytes(true, pmL));
+  uint64_t* ring = stage_all + (OCC ? 8 * 64 : 0) + threadIdx.x;
+  uint64_t* bar = stage_all + (OCC ? 8 * 64 + kRun * 256 : 0);
   __shared__ int64_t s_tile;
   __shared__ int s_req;
   __shared__ unsigned long long s_used, s_slots;
+  __shared__ NodeF s_rootf;  // the request's root box, FP32 and FP64
+  __shared__ NodeD s_root;
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  uint64_t* st64 = stage_all + warp * 128;
-  uint64_t* st32 = st64 + 64;
-  if (OCC && L.nodes_in_smem) {
-    const int4* src = reinterpret_cast<const int4*>(L.smem_nodes);
-    int4* dst = reinterpret_cast<int4*>(snodes);
-    for (int k = threadIdx.x; k < L.n_nodes_smem * 2; k += blockDim.x) dst[k] = src[k];
-  }
+  uint64_t* st64 = stage_all + warp * 64;
   if (threadIdx.x == 0) mbar_init(bar, 1);
   __syncthreads();
 
@@ -444,6 +482,10 @@ __global__ void __launch_bounds__(256, 2) k_gen_mixed(const GenBatch* __restrict
         const MixedArgs& a = L.mreqs[r];
         s_req = r;
         s_tile = g - L.tile_base[r] + a.tile0;
+        if (OCC) {
+          s_rootf = a.nodesf[0];
+          s_root = a.nodes[0];
+        }
         int64_t bi, bj;
         tile_coords(s_tile, a.nT, bi, bj);
         const uint32_t blk_bytes = (uint32_t)(kComp * a.pmax * kTile * sizeof(float));
@@ -457,7 +499,6 @@ __global__ void __launch_bounds__(256, 2) k_gen_mixed(const GenBatch* __restrict
     const int req = s_req;
     const MixedArgs& a = L.mreqs[req];
     const int pm = a.pmax;
-    const NodeF* nodesf = L.nodes_in_smem ? snodes : a.nodesf;
     int64_t bi, bj;
     tile_coords(t, a.nT, bi, bj);
     const bool ok = mbar_wait_bounded(bar, phase);
@@ -505,14 +546,14 @@ __global__ void __launch_bounds__(256, 2) k_gen_mixed(const GenBatch* __restrict
       const double* it64 = a.tab + bi * kComp * pm * kTile + li;
       const bool cullp = OCC && npj > 0 && a.rad &&
                          pair_misses_box<true>(a.cen + 3 * i, a.cen + 3 * j, fmax(a.rad[i], a.rad[j]) + a.cull_margin,
-                                               a.nodes[0]);
+                                               s_root);
       uint8_t* logp = (a.ray_log && valid)
                           ? a.ray_log + ((uint64_t)(sw ? oj : oi) * N + (sw ? oi : oj)) * a.log_pm * a.log_pm
                           : nullptr;
       double accd = 0.0;   // FP64 terms
       float acc32 = 0.0f;  // FP32 far-field terms
       int64_t slot = -1;
-      int n64 = 0, n32 = 0;
+      int n64 = 0, nr = 0;
       for (int q = 0; q < qmax; ++q) {
         const bool lq = q < npj;
         const bool far = lq && !near;
@@ -531,7 +572,11 @@ __global__ void __launch_bounds__(256, 2) k_gen_mixed(const GenBatch* __restrict
           const float r2 = fmaf(rx, rx, fmaf(ry, ry, rz * rz));
           const float di = fmaf(np0, rx, fmaf(np1, ry, np2 * rz));
           const float dj = -fmaf(nq0, rx, fmaf(nq1, ry, nq2 * rz));
-          const bool graze = far && (di * di <= 1e-10f * r2 || dj * dj <= 1e-10f * r2 || r2 < 1e-18f);
+          // Grazing point pairs (a cosine within 1e-5 of zero) take FP64 only
+          // with occlusion, where the sign of K decides whether a ray is cast.
+          // Without it the FP32 term's absolute error, ~2^-20 (|di|+|dj|)|r|/(pi r^4),
+          // is the same as for any other far-field term.
+          const bool graze = far && (r2 < 1e-18f || (OCC && (di * di <= 1e-10f * r2 || dj * dj <= 1e-10f * r2)));
           float K32 = 0.0f;
           if (far && !graze && di > 0.0f && dj > 0.0f) K32 = (di * dj) * rcp_approx(3.14159265f * (r2 * r2));
           const bool cast32 = far && !graze && K32 > 0.0f;
@@ -546,7 +591,7 @@ __global__ void __launch_bounds__(256, 2) k_gen_mixed(const GenBatch* __restrict
                 sw ? make_ray_f(xo, -rx, -ry, -rz, r2, a.delta, R) : make_ray_f(xo, rx, ry, rz, r2, a.delta, R);
             badray = !rok;
             if (rok) {
-              defer32 = slab_f(nodesf[0], R) != kMiss;
+              defer32 = slab_f(s_rootf, R) != kMiss;
               if (!defer32 && logp) logp[sw ? q * a.log_pm + p : p * a.log_pm + q] = 1;
             }
           }
@@ -556,14 +601,14 @@ __global__ void __launch_bounds__(256, 2) k_gen_mixed(const GenBatch* __restrict
           const bool need64 = lq && (near || graze || badray);
           bool defer64 = false;
           if (__any_sync(kFull, need64))
-            gen_mixed64<OCC>(a, a.nodes, it64, jb64, p, q, need64, near || graze, graze, sw, cullp,
+            gen_mixed64<OCC>(a, &s_root, it64, jb64, p, q, need64, near || graze, graze, sw, cullp,
                              (double)(wq * (wp * K32)), logp, defer64, accd, n_rays, n_rays64, n_graze);
           if (OCC && __any_sync(kFull, defer32 || defer64)) {
             slot_alloc(Q, (defer32 || defer64) && slot < 0, slot, &s_slots);
             stage_push(st64, n64, defer64, rec_make(slot, sw, p, q));
             if (n64 >= 32) stage_flush(st64, n64, 32, Q.rec64, Q.ctr + kCtrRec64, &s_used);
-            stage_push(st32, n32, defer32, rec_make(slot, sw, p, q));
-            if (n32 >= 32) stage_flush(st32, n32, 32, Q.rec32, Q.ctr + kCtrRec32, &s_used);
+            run_push(ring, nr, defer32, rec_make(slot, sw, p, q));
+            if (__any_sync(kFull, nr == kRun)) run_flush(ring, nr, false, Q.rec32, Q.ctr + kCtrRec32, &s_used);
           }
           if (far && !graze && !badray && !defer32) inner = fmaf(wp, K32, inner);
         }
@@ -571,7 +616,7 @@ __global__ void __launch_bounds__(256, 2) k_gen_mixed(const GenBatch* __restrict
       }
       if (OCC) {
         if (n64 > 0) stage_flush(st64, n64, n64, Q.rec64, Q.ctr + kCtrRec64, &s_used);
-        if (n32 > 0) stage_flush(st32, n32, n32, Q.rec32, Q.ctr + kCtrRec32, &s_used);
+        if (__any_sync(kFull, nr > 0)) run_flush(ring, nr, true, Q.rec32, Q.ctr + kCtrRec32, &s_used);
       }
       const double raw = accd + (double)acc32;
       if (slot >= 0) {
@@ -613,9 +658,24 @@ __device__ __forceinline__ void log_ray(const TraceArgs& a, int64_t i, int64_t j
   lp[sw ? q * a.log_pm + p : p * a.log_pm + q] = v;
 }
 
-__device__ __forceinline__ void set_visible(const WaveQ& Q, int64_t slot, int pm, int p, int q) {
+// Sets the (p, q) visibility bits of the warp's visible rays.  The rays of one
+// pair sit in consecutive lanes, so the bits of each run of lanes with the
+// same (slot, word) are OR-combined by a segmented scan and the last lane of
+// the run issues one atomicOr.  Lanes whose key also appears in a run further
+// back only add bits of that same word, which OR absorbs.  Warp-uniform call.
+__device__ __forceinline__ void set_visible_warp(const WaveQ& Q, bool vis, int64_t slot, int pm, int p, int q) {
+  const int lane = threadIdx.x & 31;
   const int b = p * pm + q;
-  atomicOr(reinterpret_cast<unsigned long long*>(Q.vis + slot * Q.vis_words + (b >> 6)), 1ull << (b & 63));
+  const long long key = vis ? (long long)(slot * Q.vis_words + (b >> 6)) : -1ll - lane;
+  unsigned long long bits = vis ? (1ull << (b & 63)) : 0ull;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const long long k2 = __shfl_up_sync(kFull, key, o);
+    const unsigned long long b2 = __shfl_up_sync(kFull, bits, o);
+    if (lane >= o && k2 == key) bits |= b2;
+  }
+  const long long next = __shfl_down_sync(kFull, key, 1);
+  if (vis && (lane == 31 || next != key)) atomicOr(reinterpret_cast<unsigned long long*>(Q.vis + key), bits);
 }
 
 // A queued ray: its record, its pair and its request.
@@ -693,7 +753,7 @@ __global__ void __launch_bounds__(256, 3) k_trace64(const TraceBatch* __restrict
       res = in_smem ? trace_batch(have, SwizNodes<NodeD>{reinterpret_cast<const int4*>(snodes)}, n_nodes, ws, pol, tc)
                             : trace_batch(have, GlobalNodes<NodeD>{a.nodes}, n_nodes, ws, pol, tc);
     }
-    if (have && res != kHit) set_visible(Q, x.slot, pm, x.p, x.q);
+    set_visible_warp(Q, have && res != kHit, x.slot, pm, x.p, x.q);
     if (have && a.ray_log) log_ray(a, x.i, x.j, x.sw, x.p, x.q, res == kHit ? 2 : 1);
   }
   const uint64_t s_nodes = warp_sum_u64(tc.nodes), s_prims = warp_sum_u64(tc.prims);
@@ -753,7 +813,7 @@ __global__ void __launch_bounds__(256, 4) k_trace32(const TraceBatch* __restrict
     const int res = in_smem
                         ? trace_batch(have, SwizNodes<NodeF>{reinterpret_cast<const int4*>(snodes)}, n_nodes, ws, pol, tc)
                         : trace_batch(have, GlobalNodes<NodeF>{a.nodesf}, n_nodes, ws, pol, tc);
-    if (have && res == kMiss) set_visible(Q, x.slot, pm, x.p, x.q);
+    set_visible_warp(Q, have && res == kMiss, x.slot, pm, x.p, x.q);
     if (have && a.ray_log && res != kUnsure) log_ray(a, x.i, x.j, x.sw, x.p, x.q, res == kHit ? 2 : 1);
     // uncertain rays go to the FP64 queue
     const bool uns = have && res == kUnsure;
@@ -890,11 +950,11 @@ __global__ void __launch_bounds__(256) k_resolve_mixed(const ResolveBatch* __res
 // ---------------------------------------------------------------------------
 // host launchers
 // ---------------------------------------------------------------------------
-size_t gen_smem_bytes(bool mixed, int pmax, int n_nodes_smem, bool occ) {
-  const size_t tab = (size_t)kComp * pmax * kTile * (mixed ? sizeof(float) : sizeof(double));
-  const size_t nodes = (size_t)n_nodes_smem * (mixed ? sizeof(NodeF) : sizeof(NodeD));
-  const size_t stage = occ ? (size_t)8 * (mixed ? 128 : 64) * sizeof(uint64_t) : 0;
-  return tab + nodes + stage + 16;
+size_t gen_smem_bytes(bool mixed, int pmax, bool occ) {
+  // tile block, then (occlusion) the per-warp FP64 staging (mixed) and the
+  // per-lane runs, then the mbarrier
+  const size_t stage = occ ? ((mixed ? (size_t)8 * 64 : 0) + (size_t)kRun * 256) * sizeof(uint64_t) : 0;
+  return gen_tab_bytes(mixed, pmax) + stage + 16;
 }
 
 size_t trace_smem_bytes(bool fp32, int n_nodes_smem) {
@@ -915,7 +975,7 @@ static int grid_for(F fn, size_t smem, int sm_count, int cap) {
 }
 
 cudaError_t launch_gen(const WaveShape& sh, const GenBatch* g, int sm_count, cudaStream_t st) {
-  const size_t smem = gen_smem_bytes(sh.mixed, sh.pmax_max, sh.gen_nodes_smem ? sh.n_nodes_smem : 0, sh.occ);
+  const size_t smem = gen_smem_bytes(sh.mixed, sh.pmax_max, sh.occ);
   auto launch = [&](auto fn) -> cudaError_t {
     cudaError_t e = set_smem(fn, smem);
     if (e != cudaSuccess) return e;

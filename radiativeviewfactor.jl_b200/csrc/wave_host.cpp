@@ -142,12 +142,10 @@ WaveShape wave_shape(Session* s, WaveReq* const* reqs, int n) {
   sh.occ = reqs[0]->occ;
   for (int r = 0; r < n; ++r) sh.pmax_max = std::max(sh.pmax_max, reqs[r]->pmax);
   if (n == 1 && sh.occ) {
-    const size_t cap = std::min<size_t>(s->smem_optin, 110 * 1024);
     sh.n_nodes_smem = reqs[0]->pa.n_nodes;
-    sh.gen_nodes_smem = gen_smem_bytes(sh.mixed, sh.pmax_max, sh.n_nodes_smem, true) <= cap;
     sh.trace64_nodes_smem = trace_smem_bytes(false, sh.n_nodes_smem) <= (size_t)72 * 1024;
     sh.trace32_nodes_smem = sh.mixed && trace_smem_bytes(true, sh.n_nodes_smem) <= (size_t)80 * 1024;
-    if (!sh.gen_nodes_smem && !sh.trace64_nodes_smem && !sh.trace32_nodes_smem) sh.n_nodes_smem = 0;
+    if (!sh.trace64_nodes_smem && !sh.trace32_nodes_smem) sh.n_nodes_smem = 0;
   }
   return sh;
 }
@@ -174,7 +172,7 @@ int ensure_blocks(Session* s) {
 }
 
 uint64_t shape_key(const WaveShape& sh) {
-  return (uint64_t)sh.mixed | ((uint64_t)sh.dim3 << 1) | ((uint64_t)sh.occ << 2) | ((uint64_t)sh.gen_nodes_smem << 3) |
+  return (uint64_t)sh.mixed | ((uint64_t)sh.dim3 << 1) | ((uint64_t)sh.occ << 2) |
          ((uint64_t)sh.trace64_nodes_smem << 4) | ((uint64_t)sh.trace32_nodes_smem << 5) |
          ((uint64_t)sh.pmax_max << 8) | ((uint64_t)sh.gen_bps << 16) | ((uint64_t)sh.trace_bps << 20) |
          ((uint64_t)sh.n_nodes_smem << 24);
@@ -250,9 +248,6 @@ int wave_chunk(Session* s, WaveReq* const* reqs_in, int n_in, bool use_graph, Ch
   g.n_req = n;
   g.pmax_max = sh.pmax_max;
   g.total_tiles = base[n];
-  g.nodes_in_smem = sh.gen_nodes_smem;
-  g.smem_nodes = sh.mixed ? (const void*)reqs[0]->nodes_f : (const void*)reqs[0]->nodes_d;
-  g.n_nodes_smem = sh.n_nodes_smem;
   g.q = q;
   g.counters = s->counters.as<unsigned long long>();
   g.err = s->err.as<int>();
