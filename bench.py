@@ -319,10 +319,13 @@ def roof_for(W: Workload, stats, prec, size, peak64, peak32):
 
 
 def phases(stats):
-    keys = ("ms_gen", "ms_trace", "ms_trace_fp64", "ms_resolve", "ms_duffy", "ms_pairs", "ms_prep", "ms_reduce")
+    keys = ("ms_gen", "ms_trace", "ms_lists", "ms_trace_fp64", "ms_resolve", "ms_duffy", "ms_pairs", "ms_prep",
+            "ms_reduce")
     d = {k: statistics.mean(s[k] for s in stats) for k in keys}
     d["n_chunks"] = int(stats[-1]["n_chunks"])
     d["n_rays_traced"] = int(stats[-1]["n_rays_traced"])
+    d["n_list_pairs"] = int(stats[-1]["n_list_pairs"])
+    d["n_walk_pairs"] = int(stats[-1]["n_walk_pairs"])
     return d
 
 

@@ -140,7 +140,10 @@ typedef struct {
   double ms_trace;        /*   traversal (FP32 in mixed mode) */
   double ms_trace_fp64;   /*   mixed mode: FP64 traversal of the uncertain and FP64 rays */
   double ms_resolve;      /*   visible terms of the traced rays */
-  int64_t reserved[8];
+  int64_t n_list_pairs;   /* 3-D occlusion: pending pairs whose rays test a per-pair triangle list */
+  int64_t n_walk_pairs;   /*   ... whose list overflowed (their rays walk the tree) */
+  double ms_lists;        /*   building the per-pair lists (part of ms_trace) */
+  int64_t reserved[5];
 } rvf_stats;
 
 const char* rvf_version(void);

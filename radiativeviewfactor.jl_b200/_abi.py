@@ -59,7 +59,8 @@ class Stats(C.Structure):
                 ("n_graze_fp64", C.c_int64), ("n_unsure_rays", C.c_int64), ("n_unsure_slab", C.c_int64),
                 ("n_unsure_prim", C.c_int64), ("n_unsure_dir", C.c_int64), ("n_rays_traced", C.c_int64),
                 ("n_chunks", C.c_int64), ("ms_gen", C.c_double), ("ms_trace", C.c_double),
-                ("ms_trace_fp64", C.c_double), ("ms_resolve", C.c_double), ("reserved", C.c_int64 * 8)]
+                ("ms_trace_fp64", C.c_double), ("ms_resolve", C.c_double), ("n_list_pairs", C.c_int64),
+                ("n_walk_pairs", C.c_int64), ("ms_lists", C.c_double), ("reserved", C.c_int64 * 5)]
 
     def as_dict(self):
         d = {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}

@@ -247,6 +247,37 @@ int mesh_upload(Session* s, const rvf_mesh_desc* d, rvf_mesh** out) {
     m->n_nodes = M;
     m->h_nodes = nodes;
     if ((rc = upload(s, m->nodes, nodes.data(), sizeof(NodeD) * M))) return rc;
+    std::vector<int32_t> leaf_of((size_t)d->n_obs, -1);
+    for (int k = 0; k < M; ++k)
+      for (int u = 0; u < nodes[k].b; ++u) {
+        const int64_t t = (int64_t)nodes[k].a + u;
+        if (t < 0 || t >= d->n_obs || leaf_of[t] >= 0) return set_err(RVF_EINVAL, "internal: BVH leaves do not partition the primitives");
+        leaf_of[t] = k;
+      }
+    for (int32_t v : leaf_of)
+      if (v < 0) return set_err(RVF_EINVAL, "internal: a primitive lies in no BVH leaf");
+    if ((rc = upload(s, m->leaf_of, leaf_of.data(), sizeof(int32_t) * leaf_of.size()))) return rc;
+    // Start nodes of the pair-list walk: the deepest level of the tree with
+    // at most 32 nodes (with the leaves above it), so that one round of 32
+    // lanes replaces the walk's first levels.
+    {
+      std::vector<int32_t> cur{0}, next;
+      for (;;) {
+        next.clear();
+        for (int32_t k : cur) {
+          if (nodes[k].b > 0) next.push_back(k);
+          else {
+            if (nodes[k + 1].miss >= M) return set_err(RVF_EINVAL, "internal: BVH node %d has no right child", k);
+            next.push_back(k + 1);
+            next.push_back(nodes[k + 1].miss);
+          }
+        }
+        if (next.size() > 32 || next == cur) break;
+        cur = next;
+      }
+      m->n_frontier = (int)cur.size();
+      if ((rc = upload(s, m->frontier, cur.data(), sizeof(int32_t) * cur.size()))) return rc;
+    }
     // FP32 copy for the certified FP32 traversal (rounding is inside its error allowance)
     std::vector<NodeF> nodesf(M);
     for (int k = 0; k < M; ++k) {
@@ -286,6 +317,39 @@ int mesh_upload(Session* s, const rvf_mesh_desc* d, rvf_mesh** out) {
       }
       if ((rc = upload(s, m->tris_ref, tref.data(), sizeof(TriD) * T))) return rc;
       if ((rc = upload(s, m->tris_geo, tgeo.data(), sizeof(TriD) * T))) return rc;
+      // Pair-list data per triangle: the corners v0, v0 + e1, v0 + e2 in FP32,
+      // the group, and the margin by which rounding can move a hit of the
+      // reference's Moller-Trumbore test, 2 (2^-53 / 1e-10) (65 S Lx^2 + 40 Lx^3)
+      // with Lx the longest edge and S = 2 sqrt(3) extent >= |o - v0|, t_max, Lx
+      // (rounded up).  sat_em: the separating-axis test's FP32 allowance.
+      const double S = 2.0 * std::sqrt(3.0) * m->extent;
+      m->sat_em = (float)std::ldexp(S, -16);
+      for (int pass = 0; pass < 2; ++pass) {
+        const std::vector<TriD>& src = pass == 0 ? tref : tgeo;
+        std::vector<float> sat((size_t)T * 12);
+        for (int64_t k = 0; k < T; ++k) {
+          const TriD& t = src[k];
+          double l2 = 0.0, q1 = 0.0, q2 = 0.0, q3 = 0.0;
+          for (int c = 0; c < 3; ++c) {
+            q1 += t.e1[c] * t.e1[c];
+            q2 += t.e2[c] * t.e2[c];
+            q3 += (t.e2[c] - t.e1[c]) * (t.e2[c] - t.e1[c]);
+          }
+          l2 = std::max(q1, std::max(q2, q3)) * (1.0 + 1e-9);
+          const double lx = std::min(std::sqrt(l2), S);
+          const double mt = 2.0 * 1.111e-6 * (65.0 * S * l2 + 40.0 * l2 * lx);
+          float* o = sat.data() + 12 * k;
+          for (int c = 0; c < 3; ++c) {
+            o[c] = (float)t.v0[c];
+            o[4 + c] = (float)(t.v0[c] + t.e1[c]);
+            o[8 + c] = (float)(t.v0[c] + t.e2[c]);
+          }
+          o[3] = std::nextafter((float)mt, INFINITY);
+          std::memcpy(&o[7], &t.group, 4);
+          o[11] = 0.f;
+        }
+        if ((rc = upload(s, pass == 0 ? m->sat_ref : m->sat_geo, sat.data(), sizeof(float) * sat.size()))) return rc;
+      }
       for (int pass = 0; pass < 2; ++pass) {
         const std::vector<TriD>& src = pass == 0 ? tref : tgeo;
         std::vector<TriF> tf(T);

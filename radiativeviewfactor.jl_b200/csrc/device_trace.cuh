@@ -280,6 +280,8 @@ struct PolD3 {
     Q.tmax = ws.r64.tmax[o];
     return mt_d(tr, Q) ? kHit : kMiss;
   }
+  // the lane's own ray against a triangle (pair lists: groups already excluded)
+  __device__ __forceinline__ int prim_direct(const TriD& tr) const { return mt_d(tr, R) ? kHit : kMiss; }
 };
 
 // FP64 2-D segments (src/BVH.jl:265-322): a = first end point, b = second,
@@ -357,6 +359,8 @@ struct PolF3 {
     if (r == kUnsure) ++cnt.unsure_prim;
     return r;
   }
+  // the lane's own ray against a triangle (pair lists: groups already excluded)
+  __device__ __forceinline__ int prim_direct(const TriF& tr) const { return mt_f(tr, R); }
 };
 
 }  // namespace rvf

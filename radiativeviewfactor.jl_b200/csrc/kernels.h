@@ -19,7 +19,8 @@ enum : int {
   kCtrSlots = 5,   // pending-pair slots in use
   kCtrHead64 = 6,  // traversal progress, FP64 queue
   kCtrHead32 = 7,  // traversal progress, FP32 queue
-  kCtrCount = 8
+  kCtrPool = 8,    // pair-list pool entries taken
+  kCtrCount = 9
 };
 
 // A pair with queued rays: its request (mesh) within the launch, internal
@@ -30,12 +31,28 @@ struct PendSlot {
   double acc;
 };
 
+// Per pending pair (3-D triangles): the triangles a shadow ray of the pair
+// can hit under the reference's FP64 tests (primitive indices in leaf order),
+// built by the list kernel after the generation into a pool: entries
+// pool[off, off + n).  n = -1: no list (too long, or the pool is full); the
+// pair's rays walk the tree.
+constexpr int kListCap = 256;    // longest list kept
+constexpr int kListFront = 64;   // breadth-first frontier of the list kernel's walk
+constexpr int kListLeaves = 64;  // candidate leaves per pair
+struct PairList {
+  int32_t n;
+  int32_t off;
+};
+
 struct WaveQ {
   uint64_t* rec64;  // FP64 ray queue
   uint64_t* rec32;  // FP32 ray queue (mixed precision)
   int64_t cap;      // records per queue
   PendSlot* slots;
   unsigned long long* vis;  // slots x vis_words visibility bits, bit p*pmax+q
+  PairList* plist;          // per-slot lists, or null (every ray walks the tree)
+  int32_t* pool;            // list entries
+  int64_t pool_cap;
   int64_t scap;
   int vis_words;
   unsigned long long* ctr;  // kCtrCount counters
@@ -170,6 +187,16 @@ struct TraceArgs {
   const TriF* trisf;
   const SegD* segs;
   float delta;
+  // pair lists (3-D): leaf node of each primitive (leaf order), its corners
+  // in FP32 with its margin (sat), the generation's capsule radius and
+  // margin, and the FP32 rounding allowance of the separating-axis test
+  const int32_t* leaf_of;
+  const float4* sat;
+  const int32_t* frontier;  // start nodes of the list walk (<= 32)
+  int n_frontier;
+  const double* rad;
+  double cull_margin;
+  float sat_em;
   WaveQ q;
   unsigned long long* counters;
   uint8_t* ray_log;
@@ -244,6 +271,8 @@ size_t trace_smem_bytes(bool fp32, int n_nodes_smem);
 cudaError_t launch_gen(const WaveShape& sh, const GenBatch* g, int sm_count, cudaStream_t st);
 cudaError_t launch_trace(const WaveShape& sh, const TraceBatch* t, bool fp32, int sm_count, cudaStream_t st);
 cudaError_t launch_resolve(const WaveShape& sh, const ResolveBatch* r, int sm_count, cudaStream_t st);
+// Pair lists of the chunk's pending pairs (3-D triangles with occlusion).
+cudaError_t launch_plist(const TraceBatch* t, int sm_count, cudaStream_t st);
 
 // A Quad8 pair sharing corner nodes (src/DuffyKernel.jl:95-115), i < j in the
 // caller's order (the reference integrates with elem_i = the lower index).

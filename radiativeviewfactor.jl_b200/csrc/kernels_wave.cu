@@ -658,6 +658,257 @@ __device__ __forceinline__ void log_ray(const TraceArgs& a, int64_t i, int64_t j
   lp[sw ? q * a.log_pm + p : p * a.log_pm + q] = v;
 }
 
+// ---------------------------------------------------------------------------
+// 1b. Pair lists (3-D triangles with occlusion).
+//
+// Once per pending pair, the triangles that any shadow ray of the pair can
+// hit under the reference's FP64 tests (src/GPUBVH.jl:202-285):
+//  * leaves: a walk of the tree with the pair's capsule -- the centroid
+//    segment grown by R = max(rad_i, rad_j) plus the cull margin, which holds
+//    every ray segment of the pair -- skipping each subtree whose box no ray
+//    of the pair can hit (pair_misses_box, as for the root in the generation);
+//  * triangles of the leaves left: dropped when their group is the pair's
+//    own, or when a separating axis (the triangle's normal, or the centroid
+//    segment's direction crossed with an edge) puts the triangle farther than
+//    R + M_T from the centroid segment.  M_T bounds how far rounding can move
+//    a hit of the reference's Moller-Trumbore test: with eps = 2^-53, a hit
+//    needs |a| >= 1e-10, and then its u and v differ from the exact
+//    line-plane values by at most (eps / 1e-10)(8.3 S Lx + 6.6 Lx^2) and its
+//    t by (eps / 1e-10) 14.7 S Lx^2, S bounding |o - v0| and t_max and Lx the
+//    edge lengths; a hit therefore puts a point of the ray segment within
+//    E_t + 3 (E_u + E_v) Lx of the triangle.  The list kernel uses twice that.
+// A ray of the pair tests the listed triangles only, each behind the slab
+// test of its own leaf box: with a finite 1/d the reference's slab test is
+// monotone under box inclusion (rounding is monotone and the box bounds only
+// widen the parameter intervals), every ancestor box contains the leaf box
+// (boxes are min/max unions over the triangles), so the leaf's test passing
+// means the reference's walk reaches the leaf.  A pair with more than
+// kListMax triangles keeps n = -1 and its rays walk the tree.
+// ---------------------------------------------------------------------------
+// Separation of the centroid segment (a, b) and the triangle (p0, p1, p2)
+// along w, in FP32: true when the gap exceeds rm |w|.  Squares avoid the
+// square root (rm > 0).
+__device__ __forceinline__ bool axis_separates(const float* a, const float* b, const float4& p0, const float4& p1,
+                                               const float4& p2, float wx, float wy, float wz, float rm) {
+  const float sa = fmaf(a[0], wx, fmaf(a[1], wy, a[2] * wz)), sb = fmaf(b[0], wx, fmaf(b[1], wy, b[2] * wz));
+  const float q0 = fmaf(p0.x, wx, fmaf(p0.y, wy, p0.z * wz));
+  const float q1 = fmaf(p1.x, wx, fmaf(p1.y, wy, p1.z * wz));
+  const float q2 = fmaf(p2.x, wx, fmaf(p2.y, wy, p2.z * wz));
+  const float gap = fmaxf(fminf(q0, fminf(q1, q2)) - fmaxf(sa, sb), fminf(sa, sb) - fmaxf(q0, fmaxf(q1, q2)));
+  return gap > 0.0f && gap * gap > rm * rm * fmaf(wx, wx, fmaf(wy, wy, wz * wz));
+}
+
+// True when no ray of the pair (segments within R of the centroid segment
+// a -> b, direction d) can be a hit of the reference's test of the triangle
+// with corners p0, p1, p2 (FP32) and rounding margin p0.w.  em absorbs the
+// FP32 rounding of the corners and of this test (a few 2^-24 of the
+// coordinates' magnitude, against em = S 2^-16).
+__device__ __forceinline__ bool pair_misses_tri(const float* a, const float* b, const float* d, float R, float em,
+                                                const float4& p0, const float4& p1, const float4& p2) {
+  const float rm = R + p0.w + em;
+  const float f1[3] = {p1.x - p0.x, p1.y - p0.y, p1.z - p0.z};
+  const float f2[3] = {p2.x - p0.x, p2.y - p0.y, p2.z - p0.z};
+  const float f3[3] = {p2.x - p1.x, p2.y - p1.y, p2.z - p1.z};
+  // the segment direction crossed with each edge, then the triangle's normal
+  if (axis_separates(a, b, p0, p1, p2, d[1] * f1[2] - d[2] * f1[1], d[2] * f1[0] - d[0] * f1[2],
+                     d[0] * f1[1] - d[1] * f1[0], rm))
+    return true;
+  if (axis_separates(a, b, p0, p1, p2, d[1] * f2[2] - d[2] * f2[1], d[2] * f2[0] - d[0] * f2[2],
+                     d[0] * f2[1] - d[1] * f2[0], rm))
+    return true;
+  if (axis_separates(a, b, p0, p1, p2, d[1] * f3[2] - d[2] * f3[1], d[2] * f3[0] - d[0] * f3[2],
+                     d[0] * f3[1] - d[1] * f3[0], rm))
+    return true;
+  return axis_separates(a, b, p0, p1, p2, f1[1] * f2[2] - f1[2] * f2[1], f1[2] * f2[0] - f1[0] * f2[2],
+                        f1[0] * f2[1] - f1[1] * f2[0], rm);
+}
+
+// The pair's capsule for the list walk, in FP32: the centroid segment's
+// start A and direction reciprocals (from FP64, rounded once), and the radius
+// grown by em.  A box test in FP32 (capsule_misses_box) then only reports a
+// miss when the FP64 test with the ungrown radius would: every rounding of
+// the test (the nodes' and A's FP32 copies, the subtraction, 1/d) moves a
+// slab parameter by a few 2^-24 S |1/d|, the growth by em = 2^-16 S moves it
+// by em |1/d|.  Components of d that are exactly zero use the containment
+// test, as pair_misses_box does.
+struct CapsuleF {
+  float A[3], inv[3];
+  bool zero[3];
+  float R;
+};
+
+__device__ __forceinline__ bool capsule_misses_box(const CapsuleF& c, const NodeF& nd) {
+  float te = 0.0f, tx = 1.0f;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const float lo = nd.lo[k] - c.R, hi = nd.hi[k] + c.R;
+    if (c.zero[k]) {
+      if (c.A[k] < lo || c.A[k] > hi) return true;
+      continue;
+    }
+    const float t1 = (lo - c.A[k]) * c.inv[k], t2 = (hi - c.A[k]) * c.inv[k];
+    te = fmaxf(te, fminf(t1, t2));
+    tx = fminf(tx, fmaxf(t1, t2));
+  }
+  return te > tx;
+}
+
+// The list of one pending pair, built by its warp: a breadth-first walk of
+// the tree with the capsule test from the precomputed start nodes (one node
+// per lane; every start node's box lies inside its ancestors', so skipping
+// the ancestors' tests only tests more), then the triangles of the candidate
+// leaves, four leaves of up to eight triangles per round of 32 lanes.
+// Returns the list length (entries in `list`, in a deterministic order), or
+// -1 when a frontier, the candidate leaves or the list exceed their
+// capacity.  Warp-uniform.
+__device__ int build_pair_list(const TraceArgs& a, const PendSlot& ps, int* front, int* leaves, int* list) {
+  const int lane = threadIdx.x & 31;
+  const int64_t i = ps.i, j = ps.j;
+  CapsuleF cap;
+  float bf[3];
+  const double R = fmax(a.rad[i], a.rad[j]) + a.cull_margin;
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    const double A = a.cen[3 * i + c], B = a.cen[3 * j + c];
+    const double dd = B - A;
+    cap.A[c] = (float)A;
+    bf[c] = (float)B;
+    cap.zero[c] = dd == 0.0;
+    cap.inv[c] = cap.zero[c] ? 0.0f : (float)(1.0 / dd);
+  }
+  cap.R = (float)R + a.sat_em;
+  int* cur = front;
+  int* nxt = front + kListFront;
+  if (lane < a.n_frontier) cur[lane] = a.frontier[lane];
+  __syncwarp();
+  int ncur = a.n_frontier, nleaf = 0;
+  while (ncur > 0) {  // each round descends one level: bounded by the tree depth
+    int nnext = 0;
+    for (int b = 0; b < ncur; b += 32) {
+      const int t = b + lane;
+      bool pass = false, leaf = false;
+      int k = 0, right = 0;
+      if (t < ncur && cur[t] < a.n_nodes) {
+        k = cur[t];
+        const NodeF nd = a.nodesf[k];
+        pass = !capsule_misses_box(cap, nd);
+        leaf = (nd.ab & 15) > 0;
+        if (pass && !leaf) right = a.nodesf[k + 1].miss;  // the right child follows the left subtree
+      }
+      const uint32_t ml = __ballot_sync(kFull, pass && leaf), mi = __ballot_sync(kFull, pass && !leaf);
+      const int pl = nleaf + __popc(ml & lanemask_lt());
+      if (pass && leaf && pl < kListLeaves) leaves[pl] = k;
+      nleaf += __popc(ml);
+      const int pi = nnext + 2 * __popc(mi & lanemask_lt());
+      if (pass && !leaf && pi + 1 < kListFront) {
+        nxt[pi] = k + 1;
+        nxt[pi + 1] = right;
+      }
+      nnext += 2 * __popc(mi);
+    }
+    __syncwarp();
+    if (nleaf > kListLeaves || nnext > kListFront) return -1;
+    int* tmp = cur;
+    cur = nxt;
+    nxt = tmp;
+    ncur = nnext;
+  }
+  // triangles of the candidate leaves
+  const float df[3] = {bf[0] - cap.A[0], bf[1] - cap.A[1], bf[2] - cap.A[2]};
+  const float Rf = (float)R;
+  const int32_t gi = a.group[i], gj = a.group[j];
+  int n = 0;
+  for (int b = 0; b < nleaf; b += 4) {
+    const int li = b + (lane >> 3), u8 = lane & 7;
+    bool keep = false;
+    int u = 0;
+    if (li < nleaf) {
+      const int32_t ab = a.nodesf[leaves[li]].ab;
+      if (u8 < (ab & 15)) {
+        u = (ab >> 4) + u8;
+        const float4 p0 = a.sat[3 * u], p1 = a.sat[3 * u + 1], p2 = a.sat[3 * u + 2];
+        const int32_t g = __float_as_int(p1.w);
+        keep = g != gi && g != gj && !pair_misses_tri(cap.A, bf, df, Rf, a.sat_em, p0, p1, p2);
+      }
+    }
+    const uint32_t m = __ballot_sync(kFull, keep);
+    const int pos = n + __popc(m & lanemask_lt());
+    if (keep && pos < kListCap) list[pos] = u;
+    n += __popc(m);
+    if (n > kListCap) return -1;
+  }
+  __syncwarp();
+  return n;
+}
+
+// One warp per pending pair of the chunk.
+__global__ void __launch_bounds__(256) k_plist(const TraceBatch* __restrict__ Lp) {
+  __shared__ int s_front[8][2 * kListFront];
+  __shared__ int s_leaf[8][kListLeaves];
+  __shared__ int s_list[8][kListCap];
+  const TraceBatch& L = *Lp;
+  const WaveQ& Q = L.q;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const unsigned long long ns = *(volatile unsigned long long*)(Q.ctr + kCtrSlots);
+  const unsigned long long stride = (unsigned long long)gridDim.x * 8;
+  uint32_t n_list = 0, n_walk = 0;
+  for (unsigned long long s = (unsigned long long)blockIdx.x * 8 + warp; s < ns; s += stride) {
+    const PendSlot ps = Q.slots[s];
+    const TraceArgs& a = L.reqs[ps.req];
+    int n = -1;
+    if (a.dim3 && a.leaf_of && a.rad && a.sat && a.nodesf && a.frontier)
+      n = build_pair_list(a, ps, s_front[warp], s_leaf[warp], s_list[warp]);
+    long long off = 0;
+    if (n > 0) {
+      if (lane == 0) off = (long long)atomicAdd(Q.ctr + kCtrPool, (unsigned long long)n);
+      off = __shfl_sync(kFull, off, 0);
+      if (off + n > Q.pool_cap) n = -1;  // pool full: this pair walks
+      else
+        for (int e = lane; e < n; e += 32) Q.pool[off + e] = s_list[warp][e];
+    }
+    if (lane == 0) {
+      PairList pl;
+      pl.n = n;
+      pl.off = (int32_t)off;
+      Q.plist[s] = pl;
+      n_list += n >= 0 ? 1 : 0;
+      n_walk += n < 0 ? 1 : 0;
+    }
+    __syncwarp();
+  }
+  if (lane == 0 && L.counters) {
+    atomicAdd(L.counters + 11, (unsigned long long)n_list);
+    atomicAdd(L.counters + 12, (unsigned long long)n_walk);
+  }
+}
+
+// A ray against its pair's list (entries e[0..n) of the pool): kHit
+// (blocked), kMiss or, for FP32 rays, kUnsure (some certified decision was
+// not certain and no certain hit was found).
+template <typename Src, typename Pol, typename Tri>
+__device__ __forceinline__ int trace_list(const int32_t* e, int n, const Src& nodes, const Tri* tris,
+                                          const int32_t* leaf_of, const Pol& pol, TravCount& cnt) {
+  int last = -1, s = kMiss;
+  bool unsure = false;
+  for (int k = 0; k < n; ++k) {
+    const int u = e[k];
+    const int lf = leaf_of[u];
+    if (lf != last) {
+      last = lf;
+      s = pol.node(nodes(lf));
+      ++cnt.nodes;
+      if (s == kUnsure) ++cnt.unsure_slab;
+    }
+    if (s == kMiss) continue;
+    ++cnt.prims;
+    const int m = pol.prim_direct(tris[u]);
+    if (m == kUnsure) ++cnt.unsure_prim;
+    if (m == kHit && s == kHit) return kHit;
+    if (m != kMiss) unsure = true;
+  }
+  return unsure ? kUnsure : kMiss;
+}
+
 // Sets the (p, q) visibility bits of the warp's visible rays.  The rays of one
 // pair sit in consecutive lanes, so the bits of each run of lanes with the
 // same (slot, word) are OR-combined by a segmented scan and the last lane of
@@ -740,8 +991,27 @@ __global__ void __launch_bounds__(256, 3) k_trace64(const TraceBatch* __restrict
         else make_ray(xi, rx, ry, rz, r2, pol.R);
         pol.store(ws, lane, gi, gj);
       }
-      res = in_smem ? trace_batch(have, SwizNodes<NodeD>{reinterpret_cast<const int4*>(snodes)}, n_nodes, ws, pol, tc)
-                            : trace_batch(have, GlobalNodes<NodeD>{a.nodes}, n_nodes, ws, pol, tc);
+      // the pair's list when it has one and the ray's 1/d is finite
+      int ln = -1;
+      const int32_t* le = nullptr;
+      if (have && Q.plist) {
+        const PairList pl = Q.plist[x.slot];
+        ln = pl.n;
+        le = Q.pool + pl.off;
+        if (pol.R.zdir || !(isfinite(pol.R.inv[0]) && isfinite(pol.R.inv[1]) && isfinite(pol.R.inv[2]))) ln = -1;
+      }
+      const bool walk = have && ln < 0;
+      res = kMiss;
+      if (have && ln >= 0)
+        res = in_smem ? trace_list(le, ln, SwizNodes<NodeD>{reinterpret_cast<const int4*>(snodes)}, a.tris, a.leaf_of,
+                                   pol, tc)
+                      : trace_list(le, ln, GlobalNodes<NodeD>{a.nodes}, a.tris, a.leaf_of, pol, tc);
+      if (__any_sync(kFull, walk)) {
+        const int rw =
+            in_smem ? trace_batch(walk, SwizNodes<NodeD>{reinterpret_cast<const int4*>(snodes)}, n_nodes, ws, pol, tc)
+                    : trace_batch(walk, GlobalNodes<NodeD>{a.nodes}, n_nodes, ws, pol, tc);
+        if (walk) res = rw;
+      }
     } else {
       PolD2 pol;
       pol.segs = a.segs;
@@ -810,9 +1080,26 @@ __global__ void __launch_bounds__(256, 4) k_trace32(const TraceBatch* __restrict
       pol.store(ws, lane, a.group[i], a.group[j]);
     }
     const int n_nodes = have ? a.n_nodes : 0;
-    const int res = in_smem
-                        ? trace_batch(have, SwizNodes<NodeF>{reinterpret_cast<const int4*>(snodes)}, n_nodes, ws, pol, tc)
-                        : trace_batch(have, GlobalNodes<NodeF>{a.nodesf}, n_nodes, ws, pol, tc);
+    // the pair's list when it has one (FP32 rays always have a finite 1/d)
+    int ln = -1;
+    const int32_t* le = nullptr;
+    if (have && Q.plist) {
+      const PairList pl = Q.plist[x.slot];
+      ln = pl.n;
+      le = Q.pool + pl.off;
+    }
+    const bool walk = have && ln < 0;
+    int res = kMiss;
+    if (have && ln >= 0)
+      res = in_smem ? trace_list(le, ln, SwizNodes<NodeF>{reinterpret_cast<const int4*>(snodes)}, a.trisf, a.leaf_of,
+                                 pol, tc)
+                    : trace_list(le, ln, GlobalNodes<NodeF>{a.nodesf}, a.trisf, a.leaf_of, pol, tc);
+    if (__any_sync(kFull, walk)) {
+      const int rw =
+          in_smem ? trace_batch(walk, SwizNodes<NodeF>{reinterpret_cast<const int4*>(snodes)}, n_nodes, ws, pol, tc)
+                  : trace_batch(walk, GlobalNodes<NodeF>{a.nodesf}, n_nodes, ws, pol, tc);
+      if (walk) res = rw;
+    }
     set_visible_warp(Q, have && res == kMiss, x.slot, pm, x.p, x.q);
     if (have && a.ray_log && res != kUnsure) log_ray(a, x.i, x.j, x.sw, x.p, x.q, res == kHit ? 2 : 1);
     // uncertain rays go to the FP64 queue
@@ -1000,6 +1287,11 @@ cudaError_t launch_trace(const WaveShape& sh, const TraceBatch* t, bool fp32, in
   };
   if (fp32) return launch(k_trace32);
   return sh.dim3 ? launch(k_trace64<true>) : launch(k_trace64<false>);
+}
+
+cudaError_t launch_plist(const TraceBatch* t, int sm_count, cudaStream_t st) {
+  k_plist<<<(unsigned)(sm_count * 8), 256, 0, st>>>(t);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_resolve(const WaveShape& sh, const ResolveBatch* r, int sm_count, cudaStream_t st) {

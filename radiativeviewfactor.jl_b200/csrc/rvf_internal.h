@@ -64,7 +64,7 @@ struct rvf_session {
   rvf::DevBuf counters;      // u64 x 8
   // wavefront pair pipeline (kernels_wave.cu, wave_host.cpp): queues,
   // device launch blocks, pinned counter readback, graphs per launch shape
-  rvf::DevBuf wq_ctr, wq_rec64, wq_rec32, wq_slots, wq_vis;
+  rvf::DevBuf wq_ctr, wq_rec64, wq_rec32, wq_slots, wq_vis, wq_plist, wq_pool;
   rvf::DevBuf wl_pair, wl_mixed, wl_trace, wl_resolve, wl_tilebase, wl_gen, wl_tb, wl_rb;
   unsigned long long* h_ctr = nullptr;
   std::map<uint64_t, cudaGraphExec_t> graphs;
@@ -95,6 +95,11 @@ struct rvf_mesh {
   rvf::DevBuf mc_area;                                          // Monte Carlo areas (caller's order)
   rvf::DevBuf nodes, tris_ref, tris_geo, segs;
   rvf::DevBuf nodesf, trisf_ref, trisf_geo;  // FP32 copies (mixed precision)
+  rvf::DevBuf leaf_of;                        // int32 leaf node of each primitive (leaf order)
+  rvf::DevBuf sat_ref, sat_geo;               // pair-list data per triangle (3 float4, leaf order)
+  rvf::DevBuf frontier;                       // int32 start nodes of the pair-list walk
+  int n_frontier = 0;
+  float sat_em = 0.f;
   double extent = 1.0;                        // 1 + max |coordinate| of the mesh and the soup
   int n_nodes = 0;
   int64_t n_obs = 0;

@@ -276,7 +276,7 @@ int rvf_session_destroy(rvf_session* s) {
     s->err.free_();
     s->tile_counter.free_();
     s->counters.free_();
-    s->wq_ctr.free_(); s->wq_rec64.free_(); s->wq_rec32.free_(); s->wq_slots.free_(); s->wq_vis.free_();
+    s->wq_ctr.free_(); s->wq_rec64.free_(); s->wq_rec32.free_(); s->wq_slots.free_(); s->wq_vis.free_(); s->wq_plist.free_(); s->wq_pool.free_();
     for (rvf::DevBuf* b : {&s->wl_pair, &s->wl_mixed, &s->wl_trace, &s->wl_resolve, &s->wl_tilebase, &s->wl_gen,
                            &s->wl_tb, &s->wl_rb})
       b->free_();
@@ -408,6 +408,7 @@ int rvf_solve(rvf_session* s, rvf_mesh* m, const rvf_options* o, double* F_elem,
       S.ms_trace += ci.ms_trace;
       S.ms_trace_fp64 += ci.ms_trace_fp64;
       S.ms_resolve += ci.ms_resolve;
+      S.ms_lists += ci.ms_lists;
       S.n_rays_traced += ci.rays_traced;
       if (w.claimed == before) return set_err(RVF_ENOMEM, "pair pipeline made no progress: ray queue too small for one tile");
     }
@@ -486,6 +487,8 @@ int rvf_solve(rvf_session* s, rvf_mesh* m, const rvf_options* o, double* F_elem,
     S.n_unsure_slab = mixed ? (int64_t)c[8] : 0;
     S.n_unsure_prim = mixed ? (int64_t)c[9] : 0;
     S.n_unsure_dir = mixed ? (int64_t)c[10] : 0;
+    S.n_list_pairs = (int64_t)c[11];
+    S.n_walk_pairs = (int64_t)c[12];
     if (N > 0 && m->G > 0) {
       std::vector<double> rs(N);
       cudaMemcpy(rs.data(), m->rowsum.ptr, sizeof(double) * N, cudaMemcpyDeviceToHost);

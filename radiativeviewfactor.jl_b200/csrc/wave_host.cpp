@@ -16,7 +16,7 @@ namespace rvf {
 // Capacity: every point pair of every tile when that is small, otherwise up
 // to 2^29 records per queue (4 GiB) within the HBM budget, and never below a
 // few tiles' worst case.
-int ensure_wave(Session* s, bool two_queues, bool occ, int pmax, int64_t n_tiles, WaveQ& q) {
+int ensure_wave(Session* s, bool two_queues, bool occ, bool lists, int pmax, int64_t n_tiles, WaveQ& q) {
   int rc = 0;
   if (!s->wq_ctr.ptr && (rc = s->wq_ctr.alloc(s, sizeof(unsigned long long) * kCtrCount))) return rc;
   q = WaveQ{};
@@ -29,12 +29,17 @@ int ensure_wave(Session* s, bool two_queues, bool occ, int pmax, int64_t n_tiles
   const int64_t want_s = std::min<int64_t>(n_tiles * kTile * kTile, (int64_t)1 << 25);
   const int64_t floor_s = std::min<int64_t>(n_tiles * kTile * kTile, 4 * kTile * kTile);
   const int nq = two_queues ? 2 : 1;
-  const size_t slot_bytes = sizeof(PendSlot) + sizeof(unsigned long long) * q.vis_words;
+  // pair lists: 8 B per slot and a pool of kPoolPerSlot entries per slot
+  constexpr int64_t kPoolPerSlot = 24;
+  const size_t slot_bytes = sizeof(PendSlot) + sizeof(unsigned long long) * q.vis_words +
+                            (lists ? sizeof(PairList) + sizeof(int32_t) * kPoolPerSlot : 0);
   auto have = [&](int64_t recs, int64_t slots) {
     return s->wq_rec64.bytes >= sizeof(uint64_t) * recs &&
            (!two_queues || s->wq_rec32.bytes >= sizeof(uint64_t) * recs) &&
            s->wq_slots.bytes >= sizeof(PendSlot) * slots &&
-           s->wq_vis.bytes >= sizeof(unsigned long long) * q.vis_words * slots;
+           s->wq_vis.bytes >= sizeof(unsigned long long) * q.vis_words * slots &&
+           (!lists || (s->wq_plist.bytes >= sizeof(PairList) * slots &&
+                       s->wq_pool.bytes >= sizeof(int32_t) * kPoolPerSlot * slots));
   };
   int64_t recs = want, slots = want_s;
   if (!have(recs, slots)) {
@@ -43,6 +48,8 @@ int ensure_wave(Session* s, bool two_queues, bool occ, int pmax, int64_t n_tiles
     s->wq_rec32.free_();
     s->wq_slots.free_();
     s->wq_vis.free_();
+    s->wq_plist.free_();
+    s->wq_pool.free_();
     const size_t left = s->budget > s->used ? s->budget - s->used : 0;
     while ((size_t)(recs * 8 * nq) + (size_t)slots * slot_bytes > left / 2 && (recs > floor_recs || slots > floor_s)) {
       recs = std::max<int64_t>(floor_recs, recs / 2);
@@ -52,6 +59,8 @@ int ensure_wave(Session* s, bool two_queues, bool occ, int pmax, int64_t n_tiles
     if (two_queues && (rc = s->wq_rec32.alloc(s, sizeof(uint64_t) * recs))) return rc;
     if ((rc = s->wq_slots.alloc(s, sizeof(PendSlot) * slots))) return rc;
     if ((rc = s->wq_vis.alloc(s, sizeof(unsigned long long) * q.vis_words * slots))) return rc;
+    if (lists && (rc = s->wq_plist.alloc(s, sizeof(PairList) * slots))) return rc;
+    if (lists && (rc = s->wq_pool.alloc(s, sizeof(int32_t) * kPoolPerSlot * slots))) return rc;
   }
   q.rec64 = s->wq_rec64.as<uint64_t>();
   q.rec32 = two_queues ? s->wq_rec32.as<uint64_t>() : nullptr;
@@ -61,6 +70,10 @@ int ensure_wave(Session* s, bool two_queues, bool occ, int pmax, int64_t n_tiles
   q.vis = s->wq_vis.as<unsigned long long>();
   q.scap = std::min<int64_t>((int64_t)(s->wq_slots.bytes / sizeof(PendSlot)),
                              (int64_t)(s->wq_vis.bytes / (sizeof(unsigned long long) * q.vis_words)));
+  q.plist = lists ? s->wq_plist.as<PairList>() : nullptr;
+  q.pool = lists ? s->wq_pool.as<int32_t>() : nullptr;
+  q.pool_cap = lists ? (int64_t)(s->wq_pool.bytes / sizeof(int32_t)) : 0;
+  if (lists) q.scap = std::min<int64_t>(q.scap, (int64_t)(s->wq_plist.bytes / sizeof(PairList)));
   return 0;
 }
 
@@ -122,8 +135,15 @@ int wave_prepare(Session* s, rvf_mesh* m, Tables* T, const rvf_options* o, uint8
   }
   TraceArgs& ta = w.ta;
   ta.N = N; ta.pmax = a.pmax; ta.dim3 = a.dim3; ta.tab = a.tab; ta.tabf = w.ma.tabf; ta.cen = a.cen;
-  ta.group = a.group; ta.orig = a.orig; ta.nodes = a.nodes; ta.nodesf = w.ma.nodesf; ta.n_nodes = a.n_nodes;
+  ta.group = a.group; ta.orig = a.orig; ta.nodes = a.nodes; ta.nodesf = occ ? m->nodesf.as<NodeF>() : nullptr; ta.n_nodes = a.n_nodes;
   ta.tris = a.tris; ta.trisf = w.ma.trisf; ta.segs = a.segs; ta.delta = w.ma.delta;
+  ta.leaf_of = (occ && w.dim3) ? m->leaf_of.as<int32_t>() : nullptr;
+  ta.sat = (occ && w.dim3) ? (o->geometric_soup ? m->sat_geo.as<float4>() : m->sat_ref.as<float4>()) : nullptr;
+  ta.sat_em = m->sat_em;
+  ta.frontier = (occ && w.dim3) ? m->frontier.as<int32_t>() : nullptr;
+  ta.n_frontier = (occ && w.dim3) ? m->n_frontier : 0;
+  ta.rad = a.rad;
+  ta.cull_margin = a.cull_margin;
   ta.ray_log = a.ray_log; ta.log_pm = a.log_pm;
   ResolveArgs& ra = w.ra;
   ra.N = N; ra.pmax = a.pmax; ra.dim3 = a.dim3; ra.tab = a.tab; ra.tabf = w.ma.tabf; ra.cen = a.cen;
@@ -189,8 +209,18 @@ cudaError_t enqueue_chunk(Session* s, const WaveShape& sh, bool events) {
   if ((e = launch_gen(sh, s->wl_gen.as<GenBatch>(), s->sm_count, st)) != cudaSuccess) return e;
   if (events) cudaEventRecord(s->ev[1], st);
   if (sh.occ) {
+    // the pair lists count as traversal time (the first traversal phase)
+    const bool lists = sh.dim3;
+    auto plist = [&]() -> cudaError_t {
+      if (events) cudaEventRecord(s->ev[5], st);
+      const cudaError_t el = launch_plist(s->wl_tb.as<TraceBatch>(), s->sm_count, st);
+      if (events) cudaEventRecord(s->ev[6], st);
+      return el;
+    };
+    if (lists && sh.mixed && (e = plist()) != cudaSuccess) return e;
     if (sh.mixed && (e = launch_trace(sh, s->wl_tb.as<TraceBatch>(), true, s->sm_count, st)) != cudaSuccess) return e;
     if (events) cudaEventRecord(s->ev[2], st);
+    if (lists && !sh.mixed && (e = plist()) != cudaSuccess) return e;
     if ((e = launch_trace(sh, s->wl_tb.as<TraceBatch>(), false, s->sm_count, st)) != cudaSuccess) return e;
     if (events) cudaEventRecord(s->ev[3], st);
     if ((e = launch_resolve(sh, s->wl_rb.as<ResolveBatch>(), s->sm_count, st)) != cudaSuccess) return e;
@@ -228,7 +258,7 @@ int wave_chunk(Session* s, WaveReq* const* reqs_in, int n_in, bool use_graph, Ch
   std::vector<int64_t> base(n + 1, 0);
   for (int r = 0; r < n; ++r) base[r + 1] = base[r] + offer[r];
   WaveQ q{};
-  if ((rc = ensure_wave(s, sh.mixed && sh.occ, sh.occ, sh.pmax_max, base[n], q))) return rc;
+  if ((rc = ensure_wave(s, sh.mixed && sh.occ, sh.occ, sh.occ && sh.dim3, sh.pmax_max, base[n], q))) return rc;
   std::vector<PairArgs> pa(n);
   std::vector<MixedArgs> ma(n);
   std::vector<TraceArgs> ta(n);
@@ -305,7 +335,7 @@ int wave_chunk(Session* s, WaveReq* const* reqs_in, int n_in, bool use_graph, Ch
   if (info) {
     *info = ChunkInfo{};
     info->graph = replayed;
-    info->kernels = 1 + (sh.occ ? (sh.mixed ? 3 : 2) : 0);
+    info->kernels = 1 + (sh.occ ? (sh.mixed ? 3 : 2) + (sh.dim3 ? 1 : 0) : 0);
     if (!replayed) {
       float t = 0.f;
       cudaEventElapsedTime(&t, s->ev[0], s->ev[1]);
@@ -318,6 +348,11 @@ int wave_chunk(Session* s, WaveReq* const* reqs_in, int n_in, bool use_graph, Ch
         info->ms_trace = sh.mixed ? t12 : t23;
         info->ms_trace_fp64 = sh.mixed ? t23 : 0.0;
         info->ms_resolve = t34;
+        if (sh.dim3) {
+          float tl = 0.f;
+          cudaEventElapsedTime(&tl, s->ev[5], s->ev[6]);
+          info->ms_lists = tl;
+        }
       }
     }
     info->rays_traced = (int64_t)(sh.mixed ? s->h_ctr[kCtrRec32] : s->h_ctr[kCtrRec64]);

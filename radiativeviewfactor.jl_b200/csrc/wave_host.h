@@ -23,12 +23,13 @@ struct WaveReq {
 
 struct ChunkInfo {
   double ms_gen = 0, ms_trace = 0, ms_trace_fp64 = 0, ms_resolve = 0;  // CUDA events (eager launches only)
+  double ms_lists = 0;                                                  // pair lists (inside ms_trace)
   int64_t rays_traced = 0;
   int kernels = 0;
   bool graph = false;  // replayed from a captured graph
 };
 
-int ensure_wave(Session* s, bool two_queues, bool occ, int pmax, int64_t n_tiles, WaveQ& q);
+int ensure_wave(Session* s, bool two_queues, bool occ, bool lists, int pmax, int64_t n_tiles, WaveQ& q);
 // Fills w from a mesh, its tables and the options (builds the FP32 table on
 // the first mixed-precision use).
 int wave_prepare(Session* s, rvf_mesh* m, Tables* T, const rvf_options* o, uint8_t* ray_log, WaveReq& w,

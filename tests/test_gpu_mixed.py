@@ -52,6 +52,20 @@ def test_cube_mixed_rays_identical(rvf, orc, session, near, geometric):
         assert st["n_pairs_fp64"] > 0
 
 
+def test_pair_lists_fine_cube_mixed(rvf, orc, session):
+    """Per-pair triangle lists under FP32 rays (certified decisions, FP64
+    re-tests): every sampled row within 1e-6 of the FP64 oracle."""
+    md = rvf.meshes.cube_enclosure(20, jitter=0.3, seed=2, box=True, box_edge=0.3, box_m=12)
+    N = md.n_elems
+    F, A, rs, _, st = mixed_solve(rvf, session, md, 3, [7])
+    assert st["n_list_pairs"] > 2 * st["n_walk_pairs"] > 0, st
+    m = orc.Mesh(md, [7])
+    raw, area, _, _ = orc.solve_plain(m, 3, row_stride=23)
+    assert np.array_equal(A, area)
+    for i in range(0, N, 23):
+        assert np.max(np.abs(F[i, i + 1:] - raw[i, i + 1:] / area[i])) <= ATOL_MIXED
+
+
 @pytest.mark.parametrize("family,nquad", [("quad", 3), ("quad4", 4), ("tri", 4)])
 def test_families_mixed(rvf, orc, session, family, nquad):
     md = rvf.meshes.cube_enclosure(4, family=family, box_m=2, box_edge=0.5)

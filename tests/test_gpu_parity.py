@@ -103,6 +103,25 @@ def test_cube_with_obstruction_rays_identical(rvf, orc, session, geometric):
     assert_rel(Fg, Fgo, rtol=1e-12)
 
 
+def test_pair_lists_fine_cube(rvf, orc, session):
+    """Elements much smaller than the obstruction's leaves (the headline
+    shape at 20 x 20 per face): most pending pairs test a short per-pair
+    triangle list instead of walking the tree, the rest walk it; every row
+    the oracle computes (one in 23) agrees to 1e-10."""
+    md = rvf.meshes.cube_enclosure(20, jitter=0.3, seed=2, box=True, box_edge=0.3, box_m=12)
+    N = md.n_elems
+    F, A, Fg, Ag, rs, _, st = device_solve(rvf, session, md, 3, [7])
+    d = st.as_dict()
+    assert d["n_list_pairs"] > 2 * d["n_walk_pairs"] > 0, d
+    m = orc.Mesh(md, [7])
+    raw, area, _, _ = orc.solve_plain(m, 3, row_stride=23)
+    assert np.array_equal(A, area)
+    rows = np.arange(0, N, 23)
+    for i in rows:
+        Fo = raw[i, i + 1:] / area[i]
+        assert_rel(F[i, i + 1:], Fo)
+
+
 @pytest.mark.parametrize("family,nquad", [("quad4", 2), ("quad", 3), ("tri", 4), ("tri3", 1), ("quad", 2)])
 def test_families_with_obstruction(rvf, orc, session, family, nquad):
     md = rvf.meshes.cube_enclosure(3, family=family, box_m=2, box_edge=0.5)
