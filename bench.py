@@ -89,6 +89,10 @@ def workload(rvf, size: str) -> Workload:
         return Workload(M.cube_enclosure(24, jitter=0.3, seed=2, box=True, box_edge=0.3, box_m=12),
                         "cube 24x24/face jittered Tri3 (6,912 elements) + centred 0.3 box (1,728 tris), nquad=3",
                         OBSTRUCTION, NQUAD)
+    if size == "c1":  # the CPU-runnable plain case: coaxial plates, analytic F12 = 0.19982
+        return Workload(M.parallel_plates(20, "quad4"),
+                        "two coaxial unit squares 1 apart, 20x20 Quad4 each (800 elements), Gauss-Legendre nquad=4, "
+                        "no obstruction", [], 4, precisions=("fp64",))
     if size == "c3":  # precision form with Duffy
         return Workload(M.cylinder(nc=64, na=32, caps=True, cap_rings=8, jitter=0.01, seed=3),
                         "open cylinder r=0.5 h=1, 64x32 Quad8 wall + two 64x8 Quad8 annular caps sharing the end "
@@ -593,9 +597,10 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--precision", choices=["fp64", "mixed", "both"], default="both")
-    ap.add_argument("--size", choices=["full", "medium", "small", "c3", "c4"], default="full",
-                    help="full: the headline workload (closed cube, 43,200 Tri3, occluded); c3: cylinder with "
-                         "Duffy pairs; c4: 2-D Monte Carlo cavity; medium / small: the headline shape at m = 24 / 12")
+    ap.add_argument("--size", choices=["full", "medium", "small", "c1", "c3", "c4"], default="full",
+                    help="full: the headline workload (closed cube, 43,200 Tri3, occluded); c1: 20x20 Quad4 plates; "
+                         "c3: cylinder with Duffy pairs; c4: 2-D Monte Carlo cavity; medium / small: the headline "
+                         "shape at m = 24 / 12")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--e2e-warmup", type=int, default=1)
