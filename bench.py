@@ -267,8 +267,9 @@ def timed_solves(dm, opts, steps, warmup, flush, ws, local):
 
 
 def roofline(stats, peak, bound, kernel, prec, size):
-    """Roofline of the dominant kernel, the traversal (FP32 + FP64 re-traversal
-    in mixed mode): algorithmic flop per step / CUDA-event time of the kernel."""
+    """Roofline of the dominant phase, the traversal (pair lists, FP32 rays and
+    the FP64 re-traversal in mixed mode): the reference-order traversal work
+    of the step / CUDA-event time of the phase."""
     s0 = stats[-1]
     trace_ms = statistics.mean(s["ms_trace"] + s["ms_trace_fp64"] for s in stats)
     chunks = max(1, int(s0["n_chunks"]))
@@ -318,7 +319,7 @@ def roof_for(W: Workload, stats, prec, size, peak64, peak32):
                 "kernel": "k_gen_mixed<OCC=0>" if prec == "mixed" else "k_gen_fp64<DIM3=1,OCC=0>",
                 "kernel_ms_per_launch": ms, "launches_per_step": 1, "algorithmic_flop_per_launch": flops,
                 "work_counts": "23 flop per quadrature point pair (Duffy pairs run in k_duffy, timed in phases)"}
-    kernel = "k_trace32 (+ k_trace64 re-traversal)" if prec == "mixed" else "k_trace64<DIM3=1>"
+    kernel = "k_plist + k_trace32 (+ k_trace64 re-traversal)" if prec == "mixed" else "k_plist + k_trace64<DIM3=1>"
     return roofline(stats, peak, bound, kernel, prec, size)
 
 

@@ -108,7 +108,8 @@ typedef struct {
   double near_field_factor;   /* mixed: centroid distance < factor * max diameter runs in FP64 (default 2) */
   uint8_t* ray_log;           /* debug: host buffer of n_elems^2 * ray_log_pm^2 bytes, or NULL */
   int32_t ray_log_pm;         /* stride of the ray log (>= points per element) */
-  int32_t reserved[8];
+  int32_t disable_pair_lists; /* 3-D occlusion: 1 = every ray walks the tree (same results; for testing) */
+  int32_t reserved[7];
 } rvf_options;
 
 typedef struct {

@@ -46,7 +46,8 @@ class Options(C.Structure):
     _fields_ = [("nquad", C.c_int32), ("method", C.c_int32), ("use_duffy", C.c_int32), ("n_samples", C.c_int32),
                 ("seed", C.c_uint64), ("precision", C.c_int32), ("occlusion", C.c_int32),
                 ("geometric_soup", C.c_int32), ("mc_exclude_groups", C.c_int32), ("near_field_factor", C.c_double),
-                ("ray_log", _pu8), ("ray_log_pm", C.c_int32), ("reserved", C.c_int32 * 8)]
+                ("ray_log", _pu8), ("ray_log_pm", C.c_int32), ("disable_pair_lists", C.c_int32),
+                ("reserved", C.c_int32 * 7)]
 
 
 class Stats(C.Structure):

@@ -25,7 +25,7 @@ NVCC_FLAGS = ARCH + [
     "-O3", "-lineinfo", "-std=c++17", "--fmad=false",
     "-Xcompiler", "-fPIC,-ffp-contract=off,-O2",
     "-I", str(CSRC), "-I", str(INCLUDE),
-]
+] + os.environ.get("RVF_NVCC_DEFINES", "").split()  # tuning macros, e.g. -DRVF_PAIR_MIN_BLOCKS=3
 
 
 def _nvcc() -> str:

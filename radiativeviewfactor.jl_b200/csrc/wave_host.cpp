@@ -137,7 +137,7 @@ int wave_prepare(Session* s, rvf_mesh* m, Tables* T, const rvf_options* o, uint8
   ta.N = N; ta.pmax = a.pmax; ta.dim3 = a.dim3; ta.tab = a.tab; ta.tabf = w.ma.tabf; ta.cen = a.cen;
   ta.group = a.group; ta.orig = a.orig; ta.nodes = a.nodes; ta.nodesf = occ ? m->nodesf.as<NodeF>() : nullptr; ta.n_nodes = a.n_nodes;
   ta.tris = a.tris; ta.trisf = w.ma.trisf; ta.segs = a.segs; ta.delta = w.ma.delta;
-  ta.leaf_of = (occ && w.dim3) ? m->leaf_of.as<int32_t>() : nullptr;
+  ta.leaf_of = (occ && w.dim3 && !o->disable_pair_lists) ? m->leaf_of.as<int32_t>() : nullptr;
   ta.sat = (occ && w.dim3) ? (o->geometric_soup ? m->sat_geo.as<float4>() : m->sat_ref.as<float4>()) : nullptr;
   ta.sat_em = m->sat_em;
   ta.frontier = (occ && w.dim3) ? m->frontier.as<int32_t>() : nullptr;

@@ -15,13 +15,14 @@ pytestmark = pytest.mark.gpu
 ATOL_MIXED = 1e-6
 
 
-def mixed_solve(rvf, session, md, nquad, obstruction_groups=(), geometric=False, log_pm=None, near=2.0):
+def mixed_solve(rvf, session, md, nquad, obstruction_groups=(), geometric=False, log_pm=None, near=2.0, lists=True):
     from rvf_b200 import _abi
     dm = _abi.DeviceMesh(session, rvf.mesh_desc_arrays(md, obstruction_groups))
     try:
         N = md.n_elems
         o = rvf.make_options(nquad, precision="mixed", geometric_soup=geometric, seed=0)
         o.near_field_factor = near
+        o.disable_pair_lists = 0 if lists else 1
         log = None
         if log_pm:
             log = np.zeros(N * N * log_pm * log_pm, dtype=np.uint8)
@@ -36,11 +37,12 @@ def mixed_solve(rvf, session, md, nquad, obstruction_groups=(), geometric=False,
         dm.release()
 
 
+@pytest.mark.parametrize("lists", [True, False])
 @pytest.mark.parametrize("near", [2.0, 0.0, 1e9])
 @pytest.mark.parametrize("geometric", [False, True])
-def test_cube_mixed_rays_identical(rvf, orc, session, near, geometric):
+def test_cube_mixed_rays_identical(rvf, orc, session, near, geometric, lists):
     md = rvf.meshes.cube_enclosure(8, box_m=4)
-    F, A, rs, log, st = mixed_solve(rvf, session, md, 3, [7], geometric, log_pm=7, near=near)
+    F, A, rs, log, st = mixed_solve(rvf, session, md, 3, [7], geometric, log_pm=7, near=near, lists=lists)
     Fo, Ao, Fgo, Ago, logo, cnt = oracle_solve(orc, md, 3, [7], geometric, log_pm=7)
     assert np.array_equal(A, Ao)
     assert (logo == 2).sum() > 0
@@ -58,7 +60,9 @@ def test_pair_lists_fine_cube_mixed(rvf, orc, session):
     md = rvf.meshes.cube_enclosure(20, jitter=0.3, seed=2, box=True, box_edge=0.3, box_m=12)
     N = md.n_elems
     F, A, rs, _, st = mixed_solve(rvf, session, md, 3, [7])
-    assert st["n_list_pairs"] > 2 * st["n_walk_pairs"] > 0, st
+    assert st["n_list_pairs"] > 100 * st["n_walk_pairs"], st
+    Fw, *_ = mixed_solve(rvf, session, md, 3, [7], lists=False)
+    assert np.array_equal(F, Fw, equal_nan=True)
     m = orc.Mesh(md, [7])
     raw, area, _, _ = orc.solve_plain(m, 3, row_stride=23)
     assert np.array_equal(A, area)

@@ -46,13 +46,14 @@ def concat(*meshes):
                         meshes[0].mesh_dim)
 
 
-def device_solve(rvf, session, md, nquad, obstruction_groups=(), geometric=False, log_pm=None):
+def device_solve(rvf, session, md, nquad, obstruction_groups=(), geometric=False, log_pm=None, lists=True):
     from rvf_b200 import _abi
     dm = _abi.DeviceMesh(session, rvf.mesh_desc_arrays(md, obstruction_groups))
     try:
         N = md.n_elems
         G = len(md.group_tags)
         o = rvf.make_options(nquad, geometric_soup=geometric, seed=0)
+        o.disable_pair_lists = 0 if lists else 1
         log = None
         if log_pm:
             log = np.zeros(N * N * log_pm * log_pm, dtype=np.uint8)
@@ -90,10 +91,11 @@ def test_parallel_plates_config(rvf, orc, session):
     assert st.n_pairs == 800 * 799 // 2
 
 
+@pytest.mark.parametrize("lists", [True, False])
 @pytest.mark.parametrize("geometric", [False, True])
-def test_cube_with_obstruction_rays_identical(rvf, orc, session, geometric):
+def test_cube_with_obstruction_rays_identical(rvf, orc, session, geometric, lists):
     md = rvf.meshes.cube_enclosure(6, box_m=3)
-    F, A, Fg, Ag, rs, log, st = device_solve(rvf, session, md, 3, [7], geometric, log_pm=7)
+    F, A, Fg, Ag, rs, log, st = device_solve(rvf, session, md, 3, [7], geometric, log_pm=7, lists=lists)
     Fo, Ao, Fgo, Ago, logo, cnt = oracle_solve(orc, md, 3, [7], geometric, log_pm=7)
     assert np.array_equal(A, Ao)
     assert int((logo > 0).sum()) == st.n_rays == cnt[1]
@@ -105,14 +107,18 @@ def test_cube_with_obstruction_rays_identical(rvf, orc, session, geometric):
 
 def test_pair_lists_fine_cube(rvf, orc, session):
     """Elements much smaller than the obstruction's leaves (the headline
-    shape at 20 x 20 per face): most pending pairs test a short per-pair
-    triangle list instead of walking the tree, the rest walk it; every row
-    the oracle computes (one in 23) agrees to 1e-10."""
+    shape at 20 x 20 per face): pending pairs test a short per-pair triangle
+    list instead of walking the tree.  Every row the oracle computes (one in
+    23) agrees to 1e-10, and with the lists disabled (every ray walks the
+    tree) F is bit for bit the same."""
     md = rvf.meshes.cube_enclosure(20, jitter=0.3, seed=2, box=True, box_edge=0.3, box_m=12)
     N = md.n_elems
     F, A, Fg, Ag, rs, _, st = device_solve(rvf, session, md, 3, [7])
     d = st.as_dict()
-    assert d["n_list_pairs"] > 2 * d["n_walk_pairs"] > 0, d
+    assert d["n_list_pairs"] > 100 * d["n_walk_pairs"], d
+    Fw, Aw, *_, stw = device_solve(rvf, session, md, 3, [7], lists=False)
+    assert stw.as_dict()["n_list_pairs"] == 0 and stw.as_dict()["n_walk_pairs"] == d["n_list_pairs"] + d["n_walk_pairs"]
+    assert np.array_equal(F, Fw, equal_nan=True)
     m = orc.Mesh(md, [7])
     raw, area, _, _ = orc.solve_plain(m, 3, row_stride=23)
     assert np.array_equal(A, area)
