@@ -49,10 +49,12 @@ REF_COUNTS = {
     "medium": {"n_rays": 975146106, "node_visits": 5688464541, "prim_tests": 3647097481},
     "full": {"n_rays": 38102400000, "node_visits": 222278703194, "prim_tests": 142516108216},
 }
-# DRAM bytes per traced ray of the traversal kernels (dram__bytes_read.sum +
-# dram__bytes_write.sum of one ncu capture on the medium workload divided by
-# the rays it traced; the capture is summarized under profiles/).
-TRAFFIC_PER_TRACED_RAY = {"mixed": 1.247057e9 / 137006664, "fp64": 1.243367e9 / 137012826}
+# DRAM bytes per traced ray of the traversal phase, pair lists included
+# (dram__bytes_read.sum + dram__bytes_write.sum of k_trace32 / k_trace64 and
+# k_plist in one ncu capture of the medium workload divided by the rays it
+# traced; the capture is summarized under profiles/).
+TRAFFIC_PER_TRACED_RAY = {"mixed": (1.550799e9 + 0.032135e9 + 0.077273e9 + 0.239007e9) / 137006664,
+                          "fp64": (1.552282e9 + 0.029719e9 + 0.077296e9 + 0.238736e9) / 137012826}
 
 
 def load_pkg():
