@@ -83,7 +83,8 @@ __device__ __forceinline__ void stage_flush(uint64_t* st, int& n, int k, uint64_
 // it is full and when the pair ends.  A traversal warp takes 32 consecutive
 // records, so its rays come from one or two pairs -- thin bundles whose walks
 // agree -- instead of one ray from each of 32 pairs.
-constexpr int kRun = 16;
+constexpr int kRun = 16;     // FP64 generation: 32 would cost a third of its occupancy
+constexpr int kRunMix = 32;  // mixed generation (two blocks per SM anyway): one pair per traversal warp
 
 __device__ __forceinline__ void run_push(uint64_t* ring, int& nr, bool push, uint64_t rec) {
   if (push) {
@@ -94,10 +95,11 @@ __device__ __forceinline__ void run_push(uint64_t* ring, int& nr, bool push, uin
 
 // Appends the full runs (all runs when `all`) of the warp's lanes, lane by
 // lane, with one counter update.  Warp-uniform call.
+template <int RUN>
 __device__ __forceinline__ void run_flush(uint64_t* ring, int& nr, bool all, uint64_t* queue,
                                           unsigned long long* count, unsigned long long* tile_used) {
   const int lane = threadIdx.x & 31;
-  const int mine = (all || nr == kRun) ? nr : 0;
+  const int mine = (all || nr == RUN) ? nr : 0;
   int incl = mine;
 #pragma unroll
   for (int o = 1; o < 32; o <<= 1) {
@@ -363,7 +365,8 @@ __global__ void __launch_bounds__(256, 3) k_gen_fp64(const GenBatch* __restrict_
             if (__any_sync(kFull, defer)) {
               slot_alloc(Q, defer && slot < 0, slot, &s_slots);
               run_push(ring, nr, defer, rec_make(slot, sw, p, q));
-              if (__any_sync(kFull, nr == kRun)) run_flush(ring, nr, false, Q.rec64, Q.ctr + kCtrRec64, &s_used);
+              if (__any_sync(kFull, nr == kRun))
+                run_flush<kRun>(ring, nr, false, Q.rec64, Q.ctr + kCtrRec64, &s_used);
               if (defer) K = 0.0;
             }
           }
@@ -371,7 +374,7 @@ __global__ void __launch_bounds__(256, 3) k_gen_fp64(const GenBatch* __restrict_
         }
         acc = fma(wj, inner, acc);
       }
-      if (OCC && __any_sync(kFull, nr > 0)) run_flush(ring, nr, true, Q.rec64, Q.ctr + kCtrRec64, &s_used);
+      if (OCC && __any_sync(kFull, nr > 0)) run_flush<kRun>(ring, nr, true, Q.rec64, Q.ctr + kCtrRec64, &s_used);
       if (slot >= 0) {
         PendSlot ps;
         ps.i = (int32_t)i;
@@ -455,7 +458,7 @@ __global__ void __launch_bounds__(256, 2) k_gen_mixed(const GenBatch* __restrict
   // directions, a few per cent): per-warp staging
   uint64_t* stage_all = reinterpret_cast<uint64_t*>(smem + gen_tab_bytes(true, pmL));
   uint64_t* ring = stage_all + (OCC ? 8 * 64 : 0) + threadIdx.x;
-  uint64_t* bar = stage_all + (OCC ? 8 * 64 + kRun * 256 : 0);
+  uint64_t* bar = stage_all + (OCC ? 8 * 64 + kRunMix * 256 : 0);
   __shared__ int64_t s_tile;
   __shared__ int s_req;
   __shared__ unsigned long long s_used, s_slots;
@@ -608,7 +611,8 @@ __global__ void __launch_bounds__(256, 2) k_gen_mixed(const GenBatch* __restrict
             stage_push(st64, n64, defer64, rec_make(slot, sw, p, q));
             if (n64 >= 32) stage_flush(st64, n64, 32, Q.rec64, Q.ctr + kCtrRec64, &s_used);
             run_push(ring, nr, defer32, rec_make(slot, sw, p, q));
-            if (__any_sync(kFull, nr == kRun)) run_flush(ring, nr, false, Q.rec32, Q.ctr + kCtrRec32, &s_used);
+            if (__any_sync(kFull, nr == kRunMix))
+              run_flush<kRunMix>(ring, nr, false, Q.rec32, Q.ctr + kCtrRec32, &s_used);
           }
           if (far && !graze && !badray && !defer32) inner = fmaf(wp, K32, inner);
         }
@@ -616,7 +620,7 @@ __global__ void __launch_bounds__(256, 2) k_gen_mixed(const GenBatch* __restrict
       }
       if (OCC) {
         if (n64 > 0) stage_flush(st64, n64, n64, Q.rec64, Q.ctr + kCtrRec64, &s_used);
-        if (__any_sync(kFull, nr > 0)) run_flush(ring, nr, true, Q.rec32, Q.ctr + kCtrRec32, &s_used);
+        if (__any_sync(kFull, nr > 0)) run_flush<kRunMix>(ring, nr, true, Q.rec32, Q.ctr + kCtrRec32, &s_used);
       }
       const double raw = accd + (double)acc32;
       if (slot >= 0) {
@@ -1240,7 +1244,7 @@ __global__ void __launch_bounds__(256) k_resolve_mixed(const ResolveBatch* __res
 size_t gen_smem_bytes(bool mixed, int pmax, bool occ) {
   // tile block, then (occlusion) the per-warp FP64 staging (mixed) and the
   // per-lane runs, then the mbarrier
-  const size_t stage = occ ? ((mixed ? (size_t)8 * 64 : 0) + (size_t)kRun * 256) * sizeof(uint64_t) : 0;
+  const size_t stage = occ ? ((mixed ? (size_t)8 * 64 + kRunMix * 256 : (size_t)kRun * 256)) * sizeof(uint64_t) : 0;
   return gen_tab_bytes(mixed, pmax) + stage + 16;
 }
 
