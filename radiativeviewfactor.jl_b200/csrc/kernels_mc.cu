@@ -45,9 +45,12 @@ __device__ __forceinline__ double ref_measure(int f) { return is_quad_fam(f) ? 4
 
 // sample of one element at (u, v) in [0,1]^2 (src/GPUMCKernels.jl:266-281)
 // or, for curves, at reference coordinate u (already mapped to [-1,1]).
+// A curve mesh holds line elements only, a surface mesh surface elements
+// only: each kernel compiles its own families.
+template <bool DIM3>
 __device__ __forceinline__ void mc_point(const McArgs& a, const int32_t* en, int f, double u, double v, double* x,
                                          double* n, double* dA) {
-  if (is_line_fam(f)) {
+  if (!DIM3) {
     eval_line(a.coords, en, f, u, x, n, dA);
   } else if (is_quad_fam(f)) {
     eval_surface(a.coords, en, f, 2.0 * u - 1.0, 2.0 * v - 1.0, x, n, dA);
@@ -104,14 +107,18 @@ __global__ void k_mc_area(McArgs a) {
     mc_coords(a.dim3, k, s, st, ci, cj);
     const double* c = first ? ci : cj;
     double x[3], n[3], dA;
-    mc_point(a, en, f, c[0], c[1], x, n, &dA);
+    if (a.dim3) mc_point<true>(a, en, f, c[0], c[1], x, n, &dA);
+    else mc_point<false>(a, en, f, c[0], c[1], x, n, &dA);
     A += dA;
   }
   a.area_orig[e] = (A * ref_measure(f)) / (double)a.n_samples;
 }
 
+#ifndef RVF_MC2D_MIN_BLOCKS
+#define RVF_MC2D_MIN_BLOCKS 3  // curves: resident blocks of 256 per SM the kernel is compiled for
+#endif
 template <bool DIM3, bool OCC>
-__global__ void __launch_bounds__(256) k_pairs_mc(McArgs a) {
+__global__ void __launch_bounds__(256, DIM3 ? 1 : RVF_MC2D_MIN_BLOCKS) k_pairs_mc(McArgs a) {
   __shared__ int64_t s_tile;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int64_t N = a.N;
@@ -150,8 +157,8 @@ __global__ void __launch_bounds__(256) k_pairs_mc(McArgs a) {
         double ci[2], cj[2];
         mc_coords(DIM3, k, s, st, ci, cj);
         double xi[3], ni[3], dAi, xj[3], nj[3], dAj;
-        mc_point(a, en_lo, f_lo, ci[0], ci[1], xi, ni, &dAi);
-        mc_point(a, en_hi, f_hi, cj[0], cj[1], xj, nj, &dAj);
+        mc_point<DIM3>(a, en_lo, f_lo, ci[0], ci[1], xi, ni, &dAi);
+        mc_point<DIM3>(a, en_hi, f_hi, cj[0], cj[1], xj, nj, &dAj);
         const double rx = xj[0] - xi[0], ry = xj[1] - xi[1], rz = xj[2] - xi[2];
         const double r2 = (rx * rx + ry * ry) + rz * rz;
         double K = 0.0;
@@ -219,8 +226,14 @@ __global__ void __launch_bounds__(256) k_pairs_mc(McArgs a) {
 }
 
 template <bool D3, bool O>
-static cudaError_t launch_mc_t(const McArgs& a, int grid, cudaStream_t st) {
-  k_pairs_mc<D3, O><<<grid, 256, 0, st>>>(a);
+static cudaError_t launch_mc_t(const McArgs& a, int sm_count, cudaStream_t st) {
+  // persistent blocks: as many as are resident at once
+  int per_sm = 1;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pairs_mc<D3, O>, 256, 0) != cudaSuccess || per_sm < 1)
+    per_sm = 1;
+  int64_t grid = (int64_t)sm_count * per_sm;
+  if (grid > a.tile_count) grid = a.tile_count;
+  k_pairs_mc<D3, O><<<(unsigned)grid, 256, 0, st>>>(a);
   return cudaGetLastError();
 }
 
@@ -232,12 +245,9 @@ cudaError_t launch_mc(const McArgs& a, int sm_count, cudaStream_t st) {
     if (e != cudaSuccess) return e;
   }
   if (a.tile_count <= 0) return cudaSuccess;
-  int64_t grid = (int64_t)sm_count * 3;
-  if (grid > a.tile_count) grid = a.tile_count;
-  if (grid < 1) grid = 1;
   const bool occ = a.n_nodes > 0;
-  if (a.dim3) return occ ? launch_mc_t<true, true>(a, (int)grid, st) : launch_mc_t<true, false>(a, (int)grid, st);
-  return occ ? launch_mc_t<false, true>(a, (int)grid, st) : launch_mc_t<false, false>(a, (int)grid, st);
+  if (a.dim3) return occ ? launch_mc_t<true, true>(a, sm_count, st) : launch_mc_t<true, false>(a, sm_count, st);
+  return occ ? launch_mc_t<false, true>(a, sm_count, st) : launch_mc_t<false, false>(a, sm_count, st);
 }
 
 }  // namespace rvf
