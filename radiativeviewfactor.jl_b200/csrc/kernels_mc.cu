@@ -47,20 +47,29 @@ __device__ __forceinline__ double ref_measure(int f) { return is_quad_fam(f) ? 4
 // or, for curves, at reference coordinate u (already mapped to [-1,1]).
 // A curve mesh holds line elements only, a surface mesh surface elements
 // only: each kernel compiles its own families.
-template <bool DIM3>
-__device__ __forceinline__ void mc_point(const McArgs& a, const int32_t* en, int f, double u, double v, double* x,
-                                         double* n, double* dA) {
-  if (!DIM3) {
-    eval_line(a.coords, en, f, u, x, n, dA);
-  } else if (is_quad_fam(f)) {
-    eval_surface(a.coords, en, f, 2.0 * u - 1.0, 2.0 * v - 1.0, x, n, dA);
+// Surfaces: out of line, so that the six families' geometry does not
+// hold the pair kernel's registers.
+__device__ __noinline__ void mc_surface(const double* coords, const int32_t* en, int f, double u, double v, double* x,
+                                        double* n, double* dA) {
+  if (is_quad_fam(f)) {
+    eval_surface(coords, en, f, 2.0 * u - 1.0, 2.0 * v - 1.0, x, n, dA);
   } else {
     double xi = u, eta = v;
     if (xi + eta > 1.0) {
       xi = 1.0 - xi;
       eta = 1.0 - eta;
     }
-    eval_surface(a.coords, en, f, xi, eta, x, n, dA);
+    eval_surface(coords, en, f, xi, eta, x, n, dA);
+  }
+}
+
+template <bool DIM3>
+__device__ __forceinline__ void mc_point(const McArgs& a, const int32_t* en, int f, double u, double v, double* x,
+                                         double* n, double* dA) {
+  if (!DIM3) {
+    eval_line(a.coords, en, f, u, x, n, dA);
+  } else {
+    mc_surface(a.coords, en, f, u, v, x, n, dA);
   }
 }
 
@@ -118,7 +127,7 @@ __global__ void k_mc_area(McArgs a) {
 #define RVF_MC2D_MIN_BLOCKS 3  // curves: resident blocks of 256 per SM the kernel is compiled for
 #endif
 template <bool DIM3, bool OCC>
-__global__ void __launch_bounds__(256, DIM3 ? 1 : RVF_MC2D_MIN_BLOCKS) k_pairs_mc(McArgs a) {
+__global__ void __launch_bounds__(256, DIM3 ? 2 : RVF_MC2D_MIN_BLOCKS) k_pairs_mc(McArgs a) {
   __shared__ int64_t s_tile;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int64_t N = a.N;
