@@ -54,6 +54,19 @@ def test_cube_mixed_rays_identical(rvf, orc, session, near, geometric, lists):
         assert st["n_pairs_fp64"] > 0
 
 
+@pytest.mark.parametrize("lists", [True, False])
+def test_surface_groups_as_obstructions_mixed(rvf, orc, session, lists):
+    """Faces that are both surfaces and obstructions, FP32 rays: own groups
+    skipped, ray decisions identical to the FP64 oracle's."""
+    md = rvf.meshes.cube_enclosure(6, box_m=3)
+    obs = [2, 5, 7]
+    F, A, rs, log, st = mixed_solve(rvf, session, md, 3, obs, log_pm=7, lists=lists)
+    Fo, Ao, Fgo, Ago, logo, cnt = oracle_solve(orc, md, 3, obs, log_pm=7)
+    assert (logo == 2).sum() > 0
+    assert np.array_equal(log, logo), f"{int((log != logo).sum())} ray decisions differ (stats {st})"
+    assert np.max(np.abs(F - Fo)) <= ATOL_MIXED
+
+
 def test_pair_lists_fine_cube_mixed(rvf, orc, session):
     """Per-pair triangle lists under FP32 rays (certified decisions, FP64
     re-tests): every sampled row within 1e-6 of the FP64 oracle."""

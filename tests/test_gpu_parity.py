@@ -105,6 +105,20 @@ def test_cube_with_obstruction_rays_identical(rvf, orc, session, geometric, list
     assert_rel(Fg, Fgo, rtol=1e-12)
 
 
+@pytest.mark.parametrize("lists", [True, False])
+def test_surface_groups_as_obstructions(rvf, orc, session, lists):
+    """Faces that are both surfaces and obstructions: each ray skips the
+    triangles of its own two groups (src/GPUBVH.jl:239-240), in the pair
+    lists as in the walk; ray decisions identical to the oracle's."""
+    md = rvf.meshes.cube_enclosure(6, box_m=3)
+    obs = [2, 5, 7]
+    F, A, Fg, Ag, rs, log, st = device_solve(rvf, session, md, 3, obs, log_pm=7, lists=lists)
+    Fo, Ao, Fgo, Ago, logo, cnt = oracle_solve(orc, md, 3, obs, log_pm=7)
+    assert (logo == 2).sum() > 0
+    assert np.array_equal(log, logo), f"{int((log != logo).sum())} ray decisions differ"
+    assert_rel(F, Fo)
+
+
 def test_pair_lists_fine_cube(rvf, orc, session):
     """Elements much smaller than the obstruction's leaves (the headline
     shape at 20 x 20 per face): pending pairs test a short per-pair triangle
