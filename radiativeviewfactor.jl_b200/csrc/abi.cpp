@@ -46,10 +46,32 @@ int cuda_err(cudaError_t e, const char* what) {
 int DevBuf::alloc(Session* s, size_t n) {
   free_();
   if (n == 0) return RVF_OK;
+  if (n >= kSpareMin) {
+    // the smallest cached buffer that holds n with at most a quarter to spare
+    std::lock_guard<std::mutex> lk(s->spare_mu);
+    size_t best = s->spares.size();
+    for (size_t k = 0; k < s->spares.size(); ++k) {
+      const size_t b = s->spares[k].second;
+      if (b >= n && b - n <= n / 4 && (best == s->spares.size() || b < s->spares[best].second)) best = k;
+    }
+    if (best < s->spares.size()) {
+      ptr = s->spares[best].first;
+      bytes = s->spares[best].second;
+      owner = s;
+      s->spares.erase(s->spares.begin() + (std::ptrdiff_t)best);
+      return RVF_OK;  // already charged to the budget
+    }
+  }
+  if (s->used + n > s->budget) release_spares(s);
   if (s->used + n > s->budget)
     return set_err(RVF_EBUDGET, "HBM budget exceeded: need %zu more bytes, %zu of %zu in use", n, s->used,
                    s->budget);
   cudaError_t e = cudaMalloc(&ptr, n);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    release_spares(s);
+    e = cudaMalloc(&ptr, n);
+  }
   if (e != cudaSuccess) {
     ptr = nullptr;
     cudaGetLastError();
@@ -62,12 +84,26 @@ int DevBuf::alloc(Session* s, size_t n) {
 }
 void DevBuf::free_() {
   if (ptr) {
-    cudaFree(ptr);
-    if (owner) owner->used -= bytes;
+    if (owner && bytes >= kSpareMin) {
+      std::lock_guard<std::mutex> lk(owner->spare_mu);
+      owner->spares.emplace_back(ptr, bytes);  // stays charged to the budget
+    } else {
+      cudaFree(ptr);
+      if (owner) owner->used -= bytes;
+    }
   }
   ptr = nullptr;
   bytes = 0;
   owner = nullptr;
+}
+
+void release_spares(Session* s) {
+  std::lock_guard<std::mutex> lk(s->spare_mu);
+  for (auto& sp : s->spares) {
+    cudaFree(sp.first);
+    s->used -= sp.second;
+  }
+  s->spares.clear();
 }
 
 int upload(Session* s, DevBuf& b, const void* src, size_t n) {

@@ -42,6 +42,8 @@ struct DevBuf {
 };
 
 int upload(Session* s, DevBuf& b, const void* src, size_t n);
+constexpr size_t kSpareMin = (size_t)64 << 20;
+void release_spares(Session* s);
 
 struct Tables {
   int nquad = 0, pmax = 0;
@@ -70,6 +72,13 @@ struct rvf_session {
   std::map<uint64_t, cudaGraphExec_t> graphs;
   std::set<rvf_mesh*> meshes;
   cudaEvent_t ev[8] = {};
+  // Freed device buffers of kSpareMin bytes or more, kept for reuse and still
+  // charged to the budget: solving one new mesh after another (an F of
+  // 15 GB each) then skips cudaMalloc / cudaFree, whose mapping work costs
+  // a few hundred milliseconds per mesh.  Dropped when an allocation would
+  // exceed the budget, and at session destroy.
+  std::mutex spare_mu;
+  std::vector<std::pair<void*, size_t>> spares;
 };
 
 struct rvf_mesh {

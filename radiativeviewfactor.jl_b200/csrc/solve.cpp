@@ -282,6 +282,7 @@ int rvf_session_destroy(rvf_session* s) {
       b->free_();
     for (auto& kv : s->graphs) cudaGraphExecDestroy(kv.second);
     s->graphs.clear();
+    rvf::release_spares(s);
     if (s->h_ctr) cudaFreeHost(s->h_ctr);
     s->h_ctr = nullptr;
     for (cudaEvent_t v : s->ev)
