@@ -8,11 +8,14 @@
 //      summed at once; every other ray is appended to a global ray queue as
 //      (pending-pair slot, p, q, swapped), and its pair gets a slot holding
 //      (i, j, sum of the immediate terms).  Pairs without queued rays write F.
-//   2. traversal: one queued ray per lane, 32 rays per warp traced together
+//   2. pair lists (3-D triangles): one warp per pending pair finds the
+//      triangles any ray of the pair can hit (k_plist, below).
+//   3. traversal: one queued ray per lane, 32 rays per warp traced together,
+//      each against its pair's list or by a walk of the tree
 //      (device_trace.cuh), at the occupancy a traversal-only kernel allows.
 //      Each visible ray sets its (p, q) bit in its slot's visibility words
 //      with an integer atomicOr -- order-independent, hence deterministic.
-//   3. resolve: per pending pair, the terms of the visible queued rays are
+//   4. resolve: per pending pair, the terms of the visible queued rays are
 //      formed again with the generation's arithmetic and added, in (p, q)
 //      order, to the immediate sum; F[i,j] and F[j,i] are written.
 // Mixed precision adds an FP32 queue: FP32 rays whose certified traversal is

@@ -376,7 +376,6 @@ int rvf_solve(rvf_session* s, rvf_mesh* m, const rvf_options* o, double* F_elem,
     if ((rc = log.alloc(s, lb))) return rc;
     cudaMemsetAsync(log.ptr, 0, lb, s->stream);
   }
-  const bool occ = o->occlusion && m->n_nodes > 0;
   if (mc) {  // src/GPUMCKernels.jl:295-328
     McArgs c{};
     fill_mc_args(s, m, o, o->ray_log ? log.as<uint8_t>() : nullptr, c);
