@@ -174,13 +174,22 @@ def dist_setup():
 
 
 def allreduce_max(x: float, ws: int) -> float:
+    """Max over ranks (the slowest replica's time), on the process group's
+    own device: CUDA for NCCL, the host for gloo."""
     if ws == 1:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def job_rate(units_per_rank: float, seconds_max: float, ws: int) -> float:
+    """Whole-job throughput of ws replicas that each processed units_per_rank
+    units, timed as the slowest rank (weak scaling: per-rank work is fixed)."""
+    return ws * units_per_rank / seconds_max
 
 
 def barrier(ws: int):
@@ -505,7 +514,7 @@ def run_ours(args):
         stats, clocks = timed_solves(dm, opts, args.steps, args.warmup, flush, ws, local)
         total_ms = allreduce_max(sum(s["ms_total"] for s in stats), ws)
         runs[prec] = {"stats": stats, "clocks": clocks, "ms": total_ms / args.steps,
-                      "value": ws * pairs * args.steps / (total_ms / 1e3)}
+                      "value": job_rate(pairs * args.steps, total_ms / 1e3, ws)}
         meshes[prec] = dm
     accuracy = None
     if len(precisions) == 2:
@@ -550,7 +559,7 @@ def run_ours(args):
             if k >= args.e2e_warmup:
                 times.append(t1 - t0)
         t = allreduce_max(sum(times), ws)
-        e2e = {"value": ws * pairs * len(times) / t, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+        e2e = {"value": job_rate(pairs * len(times), t, ws), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                "d2h_bytes_per_step": int(d2h), "host_buffer": "pinned" if pinned else "pageable",
                "steps": len(times), "s_per_step": t / len(times), "precision": head}
         if pinned:
