@@ -237,8 +237,9 @@ def cpu_baseline(rvf, W: Workload, seconds: float, offset: int = 0):
 
 
 def run_reference(args):
-    ws, rank, local = dist_setup() if int(os.environ.get("WORLD_SIZE", "1")) > 1 else (1, 0, 0)
-    if rank != 0:
+    # a host-only run: rank 0 measures and prints, the other ranks exit at once
+    # (no process group, no GPU)
+    if int(os.environ.get("RANK", "0")) != 0:
         return
     rvf = load_pkg()
     W = workload(rvf, args.size)
