@@ -57,6 +57,7 @@ struct Tables {
 struct rvf_session {
   int device = 0;
   cudaStream_t stream = nullptr;
+  cudaStream_t copy_stream = nullptr;  // downloads of finished F columns while later chunks compute
   size_t budget = 0, used = 0;
   int sm_count = 0;
   size_t smem_optin = 0;

@@ -252,6 +252,8 @@ int rvf_session_create(const rvf_session_opts* opts, rvf_session** out) {
   s->smem_optin = p.sharedMemPerBlockOptin;
   if ((e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking)) != cudaSuccess)
     return cuda_err(e, "cudaStreamCreate");
+  if ((e = cudaStreamCreateWithFlags(&s->copy_stream, cudaStreamNonBlocking)) != cudaSuccess)
+    return cuda_err(e, "cudaStreamCreate");
   for (cudaEvent_t& v : s->ev)
     if ((e = cudaEventCreate(&v)) != cudaSuccess) return cuda_err(e, "cudaEventCreate");
   size_t fr = 0, tot = 0;
@@ -288,6 +290,7 @@ int rvf_session_destroy(rvf_session* s) {
     for (cudaEvent_t v : s->ev)
       if (v) cudaEventDestroy(v);
     cudaStreamDestroy(s->stream);
+    if (s->copy_stream) cudaStreamDestroy(s->copy_stream);
   }
   delete s;
   return RVF_OK;
@@ -330,6 +333,56 @@ int rvf_mesh_n_elems(const rvf_mesh* m, int64_t* n) {
   return RVF_OK;
 }
 
+namespace {
+
+// Download of F overlapped with the pair pipeline.  Tiles are claimed in
+// row-major order over (bi <= bj); internal column j of F is final once tile
+// row floor(j / 32) is done -- later tiles (bi', bj') with bi' > bi write only
+// columns of internal elements in blocks >= bi' -- so after each chunk the
+// caller's columns orig[j] of the newly finished rows go to the host on the
+// copy stream while the next chunk computes (contiguous caller columns in
+// one copy).  A pageable destination makes the copies synchronous: still
+// correct, without the overlap.
+struct ColumnDownload {
+  Session* s = nullptr;
+  const rvf_mesh* m = nullptr;
+  double* host = nullptr;
+  int64_t N = 0, nT = 0, rows_done = 0;
+  bool issued = false;
+  std::vector<int32_t> cols;
+
+  // one past the last tile of row bi
+  int64_t row_end(int64_t bi) const { return (bi + 1) * nT - bi * (bi + 1) / 2; }
+
+  cudaError_t advance(int64_t claimed_tiles) {
+    cols.clear();
+    while (rows_done < nT && row_end(rows_done) <= claimed_tiles) {
+      const int64_t j1 = std::min<int64_t>(N, (rows_done + 1) * kTile);
+      for (int64_t j = rows_done * kTile; j < j1; ++j) cols.push_back(m->h_orig[j]);
+      ++rows_done;
+    }
+    std::sort(cols.begin(), cols.end());
+    const double* dev = m->F.as<double>();
+    for (size_t a = 0; a < cols.size();) {
+      size_t b = a + 1;
+      while (b < cols.size() && cols[b] == cols[b - 1] + 1) ++b;
+      const int64_t c0 = cols[a], nc = (int64_t)(b - a);
+      const cudaError_t e = cudaMemcpyAsync(host + c0 * N, dev + c0 * N, sizeof(double) * N * nc,
+                                            cudaMemcpyDeviceToHost, s->copy_stream);
+      if (e != cudaSuccess) return e;
+      issued = true;
+      a = b;
+    }
+    return cudaSuccess;
+  }
+  // copies still in flight must end before the caller's buffer can be reused
+  ~ColumnDownload() {
+    if (issued) cudaStreamSynchronize(s->copy_stream);
+  }
+};
+
+}  // namespace
+
 int rvf_solve(rvf_session* s, rvf_mesh* m, const rvf_options* o, double* F_elem, double* A_elem, double* F_group,
               double* A_group, double* row_sums, rvf_stats* st) {
   if (!s || !m || !o) return set_err(RVF_EINVAL, "null argument");
@@ -368,6 +421,9 @@ int rvf_solve(rvf_session* s, rvf_mesh* m, const rvf_options* o, double* F_elem,
   cudaMemsetAsync(s->counters.ptr, 0, 256, s->stream);
   cudaMemsetAsync(s->err.ptr, 0, sizeof(int), s->stream);
   DevBuf log;
+  ColumnDownload dl;    // quadrature with a host F: columns go down as their tile rows finish
+  int64_t w_tiles = 0;  // tiles done by the pair pipeline
+  size_t log_bytes = 0;  // the caller's log size (a reused device buffer may be larger)
   if (o->ray_log) {
     if (!mc && o->ray_log_pm < T->pmax)
       return set_err(RVF_EINVAL, "ray_log_pm %d < points per element %d", o->ray_log_pm, T->pmax);
@@ -375,6 +431,7 @@ int rvf_solve(rvf_session* s, rvf_mesh* m, const rvf_options* o, double* F_elem,
     size_t lb = (size_t)N * N * (mc ? (size_t)o->n_samples : (size_t)o->ray_log_pm * o->ray_log_pm);
     if ((rc = log.alloc(s, lb))) return rc;
     cudaMemsetAsync(log.ptr, 0, lb, s->stream);
+    log_bytes = lb;
   }
   if (mc) {  // src/GPUMCKernels.jl:295-328
     McArgs c{};
@@ -395,6 +452,14 @@ int rvf_solve(rvf_session* s, rvf_mesh* m, const rvf_options* o, double* F_elem,
     cudaError_t e = cudaSuccess;
     WaveReq w;
     if ((rc = wave_prepare(s, m, T, o, o->ray_log ? log.as<uint8_t>() : nullptr, w, &n_kernels))) return rc;
+    // Duffy pairs overwrite F after the pipeline: no early columns then
+    if (F_elem && N > 1 && !(o->use_duffy && m->dim == 2)) {
+      dl.s = s;
+      dl.m = m;
+      dl.host = F_elem;
+      dl.N = N;
+      dl.nT = (N + kTile - 1) / kTile;
+    }
     EvTimer t(s->stream);
     WaveReq* one = &w;
     while (!w.done()) {  // chunks: each claims tiles while the ray queues have room
@@ -411,7 +476,9 @@ int rvf_solve(rvf_session* s, rvf_mesh* m, const rvf_options* o, double* F_elem,
       S.ms_lists += ci.ms_lists;
       S.n_rays_traced += ci.rays_traced;
       if (w.claimed == before) return set_err(RVF_ENOMEM, "pair pipeline made no progress: ray queue too small for one tile");
+      if (dl.host && (e = dl.advance(w.claimed)) != cudaSuccess) return cuda_err(e, "F column download");
     }
+    w_tiles = w.claimed;
     S.ms_pairs = t.stop();
     if ((rc = read_err(s))) return rc;
     // Duffy integrals overwrite the singular Quad8 pairs (Duffy for
@@ -457,7 +524,12 @@ int rvf_solve(rvf_session* s, rvf_mesh* m, const rvf_options* o, double* F_elem,
   {
     EvTimer t(s->stream);
     cudaError_t e = cudaSuccess;
-    if (F_elem && N > 0) e = cudaMemcpyAsync(F_elem, m->F.ptr, sizeof(double) * N * N, cudaMemcpyDeviceToHost, s->stream);
+    if (F_elem && N > 0 && !dl.host)
+      e = cudaMemcpyAsync(F_elem, m->F.ptr, sizeof(double) * N * N, cudaMemcpyDeviceToHost, s->stream);
+    if (e == cudaSuccess && dl.host) {
+      e = dl.advance(w_tiles);  // every row: nothing left unless a chunk was cut short
+      if (e == cudaSuccess) e = cudaStreamSynchronize(s->copy_stream);
+    }
     if (e == cudaSuccess && A_elem && N > 0) e = cudaMemcpyAsync(A_elem, area_res, sizeof(double) * N, cudaMemcpyDeviceToHost, s->stream);
     if (e == cudaSuccess && F_group && m->G > 0 && N > 0)
       e = cudaMemcpyAsync(F_group, m->Fgroup.ptr, sizeof(double) * m->G * m->G, cudaMemcpyDeviceToHost, s->stream);
@@ -466,7 +538,7 @@ int rvf_solve(rvf_session* s, rvf_mesh* m, const rvf_options* o, double* F_elem,
     if (e == cudaSuccess && row_sums && N > 0)
       e = cudaMemcpyAsync(row_sums, m->rowsum.ptr, sizeof(double) * N, cudaMemcpyDeviceToHost, s->stream);
     if (e == cudaSuccess && o->ray_log)
-      e = cudaMemcpyAsync(o->ray_log, log.ptr, log.bytes, cudaMemcpyDeviceToHost, s->stream);
+      e = cudaMemcpyAsync(o->ray_log, log.ptr, log_bytes, cudaMemcpyDeviceToHost, s->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
     if (e != cudaSuccess) return cuda_err(e, "device->host copy");
     S.ms_download = t.stop();

@@ -1,0 +1,36 @@
+"""Host F downloaded column by column while later chunks compute: a session
+with a small HBM budget runs the pair pipeline in many chunks, so the
+finished columns of each chunk's tile rows go to the host early.  Every
+column must arrive, bit for bit the result of a one-chunk solve, into pinned
+(overlapped copies) and pageable (synchronous copies) host memory."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("pinned", [True, False])
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_chunked_solve_downloads_every_column(rvf, session, pinned, precision):
+    from rvf_b200 import _abi
+    md = rvf.meshes.cube_enclosure(16, box_m=6)
+    N = md.n_elems
+    o = rvf.make_options(3, seed=0, precision=precision)
+    ref = np.empty((N, N), order="F")
+    dm = _abi.DeviceMesh(session, rvf.mesh_desc_arrays(md, [7]))
+    st_ref = dm.solve(o, ref)
+    dm.release()
+    small = _abi.Session(0, hbm_budget_bytes=256 << 20)
+    buf = _abi.PinnedArray((N, N), order="F") if pinned else None
+    try:
+        F = buf.array if pinned else np.empty((N, N), order="F")
+        F.fill(-7.0)  # a column never written keeps this
+        dm = _abi.DeviceMesh(small, rvf.mesh_desc_arrays(md, [7]))
+        st = dm.solve(o, F)
+        dm.release()
+        assert st.n_chunks > 4 * st_ref.n_chunks, (st.n_chunks, st_ref.n_chunks)
+        assert np.array_equal(F, ref, equal_nan=True)
+    finally:
+        if buf is not None:
+            buf.free()
+        small.close()
