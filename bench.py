@@ -615,7 +615,7 @@ def main():
                          "c3: cylinder with Duffy pairs; c4: 2-D Monte Carlo cavity; medium / small: the headline "
                          "shape at m = 24 / 12")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--e2e-warmup", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ref-seconds", type=float, default=15.0)
