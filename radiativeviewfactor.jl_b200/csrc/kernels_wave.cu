@@ -897,21 +897,33 @@ __device__ __forceinline__ int trace_list(const int32_t* e, int n, const Src& no
                                           const int32_t* leaf_of, const Pol& pol, TravCount& cnt) {
   int last = -1, s = kMiss;
   bool unsure = false;
+  // software-pipelined: the triangle of entry k and the index and leaf of
+  // entry k+1 are loaded before entry k's box test, so the loads of one
+  // entry overlap the tests of the previous one
+  int u = n > 0 ? e[0] : 0;
+  int lf = n > 0 ? leaf_of[u] : 0;
   for (int k = 0; k < n; ++k) {
-    const int u = e[k];
-    const int lf = leaf_of[u];
+    const Tri t = tris[u];
+    int un = 0, lfn = 0;
+    if (k + 1 < n) {
+      un = e[k + 1];
+      lfn = leaf_of[un];
+    }
     if (lf != last) {
       last = lf;
       s = pol.node(nodes(lf));
       ++cnt.nodes;
       if (s == kUnsure) ++cnt.unsure_slab;
     }
-    if (s == kMiss) continue;
-    ++cnt.prims;
-    const int m = pol.prim_direct(tris[u]);
-    if (m == kUnsure) ++cnt.unsure_prim;
-    if (m == kHit && s == kHit) return kHit;
-    if (m != kMiss) unsure = true;
+    if (s != kMiss) {
+      ++cnt.prims;
+      const int m = pol.prim_direct(t);
+      if (m == kUnsure) ++cnt.unsure_prim;
+      if (m == kHit && s == kHit) return kHit;
+      if (m != kMiss) unsure = true;
+    }
+    u = un;
+    lf = lfn;
   }
   return unsure ? kUnsure : kMiss;
 }
