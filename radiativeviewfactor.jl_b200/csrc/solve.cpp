@@ -2,6 +2,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <functional>
 #include <cstring>
 #include <memory>
 #include <mutex>
@@ -462,10 +463,19 @@ int rvf_solve(rvf_session* s, rvf_mesh* m, const rvf_options* o, double* F_elem,
     }
     EvTimer t(s->stream);
     WaveReq* one = &w;
+    // the columns finished by earlier chunks are queued for download while
+    // the next chunk runs
+    cudaError_t dl_err = cudaSuccess;
+    int64_t dl_upto = 0;
+    const std::function<void()> queue_columns = [&]() {
+      if (dl.host && dl_err == cudaSuccess) dl_err = dl.advance(dl_upto);
+    };
     while (!w.done()) {  // chunks: each claims tiles while the ray queues have room
       ChunkInfo ci;
       const int64_t before = w.claimed;
-      if ((rc = wave_chunk(s, &one, 1, false, &ci))) return rc;
+      dl_upto = before;
+      if ((rc = wave_chunk(s, &one, 1, false, &ci, 0, 0, 0.0, &queue_columns))) return rc;
+      if (dl_err != cudaSuccess) return cuda_err(dl_err, "F column download");
       if ((rc = read_err(s))) return rc;
       n_kernels += ci.kernels;
       S.n_chunks += 1;
@@ -476,7 +486,6 @@ int rvf_solve(rvf_session* s, rvf_mesh* m, const rvf_options* o, double* F_elem,
       S.ms_lists += ci.ms_lists;
       S.n_rays_traced += ci.rays_traced;
       if (w.claimed == before) return set_err(RVF_ENOMEM, "pair pipeline made no progress: ray queue too small for one tile");
-      if (dl.host && (e = dl.advance(w.claimed)) != cudaSuccess) return cuda_err(e, "F column download");
     }
     w_tiles = w.claimed;
     S.ms_pairs = t.stop();

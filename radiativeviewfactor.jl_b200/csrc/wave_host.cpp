@@ -232,7 +232,7 @@ cudaError_t enqueue_chunk(Session* s, const WaveShape& sh, bool events) {
 }  // namespace
 
 int wave_chunk(Session* s, WaveReq* const* reqs_in, int n_in, bool use_graph, ChunkInfo* info, int gen_bps,
-               int trace_bps, double pp_budget) {
+               int trace_bps, double pp_budget, const std::function<void()>* on_launched) {
   if (n_in < 1 || n_in > kMaxBatch) return set_err(RVF_EINVAL, "batch of %d requests (1..%d)", n_in, kMaxBatch);
   int rc = 0;
   if ((rc = ensure_blocks(s))) return rc;
@@ -331,6 +331,7 @@ int wave_chunk(Session* s, WaveReq* const* reqs_in, int n_in, bool use_graph, Ch
     }
   }
   if (!replayed && (e = enqueue_chunk(s, sh, info != nullptr)) != cudaSuccess) return cuda_err(e, "pair pipeline launch");
+  if (on_launched) (*on_launched)();
   if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return cuda_err(e, "pair pipeline");
   if (info) {
     *info = ChunkInfo{};

@@ -1,6 +1,8 @@
 // wave_host.h -- host side of the wavefront pair pipeline (wave_host.cpp).
 #pragma once
 
+#include <functional>
+
 #include "kernels.h"
 #include "rvf_internal.h"
 
@@ -42,7 +44,9 @@ WaveShape wave_shape(Session* s, WaveReq* const* reqs, int n);
 // gen_bps / trace_bps: blocks per SM of the two grids (0 = occupancy limit);
 // pp_budget > 0 caps the point pairs (worst case 32 x 32 x pmax^2 per tile)
 // offered to the launch, given to the requests in order.
+// on_launched (optional) runs on the host once the chunk's work is queued and
+// before the host waits for it: host work that overlaps the chunk.
 int wave_chunk(Session* s, WaveReq* const* reqs, int n, bool use_graph, ChunkInfo* info, int gen_bps = 0,
-               int trace_bps = 0, double pp_budget = 0.0);
+               int trace_bps = 0, double pp_budget = 0.0, const std::function<void()>* on_launched = nullptr);
 
 }  // namespace rvf
