@@ -95,7 +95,7 @@ __device__ __forceinline__ void rotate_to_edge(double u, double v, int e, double
 
 }  // namespace
 
-__global__ void __launch_bounds__(256) k_duffy(DuffyArgs a) {
+__global__ void __launch_bounds__(256, 2) k_duffy(DuffyArgs a) {
   const int64_t pi = blockIdx.x;
   const DuffyPair P = a.pairs[pi];
   const int nq = a.nq;
