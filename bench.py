@@ -352,6 +352,7 @@ def phases(stats):
 SERVE_SIZES = {
     # requests, element count range (log-uniform), admission budget
     "small": (32, 2000, 8000, 150 << 30),
+    "medium": (128, 2000, 20000, 150 << 30),
     "full": (512, 2000, 40000, 150 << 30),
 }
 
@@ -398,10 +399,24 @@ def serve_requests(rvf, n_req, n_lo, n_hi, seed=5):
     return out
 
 
+def serve_work(r) -> int:
+    """Work of one request for the service-time estimate: quadrature point
+    pairs (points per element from the family and nquad: nquad^2 on quads,
+    the 1/3/7/13-point triangle rules), or sample pairs for Monte Carlo."""
+    N = r["N"]
+    P = N * (N - 1) // 2
+    if r["mc"]:
+        return P * 64
+    nq = r["nquad"]
+    pts = nq * nq if r["family"] in ("quad4", "quad") else (1 if nq <= 1 else 3 if nq == 2 else 7 if nq == 3 else 13)
+    return P * pts * pts
+
+
 def run_serve(rvf, sess, size: str, local: int):
     """p50/p99 latency and throughput of a Poisson request stream through the
-    serving loop, at ~80% of the measured one-at-a-time capacity; a sample of
-    the results is compared with plain FP64 one-at-a-time solves."""
+    serving loop, offered at 80% of the estimated one-at-a-time service time;
+    a sample of the results is compared with plain FP64 one-at-a-time solves."""
+    import queue
     import threading
     import numpy as np
     from rvf_b200 import _abi
@@ -409,29 +424,65 @@ def run_serve(rvf, sess, size: str, local: int):
     reqs = serve_requests(rvf, n_req, n_lo, n_hi)
     arrays = [rvf.mesh_desc_arrays(r["md"], r["obs"]) for r in reqs]
     pairs = [r["N"] * (r["N"] - 1) // 2 for r in reqs]
-    # one-at-a-time capacity on a sample, same options (mixed) and plain FP64
-    sample = list(range(0, n_req, max(1, n_req // 8)))[:8]
+    # one-at-a-time solves (the request's own options, then plain FP64) on a
+    # sample of both kinds: six quadrature requests and two Monte Carlo ones,
+    # evenly spread over the stream
+    quad = [k for k in range(n_req) if not reqs[k]["mc"]]
+    mc = [k for k in range(n_req) if reqs[k]["mc"]]
+    sample = quad[::max(1, len(quad) // 6)][:6] + mc[::max(1, len(mc) // 2)][:2]
+    # the served results of these are compared with plain FP64 solves
+    check = [k for k in sample if not reqs[k]["mc"]][:4]
+    F64 = {}
     t_mixed, t_fp64, dF = 0.0, 0.0, 0.0
+    t_kind = {False: 0.0, True: 0.0}
     for k in sample:
         r = reqs[k]
-        N, G = r["N"], max(1, len(r["md"].group_tags))
         dm = _abi.DeviceMesh(sess, arrays[k])
         dm.solve(r["opts"])  # warm (tables, queues)
         t0 = time.perf_counter()
         dm.solve(r["opts"])
-        t_mixed += time.perf_counter() - t0
+        dt = time.perf_counter() - t0
+        t_mixed += dt
+        t_kind[r["mc"]] += dt
         o64 = rvf.make_options(r["nquad"], monte_carlo=r["mc"], n_samples=64, seed=r["opts"].seed, precision="fp64")
         t0 = time.perf_counter()
         dm.solve(o64)
         t_fp64 += time.perf_counter() - t0
+        if k in check:
+            F64[k] = np.empty((r["N"], r["N"]), order="F")
+            dm.solve(rvf.make_options(r["nquad"], seed=0, precision="fp64"), F64[k])
         dm.release()
-    mean_service = t_mixed / len(sample)
+    # Offered load.  Each request's cost is its work (quadrature point pairs,
+    # or Monte Carlo sample pairs) weighted by the one-at-a-time time per unit
+    # of its kind on the sample.  The server's capacity in that cost is
+    # measured on a burst: the stream's first 32 requests submitted at once
+    # to a server of their own, each released when done.  The arrival rate
+    # puts the stream at 80% of that capacity.
+    work = [serve_work(r) for r in reqs]
+    sec_per_unit = {}
+    for kind in (False, True):
+        units = sum(work[k] for k in sample if reqs[k]["mc"] == kind)
+        sec_per_unit[kind] = t_kind[kind] / units if units else 0.0
+    if not sec_per_unit[True]:
+        sec_per_unit[True] = sec_per_unit[False]
+    cost = [work[k] * sec_per_unit[reqs[k]["mc"]] for k in range(n_req)]
+    burst = list(range(min(n_req, 32)))
+    sv = _abi.Server(sess, admit_bytes=admit)
+    t0 = time.perf_counter()
+    rids = [sv.submit(arrays[k], reqs[k]["opts"]) for k in burst]
+    for rid in rids:
+        sv.wait(rid, 3_600_000)
+        sv.release(rid)
+    t_burst = time.perf_counter() - t0
+    sv.close()
+    est_service = sum(cost) * t_burst / sum(cost[k] for k in burst)
+    mean_service = est_service / n_req
     sample_pairs = sum(pairs[k] for k in sample)
     lam = 0.8 / mean_service
     rng = np.random.default_rng(7)
     arrivals = np.cumsum(rng.exponential(1.0 / lam, size=n_req))
     sv = _abi.Server(sess, admit_bytes=admit)
-    ids = [None] * n_req
+    submitted = queue.Queue()
     err = []
 
     def submitter():
@@ -440,34 +491,32 @@ def run_serve(rvf, sess, size: str, local: int):
             dt = arrivals[k] - (time.perf_counter() - t0)
             if dt > 0:
                 time.sleep(dt)
-            ids[k] = sv.submit(arrays[k], reqs[k]["opts"])
+            submitted.put((k, sv.submit(arrays[k], reqs[k]["opts"])))
 
     th = threading.Thread(target=submitter)
     t_start = time.perf_counter()
     th.start()
-    th.join()
-    for k in range(n_req):
+    # The client reads each result (the checked ones) and releases it as soon
+    # as it is done: a finished request keeps its device memory and its
+    # admission charge until rvf_release, so releasing only at the end would
+    # stall the stream once finished results fill the admission budget.
+    for _ in range(n_req):
+        k, rid = submitted.get()
         try:
-            sv.wait(ids[k], 3_600_000)
+            sv.wait(rid, 3_600_000)
+            if k in F64:
+                F = sv.result(rid)[0]
+                dF = max(dF, float(np.nanmax(np.abs(F - F64.pop(k)))))
+                del F
         except _abi.RVFError as e:
             err.append(str(e))
-    wall = time.perf_counter() - t_start
-    # a sample of the results against plain FP64 one-at-a-time solves
-    check = [k for k in sample if not reqs[k]["mc"]][:4]
-    for k in check:
-        N = reqs[k]["N"]
-        F = sv.result(ids[k])[0]
-        dm = _abi.DeviceMesh(sess, arrays[k])
-        F64 = np.empty((N, N), order="F")
-        dm.solve(rvf.make_options(reqs[k]["nquad"], seed=0, precision="fp64"), F64)
-        dm.release()
-        dF = max(dF, float(np.nanmax(np.abs(F - F64))))
-    st = sv.stats()
-    for k in range(n_req):
         try:
-            sv.release(ids[k])
+            sv.release(rid)
         except _abi.RVFError:
             pass
+    wall = time.perf_counter() - t_start
+    th.join()
+    st = sv.stats()
     sv.close()
     total_pairs = sum(pairs)
     return {
@@ -476,7 +525,8 @@ def run_serve(rvf, sess, size: str, local: int):
         "throughput_pairs_per_s": total_pairs / wall, "wall_s": wall,
         "one_at_a_time_mixed_pairs_per_s": sample_pairs / t_mixed,
         "one_at_a_time_fp64_pairs_per_s": sample_pairs / t_fp64,
-        "lambda_per_s": lam, "offered_load": 0.8,
+        "lambda_per_s": lam, "offered_load": 0.8, "estimated_service_s": est_service,
+        "burst_s": t_burst, "burst_requests": len(burst),
         "max_abs_dF_vs_fp64_solo": dF, "checked_requests": len(check),
         "chunks": st["chunks"], "batched_requests": st["batched_requests"], "graph_replays": st["graph_replays"],
         "admit_bytes": admit, "admitted_bytes_peak": st["admitted_bytes_peak"],
@@ -619,8 +669,9 @@ def main():
     ap.add_argument("--e2e-warmup", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ref-seconds", type=float, default=15.0)
-    ap.add_argument("--serve", choices=["none", "small", "full"], default="small",
-                    help="serving stream reported beside the main line (small: 32 requests, 2k-8k elements)")
+    ap.add_argument("--serve", choices=["none", "small", "medium", "full"], default="small",
+                    help="serving stream reported beside the main line (small: 32 requests, 2k-8k elements; "
+                         "medium: 128, 2k-20k; full: 512, 2k-40k)")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
