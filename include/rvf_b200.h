@@ -109,7 +109,9 @@ typedef struct {
   uint8_t* ray_log;           /* debug: host buffer of n_elems^2 * ray_log_pm^2 bytes, or NULL */
   int32_t ray_log_pm;         /* stride of the ray log (>= points per element) */
   int32_t disable_pair_lists; /* 3-D occlusion: 1 = every ray walks the tree (same results; for testing) */
-  int32_t reserved[7];
+  int32_t self_vf;            /* 1: also integrate the pairs (i, i) -- concave elements see themselves
+                                 (src/Assembly.jl:173,193, j_start = self_vf ? i : i + 1); quadrature only */
+  int32_t reserved[6];
 } rvf_options;
 
 typedef struct {

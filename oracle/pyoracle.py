@@ -52,6 +52,7 @@ _SIG = {
     "orc_is_visible_cpu": (C.c_int, [_p, _pd, _pd, C.c_int]),
     "orc_solve_plain": (C.c_int, [C.POINTER(OrcMesh), C.c_int, C.c_int, C.c_int64, C.c_int64, C.c_int64, C.c_int,
                                   _pd, _pd, _pu8, C.c_int32, _pi64]),
+    "orc_self_gpu": (C.c_int, [C.POINTER(OrcMesh), C.c_int, C.c_int, _pd, _pd]),
     "orc_solve_mc": (C.c_int, [C.POINTER(OrcMesh), C.c_int, C.c_uint64, C.c_int, C.c_int, C.c_int64, C.c_int64,
                                C.c_int64, C.c_int, _pd, _pd, _pu8, _pi64]),
     "orc_singularity_type": (C.c_int, [C.POINTER(OrcMesh), C.c_int64, C.c_int64, _pi32, _pi32]),
@@ -230,6 +231,14 @@ def solve_plain(mesh: Mesh, nquad, geometric=False, row_begin=0, row_end=None, r
                           row_stride, threads, _d(raw), _d(area),
                           None if log is None else log.ctypes.data_as(_pu8), pm, cnt.ctypes.data_as(_pi64))
     return raw, area, log, cnt
+
+
+def self_gpu(mesh: Mesh, nquad, geometric=False):
+    """raw[i,i] and areas of the self pairs with the GPU path's arithmetic."""
+    raw = np.zeros(mesh.N)
+    area = np.zeros(mesh.N)
+    lib().orc_self_gpu(mesh.ref(), nquad, int(geometric), _d(raw), _d(area))
+    return raw, area
 
 
 def solve_mc(mesh: Mesh, n_samples, seed, exclude_groups=False, geometric=False, row_begin=0, row_end=None,

@@ -818,6 +818,43 @@ int orc_solve_plain(const orc_mesh* m, int nquad, int geometric, int64_t row_beg
   return 0;
 }
 
+// The diagonal of src/GPUKernels.jl:226-323 (i = j), for self_vf
+// (src/Assembly.jl:173,193).
+int orc_self_gpu(const orc_mesh* m, int nquad, int geometric, double* raw_diag, double* area) {
+  const int64_t N = m->n_elems;
+  Rules R = make_rules(nquad);
+  orc_bvh* bvh = (m->n_obs > 0) ? orc_bvh_build(m->obs_soup, m->obs_nv, m->n_obs) : nullptr;
+  const bool two_d = (m->mesh_dim == 1);
+  for (int64_t e = 0; e < N; ++e) {
+    Pts P;
+    element_points(m, e, R, P);
+    double A = 0.0;
+    for (int p = 0; p < P.np; ++p) A += P.w[p] * P.dA[p];
+    area[e] = A;
+    const int32_t g = m->elem_group[e];
+    double Fii = 0.0;
+    for (int p = 0; p < P.np; ++p) {
+      double inner = 0.0;
+      for (int q = 0; q < P.np; ++q) {
+        double K;
+        if (two_d) {
+          K = vf_kernel_2d(P.x[p], P.n[p], P.x[q], P.n[q]);
+          if (K > 0.0 && bvh && orc_intersect_seg(bvh, m->obs_group, P.x[p], P.x[q], g, g)) K = 0.0;
+        } else {
+          K = vf_kernel(P.x[p], P.n[p], P.x[q], P.n[q]);
+          if (bvh && K > 0.0 && ray_blocked_gpu(bvh, m->obs_group, P.x[p], P.x[q], g, g, geometric, nullptr))
+            K = 0.0;
+        }
+        inner += (P.w[q] * K) * P.dA[q];
+      }
+      Fii += (P.w[p] * inner) * P.dA[p];
+    }
+    raw_diag[e] = Fii;
+  }
+  orc_bvh_free(bvh);
+  return 0;
+}
+
 }  // extern "C"
 
 namespace {

@@ -103,6 +103,13 @@ int orc_solve_plain(const orc_mesh* m, int nquad, int geometric,
                     int64_t row_begin, int64_t row_end, int64_t row_stride, int n_threads,
                     double* raw, double* area, uint8_t* ray_log, int32_t pm, int64_t* counters);
 
+/* Self pairs (i, i), which the reference integrates on its CPU path only
+ * (self_vf, src/Assembly.jl:173,193), with the GPU path's arithmetic of
+ * orc_solve_plain: the same points, kernel, summation order and shadow rays
+ * (one tree, the element's own group skipped, t_eps; geometric as there).
+ * raw_diag[i] = raw[i,i]; area[i] = sum_p w_p dA_p for every element. */
+int orc_self_gpu(const orc_mesh* m, int nquad, int geometric, double* raw_diag, double* area);
+
 /* GPU Monte Carlo, src/GPUMCKernels.jl:146-281.  area rule: A_i from the
  * stream of pair (i,i+1) in the i-role, A_N from pair (N-1,N) in the j-role.
  * Curve meshes (mesh_dim=1) use the 2-D extension documented in the header of

@@ -47,7 +47,7 @@ class Options(C.Structure):
                 ("seed", C.c_uint64), ("precision", C.c_int32), ("occlusion", C.c_int32),
                 ("geometric_soup", C.c_int32), ("mc_exclude_groups", C.c_int32), ("near_field_factor", C.c_double),
                 ("ray_log", _pu8), ("ray_log_pm", C.c_int32), ("disable_pair_lists", C.c_int32),
-                ("reserved", C.c_int32 * 7)]
+                ("self_vf", C.c_int32), ("reserved", C.c_int32 * 6)]
 
 
 class Stats(C.Structure):

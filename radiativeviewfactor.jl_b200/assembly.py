@@ -54,8 +54,9 @@ def _gpu_float_type(backend):
 
 
 def _gpu_supports(backend, feature: str) -> bool:
-    """Capabilities beyond the reference's GPU path: Duffy pairs and curve meshes."""
-    return isinstance(backend, B200Backend) and feature in ("duffy", "curves")
+    """Capabilities beyond the reference's GPU path: Duffy pairs, curve meshes
+    and self view factors (quadrature)."""
+    return isinstance(backend, B200Backend) and feature in ("duffy", "curves", "self_vf")
 
 
 _GPU_HOOK_REF = [None]
@@ -85,6 +86,9 @@ def compute_view_factors(mesh: MeshData, *, nquad: int = 4, obstruction_groups: 
     rand(UInt64)), precision ("fp64" | "mixed"), geometric_soup (read soup
     triangles by their true vertices instead of the reference's read),
     mc_exclude_groups (skip source/destination groups in MC occlusion).
+    self_vf, CPU-only in the reference (its GPU hook never receives it), is
+    computed on the device for quadrature solves (plain and Duffy) and, as
+    the reference's GPU path does, left out for Monte Carlo (with a warning).
     """
     if backend is None:
         backend = B200Backend()
@@ -96,14 +100,19 @@ def compute_view_factors(mesh: MeshData, *, nquad: int = 4, obstruction_groups: 
     if use_duffy and monte_carlo:
         raise ValueError("use_duffy and monte_carlo cannot both be true.")
     if not isinstance(backend, CPU):
+        if self_vf and (monte_carlo or not _gpu_supports(backend, "self_vf")):
+            if monte_carlo and _gpu_supports(backend, "self_vf"):
+                warnings.warn("self_vf with monte_carlo is CPU-only; ignored for GPU backends.")
+            self_vf = False
         if mesh.mesh_dim == 1 and not _gpu_supports(backend, "curves"):
             raise ValueError("GPU backend does not support curve meshes (mesh_dim=1). "
                              "Use the CPU backend for 2D per-unit-depth view factors.")
         ArrayT = _gpu_array_type(backend)
         FloatT = _gpu_float_type(backend)
+        extra = {"self_vf": True} if self_vf else {}
         return _gpu_compute_hook(mesh, nquad, backend, FloatT, ArrayT, list(obstruction_groups), verbose,
                                  monte_carlo, n_samples, use_duffy=use_duffy, seed=seed, precision=precision,
-                                 geometric_soup=geometric_soup, mc_exclude_groups=mc_exclude_groups)
+                                 geometric_soup=geometric_soup, mc_exclude_groups=mc_exclude_groups, **extra)
     raise NotImplementedError("The CPU path is the reference's own Julia implementation; this package "
                               "provides the B200 backend only.")
 
@@ -128,7 +137,7 @@ def mesh_desc_arrays(mesh: MeshData, obstruction_groups: Sequence[int]):
 
 
 def make_options(nquad=4, monte_carlo=False, n_samples=10000, use_duffy=False, seed=None, precision="fp64",
-                 occlusion=True, geometric_soup=False, mc_exclude_groups=False) -> _abi.Options:
+                 occlusion=True, geometric_soup=False, mc_exclude_groups=False, self_vf=False) -> _abi.Options:
     o = _abi.default_options()
     o.nquad = int(nquad)
     o.method = _abi.METHOD_MONTE_CARLO if monte_carlo else _abi.METHOD_QUADRATURE
@@ -143,13 +152,14 @@ def make_options(nquad=4, monte_carlo=False, n_samples=10000, use_duffy=False, s
     o.occlusion = int(bool(occlusion))
     o.geometric_soup = int(bool(geometric_soup))
     o.mc_exclude_groups = int(bool(mc_exclude_groups))
+    o.self_vf = int(bool(self_vf))
     return o
 
 
 def compute_view_factors_b200(mesh: MeshData, nquad: int, backend: B200Backend, FloatT, ArrayT, *,
                               obstruction_groups=(), verbose=True, monte_carlo=False, n_samples=10000,
                               use_duffy=False, seed=None, precision="fp64", geometric_soup=False,
-                              mc_exclude_groups=False) -> ViewFactorResult:
+                              mc_exclude_groups=False, self_vf=False) -> ViewFactorResult:
     """The hook target: compute_view_factors_gpu (src/GPUAssembly.jl:32-105) on the B200 library."""
     N = mesh.n_elems
     if verbose:
@@ -170,7 +180,7 @@ def compute_view_factors_b200(mesh: MeshData, nquad: int, backend: B200Backend, 
         Ag = np.empty(G, dtype=np.float64)
         rs = np.empty(N, dtype=np.float64)
         o = make_options(nquad, monte_carlo, n_samples, use_duffy, seed, precision, True, geometric_soup,
-                         mc_exclude_groups)
+                         mc_exclude_groups, self_vf)
         st = dm.solve(o, F, A, Fg if G else None, Ag if G else None, rs if N else None)
     finally:
         dm.release()

@@ -305,6 +305,10 @@ struct DuffyArgs {
 
 cudaError_t launch_duffy(const DuffyArgs& a, cudaStream_t st);
 
+// Self view factors: F[i,i] for every element, one warp per element, with the
+// FP64 pair arguments of the solve (kernels_self.cu).
+cudaError_t launch_self(const PairArgs& a, cudaStream_t st);
+
 struct McArgs {
   int64_t N, nT, n_tiles;
   int64_t tile0, tile_count;  // this launch integrates tiles [tile0, tile0 + tile_count)

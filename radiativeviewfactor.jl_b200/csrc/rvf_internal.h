@@ -116,7 +116,8 @@ struct rvf_mesh {
   std::map<int, std::unique_ptr<rvf::Tables>> tables;
   // Quad8 pairs sharing corners (built on the first use_duffy solve)
   bool duffy_built = false;
-  int64_t n_duffy = 0;
+  int64_t n_duffy = 0;       // pairs (i, j), i < j, sharing corners
+  int64_t n_duffy_self = 0;  // the Quad8 pairs (i, i) of self_vf solves, after them in duffy_pairs
   rvf::DevBuf duffy_pairs;
   std::map<int, std::unique_ptr<rvf::DevBuf>> duffy_rules;  // nquad -> [p01 | w01]
   // results of the last solve
@@ -132,6 +133,9 @@ int ensure_tables(Session* s, rvf_mesh* m, int nquad, Tables** out);
 int read_err(Session* s);
 int validate_options(const rvf_mesh* m, const rvf_options* o);
 int run_reduce(Session* s, rvf_mesh* m, const double* area);
+// The self pairs (i, i) of a quadrature solve with the pipeline's FP64
+// arguments, counted in the session's counters.
+cudaError_t launch_self_pairs(Session* s, const PairArgs& pa, cudaStream_t st);
 int ensure_duffy(Session* s, rvf_mesh* m, int nquad, const double** p01, const double** w01);
 void fill_mc_args(Session* s, rvf_mesh* m, const rvf_options* o, uint8_t* ray_log, McArgs& c);
 }  // namespace rvf

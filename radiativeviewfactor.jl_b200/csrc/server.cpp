@@ -226,21 +226,23 @@ int admit_one(rvf_server* sv, Req* r) {
   return e == cudaSuccess ? RVF_OK : cuda_err(e, "request set-up");
 }
 
-// Duffy pairs, the one-element case and the reductions of a request whose
-// tiles are all integrated (s->mu held) -- the tail of rvf_solve.
+// Self pairs, Duffy pairs, the one-element case and the reductions of a
+// request whose tiles are all integrated (s->mu held) -- the tail of rvf_solve.
 int finish_quad(Session* s, Req* r) {
   rvf_mesh* m = r->m;
   const rvf_options& o = r->opts;
   const int64_t N = m->N;
   int rc = 0;
   cudaError_t e = cudaSuccess;
+  if (o.self_vf && N > 0 && (e = launch_self_pairs(s, r->w.pa, s->stream)) != cudaSuccess)
+    return cuda_err(e, "self-pair kernel launch");
   if (o.use_duffy && m->dim == 2 && N > 0) {
     DuffyArgs d{};
     if ((rc = ensure_duffy(s, m, o.nquad, &d.p01, &d.w01))) return rc;
     d.N = N;
     d.nq = o.nquad;
     d.pairs = m->duffy_pairs.as<DuffyPair>();
-    d.n_pairs = m->n_duffy;
+    d.n_pairs = m->n_duffy + (o.self_vf ? m->n_duffy_self : 0);
     d.coords = m->coords.as<double>();
     d.enodes = m->enodes.as<int32_t>();
     d.area_orig = r->T->area_orig.as<double>();

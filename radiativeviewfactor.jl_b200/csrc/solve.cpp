@@ -63,6 +63,9 @@ int validate_options(const rvf_mesh* m, const rvf_options* o) {
   if (o->method == RVF_METHOD_MONTE_CARLO && o->n_samples < 1)
     return set_err(RVF_EINVAL, "n_samples must be >= 1");
   if (o->ray_log && o->ray_log_pm < 1) return set_err(RVF_EINVAL, "ray_log needs ray_log_pm >= 1");
+  if (o->self_vf != 0 && o->self_vf != 1) return set_err(RVF_EINVAL, "self_vf must be 0 or 1, got %d", o->self_vf);
+  if (o->self_vf && o->method == RVF_METHOD_MONTE_CARLO)
+    return set_err(RVF_EINVAL, "self_vf is supported with quadrature only");
   (void)m;
   return RVF_OK;
 }
@@ -97,6 +100,12 @@ void fill_mc_args(Session* s, rvf_mesh* m, const rvf_options* o, uint8_t* ray_lo
   c.tile_counter = s->tile_counter.as<unsigned long long>();
   c.counters = s->counters.as<unsigned long long>();
   c.ray_log = ray_log;
+}
+
+cudaError_t launch_self_pairs(Session* s, const PairArgs& pa, cudaStream_t st) {
+  PairArgs a = pa;
+  a.counters = s->counters.as<unsigned long long>();
+  return launch_self(a, st);
 }
 
 int run_reduce(Session* s, rvf_mesh* m, const double* area) {
@@ -152,6 +161,28 @@ int ensure_duffy(Session* s, rvf_mesh* m, int nquad, const double** p01, const d
       return 1;
     };
     std::vector<DuffyPair> pairs;
+    // singularity_type (src/DuffyKernel.jl:95-115): corners equal by node
+    // index, in the reference's loop order (corner of i outer, of j inner)
+    auto classify = [&](int64_t i, int32_t j) {
+      const int32_t* a = &m->h_enodes[(size_t)i * 8];
+      const int32_t* b = &m->h_enodes[(size_t)j * 8];
+      int n = 0, ci[2] = {0, 0}, cj[2] = {0, 0};
+      for (int x = 0; x < 4; ++x)
+        for (int y = 0; y < 4; ++y)
+          if (a[x] == b[y]) {
+            if (n < 2) { ci[n] = x + 1; cj[n] = y + 1; }
+            ++n;
+          }
+      if (n == 0) return;
+      DuffyPair P{};
+      P.i = (int32_t)i; P.j = j; P.ii = inv[i]; P.jj = inv[j];
+      P.stype = n == 1 ? 1 : 2;
+      P.ci0 = ci[0]; P.cj0 = cj[0];
+      P.edge_i = n >= 2 ? corners_to_edge(ci[0], ci[1]) : 1;
+      P.edge_j = n >= 2 ? corners_to_edge(cj[0], cj[1]) : 1;
+      P.gi = m->h_group[i]; P.gj = m->h_group[j];
+      pairs.push_back(P);
+    };
     for (int64_t i = 0; i < N; ++i) {
       if (m->h_fam[i] != 0) continue;
       std::vector<int32_t> cand;
@@ -160,30 +191,18 @@ int ensure_duffy(Session* s, rvf_mesh* m, int nquad, const double** p01, const d
           if (j > i) cand.push_back(j);
       std::sort(cand.begin(), cand.end());
       cand.erase(std::unique(cand.begin(), cand.end()), cand.end());
-      const int32_t* a = &m->h_enodes[(size_t)i * 8];
-      for (int32_t j : cand) {
-        const int32_t* b = &m->h_enodes[(size_t)j * 8];
-        int n = 0, ci[2] = {0, 0}, cj[2] = {0, 0};
-        for (int x = 0; x < 4; ++x)
-          for (int y = 0; y < 4; ++y)
-            if (a[x] == b[y]) {
-              if (n < 2) { ci[n] = x + 1; cj[n] = y + 1; }
-              ++n;
-            }
-        if (n == 0) continue;
-        DuffyPair P{};
-        P.i = (int32_t)i; P.j = j; P.ii = inv[i]; P.jj = inv[j];
-        P.stype = n == 1 ? 1 : 2;
-        P.ci0 = ci[0]; P.cj0 = cj[0];
-        P.edge_i = n >= 2 ? corners_to_edge(ci[0], ci[1]) : 1;
-        P.edge_j = n >= 2 ? corners_to_edge(cj[0], cj[1]) : 1;
-        P.gi = m->h_group[i]; P.gj = m->h_group[j];
-        pairs.push_back(P);
-      }
+      for (int32_t j : cand) classify(i, j);
     }
+    const size_t n_regular = pairs.size();
+    // then the self pairs (i, i) of self_vf solves: an element shares every
+    // corner with itself, so the reference treats it as a common-edge pair on
+    // the first two matches, (1, 1) and (2, 2)
+    for (int64_t i = 0; i < N; ++i)
+      if (m->h_fam[i] == 0) classify(i, (int32_t)i);
     int rc;
     if (!pairs.empty() && (rc = upload(s, m->duffy_pairs, pairs.data(), sizeof(DuffyPair) * pairs.size()))) return rc;
-    m->n_duffy = (int64_t)pairs.size();
+    m->n_duffy = (int64_t)n_regular;
+    m->n_duffy_self = (int64_t)(pairs.size() - n_regular);
     m->duffy_built = true;
   }
   auto it = m->duffy_rules.find(nquad);
@@ -453,8 +472,8 @@ int rvf_solve(rvf_session* s, rvf_mesh* m, const rvf_options* o, double* F_elem,
     cudaError_t e = cudaSuccess;
     WaveReq w;
     if ((rc = wave_prepare(s, m, T, o, o->ray_log ? log.as<uint8_t>() : nullptr, w, &n_kernels))) return rc;
-    // Duffy pairs overwrite F after the pipeline: no early columns then
-    if (F_elem && N > 1 && !(o->use_duffy && m->dim == 2)) {
+    // Duffy and self pairs overwrite F after the pipeline: no early columns then
+    if (F_elem && N > 1 && !(o->use_duffy && m->dim == 2) && !o->self_vf) {
       dl.s = s;
       dl.m = m;
       dl.host = F_elem;
@@ -488,6 +507,10 @@ int rvf_solve(rvf_session* s, rvf_mesh* m, const rvf_options* o, double* F_elem,
       if (w.claimed == before) return set_err(RVF_ENOMEM, "pair pipeline made no progress: ray queue too small for one tile");
     }
     w_tiles = w.claimed;
+    if (o->self_vf) {  // the pairs (i, i), before Duffy (which replaces the Quad8 ones)
+      if ((e = launch_self_pairs(s, w.pa, s->stream)) != cudaSuccess) return cuda_err(e, "self-pair kernel launch");
+      n_kernels += 1;
+    }
     S.ms_pairs = t.stop();
     if ((rc = read_err(s))) return rc;
     // Duffy integrals overwrite the singular Quad8 pairs (Duffy for
@@ -499,7 +522,7 @@ int rvf_solve(rvf_session* s, rvf_mesh* m, const rvf_options* o, double* F_elem,
       d.N = N;
       d.nq = o->nquad;
       d.pairs = m->duffy_pairs.as<DuffyPair>();
-      d.n_pairs = m->n_duffy;
+      d.n_pairs = m->n_duffy + (o->self_vf ? m->n_duffy_self : 0);
       d.coords = m->coords.as<double>();
       d.enodes = m->enodes.as<int32_t>();
       d.area_orig = T->area_orig.as<double>();
