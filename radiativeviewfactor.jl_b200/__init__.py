@@ -10,17 +10,18 @@ Python identifier; import it through importlib, e.g.
         "rvf_b200", "radiativeviewfactor.jl_b200/__init__.py",
         submodule_search_locations=["radiativeviewfactor.jl_b200"])
 """
-from . import meshes
+from . import meshes, meshio
 from ._abi import PinnedArray, RVFError, Session, DeviceMesh, load_library
 from .assembly import (B200Backend, CPU, compute_view_factors, compute_view_factors_b200, make_options,
                        mesh_desc_arrays, register_gpu_hook)
 from .mesh import FAMILY_CODES, MeshData, SurfaceElement, build_group_obs_soups, flatten, merged_obstruction
+from .meshio import load_mesh
 from .results import (ViewFactorResult, aggregate_by_group, check_closure, check_reciprocity,
                       reciprocity_error)
 
 __all__ = [
     "B200Backend", "CPU", "DeviceMesh", "FAMILY_CODES", "MeshData", "PinnedArray", "RVFError", "Session",
     "SurfaceElement", "ViewFactorResult", "aggregate_by_group", "build_group_obs_soups", "check_closure",
-    "check_reciprocity", "compute_view_factors", "compute_view_factors_b200", "flatten", "load_library",
-    "make_options", "merged_obstruction", "mesh_desc_arrays", "meshes", "reciprocity_error", "register_gpu_hook",
+    "check_reciprocity", "compute_view_factors", "compute_view_factors_b200", "flatten", "load_library", "load_mesh",
+    "make_options", "merged_obstruction", "mesh_desc_arrays", "meshes", "meshio", "reciprocity_error", "register_gpu_hook",
 ]
