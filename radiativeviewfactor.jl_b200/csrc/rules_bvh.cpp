@@ -5,6 +5,7 @@
 // ray decisions are required to match the reference ray by ray.
 #include <algorithm>
 #include <cmath>
+#include <thread>
 #include <utility>
 
 #include "rvf_host.h"
@@ -160,67 +161,96 @@ Rule line_rule(int n) {
 // ---------------------------------------------------------------------------
 // BVH build: median split on the longest axis, stable sort by centroid,
 // LEAF_MAX = 8, parent slot reserved before the children (src/BVH.jl:71-148).
+//
+// The tree is the reference's bit for bit; two things make it fast.  Each
+// primitive's box and centroids are evaluated once, with the reference's
+// arithmetic, instead of at every level.  And a subtree's node count depends
+// on its primitive count only (the split is mid = (start + stop) / 2), so the
+// pre-order slot of every node is known before its subtree is built: the two
+// halves of a large node are built on different threads, each into its own
+// slots and its own range of the index array.
 // ---------------------------------------------------------------------------
 namespace {
+
+constexpr int64_t kLeafMax = 8;
+constexpr int64_t kParallelMin = 8192;  // primitives below which a subtree stays on one thread
+
+int64_t subtree_nodes(int64_t n) {
+  if (n <= kLeafMax) return 1;
+  const int64_t l = (n - 1) / 2 + 1;  // mid - start + 1 for mid = (start + stop) / 2
+  return 1 + subtree_nodes(l) + subtree_nodes(n - l);
+}
 
 struct Builder {
   const double* soup;
   int nv;
   HostBVH* out;
+  std::vector<double> box;   // per primitive: lo x,y,z, hi x,y,z
+  std::vector<double> cent;  // per primitive: centroid x,y,z
   double S(int c, int v, int64_t t) const { return soup[c + 3 * (v + (int64_t)nv * t)]; }
-  void aabb(int64_t t, double* lo, double* hi) const {
-    double lox = S(0, 0, t), hix = lox, loy = S(1, 0, t), hiy = loy, loz = S(2, 0, t), hiz = loz;
-    for (int v = 1; v < nv; ++v) {
-      double x = S(0, v, t); lox = jmin(lox, x); hix = jmax(hix, x);
-      double y = S(1, v, t); loy = jmin(loy, y); hiy = jmax(hiy, y);
-      double z = S(2, v, t); loz = jmin(loz, z); hiz = jmax(hiz, z);
+  void prepare(int64_t n) {
+    box.resize((size_t)n * 6);
+    cent.resize((size_t)n * 3);
+    for (int64_t t = 0; t < n; ++t) {
+      double lox = S(0, 0, t), hix = lox, loy = S(1, 0, t), hiy = loy, loz = S(2, 0, t), hiz = loz;
+      for (int v = 1; v < nv; ++v) {
+        double x = S(0, v, t); lox = jmin(lox, x); hix = jmax(hix, x);
+        double y = S(1, v, t); loy = jmin(loy, y); hiy = jmax(hiy, y);
+        double z = S(2, v, t); loz = jmin(loz, z); hiz = jmax(hiz, z);
+      }
+      double* b = &box[(size_t)t * 6];
+      b[0] = lox; b[1] = loy; b[2] = loz; b[3] = hix; b[4] = hiy; b[5] = hiz;
+      for (int axis = 0; axis < 3; ++axis) {
+        double c = 0.0;
+        for (int v = 0; v < nv; ++v) c += S(axis, v, t);
+        cent[(size_t)t * 3 + axis] = c / (double)nv;
+      }
     }
-    lo[0] = lox; lo[1] = loy; lo[2] = loz;
-    hi[0] = hix; hi[1] = hiy; hi[2] = hiz;
   }
-  double centroid(int64_t t, int axis) const {
-    double c = 0.0;
-    for (int v = 0; v < nv; ++v) c += S(axis, v, t);
-    return c / (double)nv;
-  }
-  int64_t rec(int64_t start, int64_t stop) {  // 1-based inclusive range of tri_idx
+  // Builds the subtree of tri_idx[start-1 .. stop-1] (1-based inclusive) with
+  // its root at node `self` (1-based); `spawn` halves left may go to threads.
+  void rec(int64_t start, int64_t stop, int64_t self, int spawn) {
     std::vector<int64_t>& idx = out->tri_idx;
-    double lo[3], hi[3];
-    aabb(idx[start - 1] - 1, lo, hi);
+    const double* b0 = &box[(size_t)(idx[start - 1] - 1) * 6];
+    double lo[3] = {b0[0], b0[1], b0[2]}, hi[3] = {b0[3], b0[4], b0[5]};
     for (int64_t i = start + 1; i <= stop; ++i) {
-      double l2[3], h2[3];
-      aabb(idx[i - 1] - 1, l2, h2);
-      for (int c = 0; c < 3; ++c) { lo[c] = jmin(lo[c], l2[c]); hi[c] = jmax(hi[c], h2[c]); }
+      const double* b = &box[(size_t)(idx[i - 1] - 1) * 6];
+      for (int c = 0; c < 3; ++c) { lo[c] = jmin(lo[c], b[c]); hi[c] = jmax(hi[c], b[3 + c]); }
     }
-    HostBVH::Node nd{};
+    HostBVH::Node& nd = out->nodes[self - 1];
     for (int c = 0; c < 3; ++c) { nd.lo[c] = lo[c]; nd.hi[c] = hi[c]; }
-    int64_t count = stop - start + 1;
-    if (count <= 8) {
+    const int64_t count = stop - start + 1;
+    if (count <= kLeafMax) {
       nd.tri_start = start;
       nd.tri_count = count;
-      out->nodes.push_back(nd);
-      return (int64_t)out->nodes.size();
+      return;
     }
     double ext[3] = {hi[0] - lo[0], hi[1] - lo[1], hi[2] - lo[2]};
     int axis = 0;
     for (int c = 1; c < 3; ++c)
       if (jisless(ext[axis], ext[c])) axis = c;
-    int64_t mid = (start + stop) / 2;
+    const int64_t mid = (start + stop) / 2;
     std::vector<std::pair<double, int64_t>> keyed;
     keyed.reserve(count);
-    for (int64_t i = start; i <= stop; ++i) keyed.push_back({centroid(idx[i - 1] - 1, axis), idx[i - 1]});
+    for (int64_t i = start; i <= stop; ++i) keyed.push_back({cent[(size_t)(idx[i - 1] - 1) * 3 + axis], idx[i - 1]});
     std::stable_sort(keyed.begin(), keyed.end(),
                      [](const std::pair<double, int64_t>& a, const std::pair<double, int64_t>& b) {
                        return jisless(a.first, b.first);
                      });
     for (int64_t i = start; i <= stop; ++i) idx[i - 1] = keyed[i - start].second;
-    out->nodes.push_back(nd);
-    int64_t self = (int64_t)out->nodes.size();
-    int64_t l = rec(start, mid);
-    int64_t r = rec(mid + 1, stop);
-    out->nodes[self - 1].left = l;
-    out->nodes[self - 1].right = r;
-    return self;
+    std::vector<std::pair<double, int64_t>>().swap(keyed);
+    const int64_t l = self + 1;
+    const int64_t r = l + subtree_nodes(mid - start + 1);
+    nd.left = l;
+    nd.right = r;
+    if (spawn > 0 && count >= kParallelMin) {
+      std::thread t([&, start, mid, l, spawn] { rec(start, mid, l, spawn - 1); });
+      rec(mid + 1, stop, r, spawn - 1);
+      t.join();
+    } else {
+      rec(start, mid, l, 0);
+      rec(mid + 1, stop, r, 0);
+    }
   }
   void miss(int64_t node, int64_t next) {  // src/GPUBVH.jl:69-82
     out->nodes[node - 1].miss = next;
@@ -239,8 +269,13 @@ HostBVH build_bvh(const double* soup, int nv, int64_t n_prims) {
   if (n_prims <= 0) return b;
   b.tri_idx.resize(n_prims);
   for (int64_t i = 0; i < n_prims; ++i) b.tri_idx[i] = i + 1;
-  Builder bl{soup, nv, &b};
-  bl.rec(1, n_prims);
+  b.nodes.assign((size_t)subtree_nodes(n_prims), HostBVH::Node{});
+  Builder bl{soup, nv, &b, {}, {}};
+  bl.prepare(n_prims);
+  const unsigned hc = std::thread::hardware_concurrency();
+  int spawn = 0;  // levels that fork: 2^spawn threads at most
+  while (spawn < 4 && (2u << spawn) <= std::max(1u, hc)) ++spawn;
+  bl.rec(1, n_prims, 1, spawn);
   bl.miss(1, 0);
   return b;
 }

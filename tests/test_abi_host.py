@@ -116,8 +116,9 @@ def _random_soup(rng, T, nv=3, jitter_ties=True):
     return s
 
 
-@pytest.mark.parametrize("T,nv", [(1, 3), (8, 3), (9, 3), (100, 3), (1728, 3), (37, 2), (800, 2)])
-def test_bvh_build_matches_oracle(orc, T, nv):
+@pytest.mark.parametrize("T,nv", [(1, 3), (8, 3), (9, 3), (100, 3), (1728, 3), (37, 2), (800, 2), (50000, 3),
+                                  (20001, 2)])
+def test_bvh_build_matches_oracle(rvf, orc, T, nv):
     from rvf_b200 import _abi
     rng = np.random.default_rng(T)
     soup = _random_soup(rng, T, nv)
@@ -130,6 +131,19 @@ def test_bvh_build_matches_oracle(orc, T, nv):
     for k in range(meta.shape[0]):
         if meta[k, 0] != 0:
             assert meta[k, 0] == k + 2
+
+
+def test_bvh_build_with_ties_matches_oracle(rvf, orc):
+    """A structured soup (many equal centroids along every axis) large enough
+    for the threaded build: the stable sort keeps ties in their current order."""
+    from rvf_b200 import _abi
+    md = rvf.meshes.cube_enclosure(40, family="tri3", jitter=0.0)
+    soup = np.concatenate([md.group_tri_soup[g] for g in sorted(md.group_tri_soup)])
+    assert soup.shape[0] >= 9000
+    lo, hi, meta, idx = _abi.bvh_build_host(soup)
+    lo2, hi2, meta2, idx2 = orc.BVH(soup).export()
+    assert np.array_equal(meta, meta2) and np.array_equal(idx, idx2)
+    assert np.array_equal(lo, lo2) and np.array_equal(hi, hi2)
 
 
 def test_bvh_box_soup_matches_oracle(rvf, orc):
