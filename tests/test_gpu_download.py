@@ -34,3 +34,28 @@ def test_chunked_solve_downloads_every_column(rvf, session, pinned, precision):
         if buf is not None:
             buf.free()
         small.close()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_odd_size_pinned_equals_pageable(rvf, session, precision):
+    """An odd N (columns of F not 16-byte aligned in host memory): pinned
+    (overlapped copies) and pageable destinations receive the same F."""
+    from rvf_b200 import _abi
+    full = rvf.meshes.cube_enclosure(5, box_m=2)
+    md = rvf.MeshData(full.coords, full.elem_nodes[:-1], full.elem_family[:-1], full.elem_group[:-1],
+                      dict(full.group_tags), dict(full.group_tri_soup), 2)
+    N = md.n_elems
+    assert N % 2 == 1
+    o = rvf.make_options(3, seed=0, precision=precision)
+    dm = _abi.DeviceMesh(session, rvf.mesh_desc_arrays(md, [7]))
+    buf = _abi.PinnedArray((N, N), order="F")
+    try:
+        ref = np.empty((N, N), order="F")
+        dm.solve(o, ref)
+        F = buf.array
+        F.fill(-7.0)
+        dm.solve(o, F)
+        assert np.array_equal(F, ref, equal_nan=True)
+    finally:
+        buf.free()
+        dm.release()
