@@ -118,6 +118,7 @@ int upload(Session* s, DevBuf& b, const void* src, size_t n) {
 // mesh upload
 // ---------------------------------------------------------------------------
 static const int kFamNodes[6] = {8, 6, 4, 3, 3, 2};
+static const int64_t kOrderRun = 8;  // caller-consecutive elements kept together in the internal order
 
 int mesh_upload(Session* s, const rvf_mesh_desc* d, rvf_mesh** out) {
   if (!d || !out) return set_err(RVF_EINVAL, "null argument");
@@ -177,10 +178,13 @@ int mesh_upload(Session* s, const rvf_mesh_desc* d, rvf_mesh** out) {
     m->h_members.insert(m->h_members.end(), mem[g].begin(), mem[g].end());
   }
 
-  // Internal element order: Morton (Z-order) curve of the element centroids,
-  // so that 32 consecutive elements form a compact patch and the shadow rays
-  // of one warp leave or reach neighbouring points.  Results stay in the
-  // caller's order (orig[internal] = original index).
+  // Internal element order: runs of kOrderRun consecutive elements of the
+  // caller, ordered along a Morton (Z-order) curve of the runs' centroids, so
+  // that 32 consecutive internal elements form a compact patch (the shadow
+  // rays of one warp leave or reach neighbouring points) while the caller's
+  // columns of F that finish together stay in runs of kOrderRun (one copy
+  // each when F is downloaded during the solve).  Results do not depend on
+  // this order; they stay in the caller's (orig[internal] = original index).
   m->h_orig.resize(N);
   {
     std::vector<double> cx(N), cy(N), cz(N);
@@ -203,22 +207,30 @@ int mesh_upload(Session* s, const rvf_mesh_desc* d, rvf_mesh** out) {
       v = (v | v << 2) & 0x1249249249249249ULL;
       return v;
     };
-    std::vector<std::pair<uint64_t, int32_t>> key(N);
-    for (int64_t e = 0; e < N; ++e) {
-      const double cc[3] = {cx[e], cy[e], cz[e]};
+    const int64_t n_runs = (N + kOrderRun - 1) / kOrderRun;
+    std::vector<std::pair<uint64_t, int32_t>> key(n_runs);
+    for (int64_t r = 0; r < n_runs; ++r) {
+      const int64_t e0 = r * kOrderRun, e1 = std::min<int64_t>(N, e0 + kOrderRun);
+      double cc[3] = {0.0, 0.0, 0.0};
+      for (int64_t e = e0; e < e1; ++e) { cc[0] += cx[e]; cc[1] += cy[e]; cc[2] += cz[e]; }
       uint64_t q3[3];
       for (int q = 0; q < 3; ++q) {
+        cc[q] /= (double)(e1 - e0);
         const double span = hi[q] - lo[q];
         const double f = span > 0.0 ? (cc[q] - lo[q]) / span : 0.0;
         q3[q] = (uint64_t)std::min(2097151.0, std::max(0.0, f * 2097151.0));
       }
-      key[e] = {spread(q3[0]) | (spread(q3[1]) << 1) | (spread(q3[2]) << 2), (int32_t)e};
+      key[r] = {spread(q3[0]) | (spread(q3[1]) << 1) | (spread(q3[2]) << 2), (int32_t)r};
     }
     std::stable_sort(key.begin(), key.end(),
                      [](const std::pair<uint64_t, int32_t>& a, const std::pair<uint64_t, int32_t>& b) {
                        return a.first < b.first;
                      });
-    for (int64_t e = 0; e < N; ++e) m->h_orig[e] = key[e].second;
+    int64_t at = 0;
+    for (int64_t k = 0; k < n_runs; ++k) {
+      const int64_t e0 = (int64_t)key[k].second * kOrderRun, e1 = std::min<int64_t>(N, e0 + kOrderRun);
+      for (int64_t e = e0; e < e1; ++e) m->h_orig[at++] = (int32_t)e;
+    }
   }
   std::vector<int32_t> p_enodes((size_t)N * 8), p_group(N);
   std::vector<int8_t> p_fam(N);
