@@ -46,6 +46,7 @@ extern "C" {
 #define RVF_ENODEV (-8)       /* no usable sm_100 device */
 #define RVF_EBUSY (-9)        /* result not ready yet (rvf_poll) */
 #define RVF_ECLOSED (-10)     /* serving queue closed */
+#define RVF_EINTERNAL (-11)   /* unexpected internal error (no C++ exception crosses this interface) */
 
 /* element family codes: src/GPUKernels.jl:344 (0..3), extended with curves */
 #define RVF_QUAD8 0

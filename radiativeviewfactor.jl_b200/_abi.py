@@ -17,7 +17,7 @@ LIB_PATH = Path(__file__).resolve().parent / "lib" / "librvf_b200.so"
 RVF_OK = 0
 STATUS_NAMES = {0: "RVF_OK", -1: "RVF_EINVAL", -2: "RVF_ENOMEM", -3: "RVF_EBUDGET", -4: "RVF_ECUDA",
                 -5: "RVF_ETIMEDOUT", -6: "RVF_ECANCELED", -7: "RVF_EUNSUPPORTED", -8: "RVF_ENODEV",
-                -9: "RVF_EBUSY", -10: "RVF_ECLOSED"}
+                -9: "RVF_EBUSY", -10: "RVF_ECLOSED", -11: "RVF_EINTERNAL"}
 globals().update({name: code for code, name in STATUS_NAMES.items()})  # RVF_EINVAL, ...
 
 METHOD_QUADRATURE, METHOD_MONTE_CARLO = 0, 1

@@ -11,8 +11,10 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <exception>
 #include <map>
 #include <memory>
+#include <new>
 #include <mutex>
 #include <string>
 #include <thread>
@@ -38,6 +40,24 @@ int set_err(int code, const char* fmt, ...) {
 
 int cuda_err(cudaError_t e, const char* what) {
   return set_err(RVF_ECUDA, "%s: %s (%s)", what, cudaGetErrorName(e), cudaGetErrorString(e));
+}
+
+int exception_status() noexcept {
+  int code = RVF_EINTERNAL;
+  try {
+    try {
+      throw;
+    } catch (const std::bad_alloc&) {
+      code = RVF_ENOMEM;
+      set_err(code, "host memory allocation failed");
+    } catch (const std::exception& e) {
+      set_err(code, "internal error: %s", e.what());
+    } catch (...) {
+      set_err(code, "internal error");
+    }
+  } catch (...) {  // recording the message failed too
+  }
+  return code;
 }
 
 // ---------------------------------------------------------------------------

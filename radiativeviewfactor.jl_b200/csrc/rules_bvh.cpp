@@ -5,6 +5,7 @@
 // ray decisions are required to match the reference ray by ray.
 #include <algorithm>
 #include <cmath>
+#include <exception>
 #include <thread>
 #include <utility>
 
@@ -244,9 +245,22 @@ struct Builder {
     nd.left = l;
     nd.right = r;
     if (spawn > 0 && count >= kParallelMin) {
-      std::thread t([&, start, mid, l, spawn] { rec(start, mid, l, spawn - 1); });
-      rec(mid + 1, stop, r, spawn - 1);
+      std::exception_ptr err;  // an exception of the helper thread is rethrown here
+      std::thread t([&, start, mid, l, spawn] {
+        try {
+          rec(start, mid, l, spawn - 1);
+        } catch (...) {
+          err = std::current_exception();
+        }
+      });
+      try {
+        rec(mid + 1, stop, r, spawn - 1);
+      } catch (...) {
+        t.join();
+        throw;
+      }
       t.join();
+      if (err) std::rethrow_exception(err);
     } else {
       rec(start, mid, l, 0);
       rec(mid + 1, stop, r, 0);

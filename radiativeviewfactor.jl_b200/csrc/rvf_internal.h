@@ -24,6 +24,9 @@ using Session = ::rvf_session;
 
 int set_err(int code, const char* fmt, ...);
 int cuda_err(cudaError_t e, const char* what);
+// Status of the exception being handled (call inside a catch block): every
+// entry point of the C interface turns exceptions into a status this way.
+int exception_status() noexcept;
 extern thread_local std::string g_last_error;
 
 // Device allocation charged against the session's HBM budget.

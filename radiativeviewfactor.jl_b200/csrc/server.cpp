@@ -418,7 +418,30 @@ void run_mc_chunk(rvf_server* sv, Req* r) {
   }
 }
 
+void worker_loop(rvf_server* sv);
+
+// The worker thread: an exception (a failed host allocation) fails the
+// requests in progress, whose state is then unknown, and the loop goes on.
 void worker_main(rvf_server* sv) {
+  for (;;) {
+    try {
+      worker_loop(sv);
+      return;
+    } catch (...) {
+      const int rc = exception_status();
+      std::lock_guard<std::mutex> lk(sv->mu);
+      for (auto& kv : sv->reqs) {
+        Req* r = kv.second.get();
+        if (r->state != RVF_REQ_RUNNING) continue;
+        finish(sv, r, RVF_REQ_FAILED, rc);
+        drop_device(sv, r);
+      }
+      sv->active.clear();
+    }
+  }
+}
+
+void worker_loop(rvf_server* sv) {
   for (;;) {
     std::vector<Req*> admit;
     {
@@ -535,7 +558,7 @@ int report(const Req* r, rvf_request_info* info) {
 
 extern "C" {
 
-int rvf_server_create(rvf_session* s, const rvf_server_opts* o, rvf_server** out) {
+int rvf_server_create(rvf_session* s, const rvf_server_opts* o, rvf_server** out) try {
   if (!s || !out) return set_err(RVF_EINVAL, "null argument");
   auto sv = std::make_unique<rvf_server>();
   sv->s = s;
@@ -544,13 +567,14 @@ int rvf_server_create(rvf_session* s, const rvf_server_opts* o, rvf_server** out
     return set_err(RVF_EINVAL, "max_batch %d outside 0..%d", sv->o.max_batch, kMaxBatch);
   sv->admit_budget = sv->o.admit_bytes ? sv->o.admit_bytes : (uint64_t)(0.7 * (double)s->budget);
   sv->t0 = Clock::now();
-  rvf_server* p = sv.release();
-  p->worker = std::thread(worker_main, p);
-  *out = p;
+  sv->worker = std::thread(worker_main, sv.get());
+  *out = sv.release();
   return RVF_OK;
+} catch (...) {
+  return exception_status();
 }
 
-int rvf_server_destroy(rvf_server* sv) {
+int rvf_server_destroy(rvf_server* sv) try {
   if (!sv) return RVF_OK;
   {
     std::lock_guard<std::mutex> lk(sv->mu);
@@ -567,9 +591,11 @@ int rvf_server_destroy(rvf_server* sv) {
   }
   delete sv;
   return RVF_OK;
+} catch (...) {
+  return exception_status();
 }
 
-int rvf_submit(rvf_server* sv, const rvf_mesh_desc* d, const rvf_options* o, int64_t* id) {
+int rvf_submit(rvf_server* sv, const rvf_mesh_desc* d, const rvf_options* o, int64_t* id) try {
   if (!sv || !d || !o || !id) return set_err(RVF_EINVAL, "null argument");
   if (o->ray_log) return set_err(RVF_EINVAL, "ray_log is not supported by the server");
   if (d->n_elems < 0 || d->n_elems > INT32_MAX) return set_err(RVF_EINVAL, "n_elems %lld out of range", (long long)d->n_elems);
@@ -590,17 +616,21 @@ int rvf_submit(rvf_server* sv, const rvf_mesh_desc* d, const rvf_options* o, int
   ++sv->submitted;
   sv->cv_work.notify_all();
   return RVF_OK;
+} catch (...) {
+  return exception_status();
 }
 
-int rvf_poll(rvf_server* sv, int64_t id, rvf_request_info* info) {
+int rvf_poll(rvf_server* sv, int64_t id, rvf_request_info* info) try {
   if (!sv) return set_err(RVF_EINVAL, "null server");
   std::lock_guard<std::mutex> lk(sv->mu);
   Req* r = find(sv, id);
   if (!r) return set_err(RVF_EINVAL, "unknown request %lld", (long long)id);
   return report(r, info);
+} catch (...) {
+  return exception_status();
 }
 
-int rvf_wait(rvf_server* sv, int64_t id, int64_t timeout_ms, rvf_request_info* info) {
+int rvf_wait(rvf_server* sv, int64_t id, int64_t timeout_ms, rvf_request_info* info) try {
   if (!sv) return set_err(RVF_EINVAL, "null server");
   std::unique_lock<std::mutex> lk(sv->mu);
   Req* r = find(sv, id);
@@ -615,9 +645,11 @@ int rvf_wait(rvf_server* sv, int64_t id, int64_t timeout_ms, rvf_request_info* i
   if (rc == RVF_ECANCELED) return set_err(rc, "request %lld was cancelled", (long long)id);
   if (rc != RVF_OK) return set_err(rc, "request %lld failed (status %d)", (long long)id, rc);
   return RVF_OK;
+} catch (...) {
+  return exception_status();
 }
 
-int rvf_cancel(rvf_server* sv, int64_t id) {
+int rvf_cancel(rvf_server* sv, int64_t id) try {
   if (!sv) return set_err(RVF_EINVAL, "null server");
   std::lock_guard<std::mutex> lk(sv->mu);
   Req* r = find(sv, id);
@@ -625,10 +657,12 @@ int rvf_cancel(rvf_server* sv, int64_t id) {
   if (r->state == RVF_REQ_QUEUED || r->state == RVF_REQ_RUNNING) r->cancel = true;
   sv->cv_work.notify_all();
   return RVF_OK;
+} catch (...) {
+  return exception_status();
 }
 
 int rvf_request_result(rvf_server* sv, int64_t id, double* F_elem, double* A_elem, double* F_group,
-                       double* A_group, double* row_sums) {
+                       double* A_group, double* row_sums) try {
   if (!sv) return set_err(RVF_EINVAL, "null server");
   rvf_mesh* m = nullptr;
   {
@@ -655,9 +689,11 @@ int rvf_request_result(rvf_server* sv, int64_t id, double* F_elem, double* A_ele
   }
   if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
   return e == cudaSuccess ? RVF_OK : cuda_err(e, "result copy");
+} catch (...) {
+  return exception_status();
 }
 
-int rvf_release(rvf_server* sv, int64_t id) {
+int rvf_release(rvf_server* sv, int64_t id) try {
   if (!sv) return set_err(RVF_EINVAL, "null server");
   std::lock_guard<std::mutex> lk(sv->mu);
   Req* r = find(sv, id);
@@ -667,9 +703,11 @@ int rvf_release(rvf_server* sv, int64_t id) {
   drop_device(sv, r);
   sv->reqs.erase(id);
   return RVF_OK;
+} catch (...) {
+  return exception_status();
 }
 
-int rvf_server_stats_get(rvf_server* sv, rvf_server_stats* st) {
+int rvf_server_stats_get(rvf_server* sv, rvf_server_stats* st) try {
   if (!sv || !st) return set_err(RVF_EINVAL, "null argument");
   std::lock_guard<std::mutex> lk(sv->mu);
   *st = rvf_server_stats{};
@@ -698,6 +736,8 @@ int rvf_server_stats_get(rvf_server* sv, rvf_server_stats* st) {
   st->batched_requests = sv->batched;
   st->admitted_bytes_peak = sv->admitted_peak;
   return RVF_OK;
+} catch (...) {
+  return exception_status();
 }
 
 }  // extern "C"

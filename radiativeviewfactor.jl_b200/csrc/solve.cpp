@@ -251,7 +251,7 @@ void rvf_default_options(rvf_options* o) {
   o->near_field_factor = 2.0;
 }
 
-int rvf_session_create(const rvf_session_opts* opts, rvf_session** out) {
+int rvf_session_create(const rvf_session_opts* opts, rvf_session** out) try {
   if (!out) return set_err(RVF_EINVAL, "null out");
   *out = nullptr;
   int dev = opts ? opts->device : 0;
@@ -285,9 +285,11 @@ int rvf_session_create(const rvf_session_opts* opts, rvf_session** out) {
   if ((rc = s->counters.alloc(s.get(), 256))) return rc;
   *out = s.release();
   return RVF_OK;
+} catch (...) {
+  return exception_status();
 }
 
-int rvf_session_destroy(rvf_session* s) {
+int rvf_session_destroy(rvf_session* s) try {
   if (!s) return RVF_OK;
   {
     std::lock_guard<std::mutex> lk(s->mu);
@@ -314,6 +316,8 @@ int rvf_session_destroy(rvf_session* s) {
   }
   delete s;
   return RVF_OK;
+} catch (...) {
+  return exception_status();
 }
 
 int rvf_device_info(rvf_session* s, int* sm_count, uint64_t* hbm_total, uint64_t* hbm_free) {
@@ -327,16 +331,18 @@ int rvf_device_info(rvf_session* s, int* sm_count, uint64_t* hbm_total, uint64_t
   return RVF_OK;
 }
 
-int rvf_mesh_upload(rvf_session* s, const rvf_mesh_desc* d, rvf_mesh** out) {
+int rvf_mesh_upload(rvf_session* s, const rvf_mesh_desc* d, rvf_mesh** out) try {
   if (!s) return set_err(RVF_EINVAL, "null session");
   std::lock_guard<std::mutex> lk(s->mu);
   cudaSetDevice(s->device);
   int rc = mesh_upload(s, d, out);
   if (rc == RVF_OK) s->meshes.insert(*out);
   return rc;
+} catch (...) {
+  return exception_status();
 }
 
-int rvf_mesh_release(rvf_session* s, rvf_mesh* m) {
+int rvf_mesh_release(rvf_session* s, rvf_mesh* m) try {
   if (!s || !m) return set_err(RVF_EINVAL, "null argument");
   std::lock_guard<std::mutex> lk(s->mu);
   if (!s->meshes.count(m)) return set_err(RVF_EINVAL, "mesh does not belong to this session");
@@ -345,6 +351,8 @@ int rvf_mesh_release(rvf_session* s, rvf_mesh* m) {
   s->meshes.erase(m);
   delete m;
   return RVF_OK;
+} catch (...) {
+  return exception_status();
 }
 
 int rvf_mesh_n_elems(const rvf_mesh* m, int64_t* n) {
@@ -404,7 +412,7 @@ struct ColumnDownload {
 }  // namespace
 
 int rvf_solve(rvf_session* s, rvf_mesh* m, const rvf_options* o, double* F_elem, double* A_elem, double* F_group,
-              double* A_group, double* row_sums, rvf_stats* st) {
+              double* A_group, double* row_sums, rvf_stats* st) try {
   if (!s || !m || !o) return set_err(RVF_EINVAL, "null argument");
   std::lock_guard<std::mutex> lk(s->mu);
   if (!s->meshes.count(m)) return set_err(RVF_EINVAL, "mesh does not belong to this session");
@@ -604,9 +612,11 @@ int rvf_solve(rvf_session* s, rvf_mesh* m, const rvf_options* o, double* F_elem,
     *st = S;
   }
   return RVF_OK;
+} catch (...) {
+  return exception_status();
 }
 
-int rvf_result_copy(rvf_session* s, rvf_mesh* m, double* F_elem, double* A_elem) {
+int rvf_result_copy(rvf_session* s, rvf_mesh* m, double* F_elem, double* A_elem) try {
   if (!s || !m) return set_err(RVF_EINVAL, "null argument");
   std::lock_guard<std::mutex> lk(s->mu);
   if (!m->has_result) return set_err(RVF_EINVAL, "no result on this mesh yet");
@@ -616,6 +626,8 @@ int rvf_result_copy(rvf_session* s, rvf_mesh* m, double* F_elem, double* A_elem)
   if (e == cudaSuccess && A_elem) e = cudaMemcpyAsync(A_elem, m->result_area, sizeof(double) * m->N, cudaMemcpyDeviceToHost, s->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
   return e == cudaSuccess ? RVF_OK : cuda_err(e, "rvf_result_copy");
+} catch (...) {
+  return exception_status();
 }
 
 int rvf_result_device(rvf_mesh* m, const double** F_dev, const double** A_dev) {
@@ -641,7 +653,7 @@ int rvf_host_free(void* p) {
   return RVF_OK;
 }
 
-int rvf_quadrature_rule(int32_t family, int32_t nquad, double* pts, double* wts, int32_t* n_pts) {
+int rvf_quadrature_rule(int32_t family, int32_t nquad, double* pts, double* wts, int32_t* n_pts) try {
   if (family < 0 || family > 5 || nquad < 1) return set_err(RVF_EINVAL, "bad family/nquad");
   Rule r = (family == 0 || family == 2) ? gl2d(nquad) : (family == 1 || family == 3) ? tri_rule(nquad) : line_rule(nquad);
   if (n_pts) *n_pts = r.size();
@@ -650,10 +662,12 @@ int rvf_quadrature_rule(int32_t family, int32_t nquad, double* pts, double* wts,
     if (wts) wts[k] = r.w[k];
   }
   return RVF_OK;
+} catch (...) {
+  return exception_status();
 }
 
 int rvf_bvh_build_host(const double* soup, int32_t nv, int64_t n_prims, double* lo, double* hi, int32_t* meta,
-                       int32_t* tri_idx, int64_t* n_nodes) {
+                       int32_t* tri_idx, int64_t* n_nodes) try {
   if (!soup || n_prims <= 0 || (nv != 2 && nv != 3)) return set_err(RVF_EINVAL, "bad soup");
   HostBVH b = build_bvh(soup, nv, n_prims);
   if (n_nodes) *n_nodes = (int64_t)b.nodes.size();
@@ -675,6 +689,8 @@ int rvf_bvh_build_host(const double* soup, int32_t nv, int64_t n_prims, double* 
   if (tri_idx)
     for (int64_t t = 0; t < n_prims; ++t) tri_idx[t] = (int32_t)b.tri_idx[t];
   return RVF_OK;
+} catch (...) {
+  return exception_status();
 }
 
 }  // extern "C"

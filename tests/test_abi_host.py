@@ -146,6 +146,21 @@ def test_bvh_build_with_ties_matches_oracle(rvf, orc):
     assert np.array_equal(lo, lo2) and np.array_equal(hi, hi2)
 
 
+def test_exceptions_do_not_cross_the_interface(rvf):
+    """A C++ exception inside an entry point comes back as a status: 2^62
+    primitives overflow the build's index array (std::length_error)."""
+    import ctypes as C
+    from rvf_b200 import _abi
+    lib = _abi.load_library()
+    soup = np.zeros((1, 3, 3))
+    n = C.c_int64(-1)
+    rc = lib.rvf_bvh_build_host(soup.ctypes.data_as(C.POINTER(C.c_double)), 3, 1 << 62, None, None, None, None,
+                                C.byref(n))
+    assert rc in (_abi.RVF_ENOMEM, _abi.RVF_EINTERNAL)
+    assert n.value == -1
+    assert "internal error" in _abi.last_error(lib) or "allocation" in _abi.last_error(lib)
+
+
 def test_bvh_box_soup_matches_oracle(rvf, orc):
     from rvf_b200 import _abi
     soup = rvf.meshes.obstruction_box()
