@@ -1,4 +1,4 @@
-"""Mesh ingest: Gmsh .msh 4.1 ASCII files -> MeshData (src/MeshIO.jl:94-149).
+"""Mesh ingest: Gmsh .msh 4.1 / 2.2 ASCII files -> MeshData (src/MeshIO.jl:94-149).
 
 The reference opens meshes through the Gmsh API (`load_mesh`); Gmsh is not
 part of this backend, so this module reads the file format itself.  A 4.1
@@ -32,7 +32,10 @@ src/MeshIO.jl:388-392), which Julia does not define, this reader takes
 ascending tags and ascending node positions: elements come grouped by
 ascending physical tag, so the element-level F is a permutation of the
 reference's by groups and every group-level result is the same.
-Binary files and format versions other than 4.1 are rejected.
+.msh 2.2 ASCII files are read too: there an entity is an elementary tag,
+its physical groups are those its elements name, and each node is
+classified on the lowest-dimensional entity whose elements use it.  Binary
+files and other format versions are rejected.
 """
 from __future__ import annotations
 
@@ -109,37 +112,90 @@ def _sections(text: str):
 
 
 def read_msh(filename: str) -> MshModel:
-    """Parse a Gmsh .msh 4.1 ASCII file."""
+    """Parse a Gmsh .msh file, 4.1 or 2.2 ASCII."""
     with open(filename, "rb") as f:
         raw = f.read()
     try:
         text = raw.decode("utf-8")
     except UnicodeDecodeError:
         raise ValueError(f"{filename}: not an ASCII .msh file (binary .msh is not supported)") from None
-    model = MshModel()
-    seen_format = False
+    sections: Dict[str, List[str]] = {}
     for name, body in _sections(text):
-        if name == "MeshFormat":
-            parts = body[0].split()
-            version, ftype = parts[0], int(parts[1])
-            if version != "4.1":
-                raise ValueError(f"{filename}: .msh version {version} is not supported (4.1 ASCII only)")
-            if ftype != 0:
-                raise ValueError(f"{filename}: binary .msh is not supported (4.1 ASCII only)")
-            seen_format = True
-        elif name == "PhysicalNames":
-            for ln in body[1:1 + int(body[0])]:
-                p = shlex.split(ln)
-                model.physical_names[(int(p[0]), int(p[1]))] = p[2] if len(p) > 2 else ""
-        elif name == "Entities":
-            _parse_entities(body, model)
-        elif name == "Nodes":
-            _parse_nodes(body, model)
-        elif name == "Elements":
-            _parse_elements(body, model)
-    if not seen_format:
+        sections.setdefault(name, body)
+    if "MeshFormat" not in sections:
         raise ValueError(f"{filename}: no $MeshFormat section (not a Gmsh .msh file)")
+    parts = sections["MeshFormat"][0].split()
+    version, ftype = parts[0], int(parts[1])
+    if version not in ("4.1", "2.2"):
+        raise ValueError(f"{filename}: .msh version {version} is not supported (4.1 or 2.2 ASCII)")
+    if ftype != 0:
+        raise ValueError(f"{filename}: binary .msh is not supported (4.1 or 2.2 ASCII)")
+    model = MshModel()
+    body = sections.get("PhysicalNames")
+    if body:
+        for ln in body[1:1 + int(body[0])]:
+            p = shlex.split(ln)
+            model.physical_names[(int(p[0]), int(p[1]))] = p[2] if len(p) > 2 else ""
+    if version == "4.1":
+        if "Entities" in sections:
+            _parse_entities(sections["Entities"], model)
+        if "Nodes" in sections:
+            _parse_nodes(sections["Nodes"], model)
+        if "Elements" in sections:
+            _parse_elements(sections["Elements"], model)
+    elif "Nodes" in sections:
+        _parse_v2(sections["Nodes"], sections.get("Elements", ["0"]), model, filename)
     return model
+
+
+# dimension of each Gmsh element type (points 15; lines 1, 8; surfaces 2, 3,
+# 9, 10, 16; the rest are volumes or higher-order types not read here)
+_TYPE_DIM = {15: 0, 1: 1, 8: 1, 26: 1, 27: 1, 28: 1, 2: 2, 3: 2, 9: 2, 10: 2, 16: 2, 20: 2, 21: 2, 22: 2, 23: 2,
+             24: 2, 25: 2}
+
+
+def _parse_v2(node_body: List[str], body: List[str], model: MshModel, filename: str):
+    """.msh 2.2: elements carry their physical and elementary tags; there are
+    no entity blocks, so an entity is an elementary tag of a dimension, it
+    belongs to the physical groups its elements name, and a node is
+    classified on the lowest-dimensional entity whose elements use it (a
+    model point, then a curve, ...), as Gmsh classifies mesh nodes."""
+    n_nodes = int(node_body[0].split()[0])
+    tags = np.empty(n_nodes, dtype=np.int64)
+    xyz = np.empty((n_nodes, 3))
+    for a in range(n_nodes):
+        v = node_body[1 + a].split()
+        tags[a] = int(v[0])
+        xyz[a] = [float(v[1]), float(v[2]), float(v[3])]
+    n_el = int(body[0].split()[0])
+    blocks: Dict[Tuple[int, int, int], list] = {}
+    owner: Dict[int, Tuple[int, int]] = {}
+    for a in range(n_el):
+        v = [int(x) for x in body[1 + a].split()]
+        etag, etype, ntags = v[0], v[1], v[2]
+        tg = v[3:3 + ntags]
+        phys = tg[0] if ntags >= 1 else 0
+        ent = tg[1] if ntags >= 2 else 0
+        nodes = v[3 + ntags:]
+        width = ELEM_INFO[etype][0] if etype in ELEM_INFO else _OTHER_NODES.get(etype, len(nodes))
+        if len(nodes) != width:
+            raise ValueError(f"{filename}: element {etag} of type {etype} has {len(nodes)} nodes, expected {width}")
+        dim = _TYPE_DIM.get(etype, 3)
+        ps = model.entity_physicals.setdefault((dim, ent), [])
+        if phys and phys not in ps:
+            ps.append(phys)
+        blocks.setdefault((dim, ent, etype), []).append([etag] + nodes)
+        for t in nodes:
+            cur = owner.get(t)
+            if cur is None or (dim, ent) < cur:
+                owner[t] = (dim, ent)
+    for (dim, ent, etype), rows in blocks.items():
+        model.elem_blocks.append((dim, ent, etype, np.array(rows, dtype=np.int64)))
+    per_block: Dict[Tuple[int, int], List[int]] = {}
+    for a in range(n_nodes):
+        per_block.setdefault(owner.get(int(tags[a]), (3, 0)), []).append(a)
+    for (dim, ent), idx in per_block.items():
+        model.node_blocks.append((dim, ent, tags[idx], xyz[idx]))
 
 
 def _parse_entities(body: List[str], model: MshModel):
@@ -188,7 +244,7 @@ def _parse_elements(body: List[str], model: MshModel):
 
 def load_mesh(filename: str, surface_dim: int = 2, reverse_normals: bool = False,
               verbose: bool = True) -> MeshData:
-    """src/MeshIO.jl:94-149 for Gmsh .msh 4.1 ASCII files."""
+    """src/MeshIO.jl:94-149 for Gmsh .msh 4.1 and 2.2 ASCII files."""
     if not os.path.isfile(filename):
         raise FileNotFoundError(f"Mesh file not found: {filename}")
     if surface_dim not in (1, 2):

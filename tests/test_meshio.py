@@ -1,8 +1,9 @@
-"""Mesh ingest (load_mesh on Gmsh .msh 4.1 ASCII files, src/MeshIO.jl:94-149).
+"""Mesh ingest (load_mesh on Gmsh .msh 4.1 / 2.2 ASCII files, src/MeshIO.jl:94-149).
 
 tests/golden/plate_quad9.msh is written by hand in the format Gmsh writes
 (corner nodes on point entities, edge nodes on curves, interior nodes on the
-surface; point, Line3 and Quad9 element blocks).  The other files are written
+surface; point, Line3 and Quad9 element blocks); plate_quad9_v22.msh is the
+same plate in the legacy 2.2 format.  The other files are written
 by write_msh from the package's meshes or from Delaunay triangulations, which
 stand in for Gmsh's unstructured meshing in the reference's own load_mesh
 tests (test/runtests.jl:303-420: families by order, total plate area 1, the
@@ -90,6 +91,28 @@ def test_golden_plate_curves_default_group(rvf):
     assert md.elem_nodes[:, :3].tolist() == [[1, 6, 5], [6, 2, 7]]  # normals already point into the plate
 
 
+def test_legacy_v22_matches_v41(rvf):
+    """The same plate written in the .msh 2.2 format: same elements (by
+    geometry), families, groups and curve orientation."""
+    v22 = GOLDEN / "plate_quad9_v22.msh"
+    for dim in (2, 1):
+        a = rvf.load_mesh(str(PLATE), surface_dim=dim, verbose=False)
+        b = rvf.load_mesh(str(v22), surface_dim=dim, verbose=False)
+        assert a.group_tags == b.group_tags
+        assert np.array_equal(a.elem_family, b.elem_family) and np.array_equal(a.elem_group, b.elem_group)
+        for x, y in zip(element_geometry(a), element_geometry(b)):
+            assert np.array_equal(x, y)
+
+
+def test_legacy_v22_lines_turned_toward_the_surface(rvf, tmp_path):
+    text = (GOLDEN / "plate_quad9_v22.msh").read_text().replace("2 8 2 0 1 1 6 5\n", "2 8 2 0 1 6 1 5\n")
+    f = tmp_path / "reversed_v22.msh"
+    f.write_text(text)
+    md = rvf.load_mesh(str(f), surface_dim=1, verbose=False)
+    ref = rvf.load_mesh(str(GOLDEN / "plate_quad9_v22.msh"), surface_dim=1, verbose=False)
+    assert np.array_equal(md.elem_nodes, ref.elem_nodes)
+
+
 def test_line_elements_turned_toward_the_surface(rvf, tmp_path, capsys):
     text = PLATE.read_text().replace("2 1 6 5\n3 6 2 7\n", "2 6 1 5\n3 2 6 7\n")
     f = tmp_path / "reversed.msh"
@@ -157,8 +180,8 @@ def test_load_errors(rvf, tmp_path):
         rvf.load_mesh(str(tmp_path / "missing.msh"))
     with pytest.raises(ValueError, match="surface_dim"):
         rvf.load_mesh(str(PLATE), surface_dim=3)
-    old = tmp_path / "v22.msh"
-    old.write_text("$MeshFormat\n2.2 0 8\n$EndMeshFormat\n")
+    old = tmp_path / "v30.msh"
+    old.write_text("$MeshFormat\n3.0 0 8\n$EndMeshFormat\n")
     with pytest.raises(ValueError, match="not supported"):
         rvf.load_mesh(str(old))
     binary = tmp_path / "bin.msh"
