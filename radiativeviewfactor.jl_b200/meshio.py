@@ -242,6 +242,29 @@ def _parse_elements(body: List[str], model: MshModel):
         model.elem_blocks.append((dim, tag, etype, np.array(rows, dtype=np.int64).reshape(n, 1 + width)))
 
 
+def is_xml_vtk(filename: str) -> bool:
+    """src/MeshIO.jl:158-170: XML VTK by extension, or a .vtk file whose head
+    is XML."""
+    ext = os.path.splitext(filename)[1].lower()
+    if ext in (".vtu", ".pvtu", ".vts", ".vtr", ".vti", ".vtp"):
+        return True
+    if ext != ".vtk":
+        return False
+    with open(filename, "rb") as f:
+        head = f.read(512).decode("latin-1")
+    return "<?xml" in head or "<VTKFile" in head
+
+
+def load_vtu(filename: str, surface_dim: int = 2, reverse_normals: bool = False, verbose: bool = True,
+             group_field=None) -> MeshData:
+    """src/MeshIO.jl:191-206.  The reference reads XML VTK through its ReadVTK
+    extension and raises when ReadVTK is not loaded; this backend has no XML
+    VTK reader, so it always raises."""
+    raise NotImplementedError(
+        f"{filename}: reading XML VTK files (.vtu) needs the reference's ReadVTK extension, which this backend "
+        "does not provide; write the mesh as Gmsh .msh (4.1 or 2.2 ASCII) and use load_mesh.")
+
+
 def load_mesh(filename: str, surface_dim: int = 2, reverse_normals: bool = False,
               verbose: bool = True) -> MeshData:
     """src/MeshIO.jl:94-149 for Gmsh .msh 4.1 and 2.2 ASCII files."""
@@ -249,6 +272,8 @@ def load_mesh(filename: str, surface_dim: int = 2, reverse_normals: bool = False
         raise FileNotFoundError(f"Mesh file not found: {filename}")
     if surface_dim not in (1, 2):
         raise ValueError(f"surface_dim must be 1 or 2, got {surface_dim}")
+    if is_xml_vtk(filename):  # src/MeshIO.jl:101-103
+        return load_vtu(filename, surface_dim, reverse_normals, verbose)
     model = read_msh(filename)
     dim = surface_dim
     # nodes (getNodes(): every entity block, by dimension then tag)

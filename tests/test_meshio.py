@@ -175,6 +175,20 @@ def test_unstructured_plates_area(rvf, orc, tmp_path, order):
         assert abs(A[md.elem_group == g].sum() - 1.0) < 1e-9
 
 
+def test_xml_vtk_is_routed_to_load_vtu(rvf, tmp_path):
+    """src/MeshIO.jl:101-103 and 158-170: XML VTK goes to load_vtu, which
+    needs ReadVTK in the reference and is not provided here."""
+    f = tmp_path / "plate.vtu"
+    f.write_text('<?xml version="1.0"?>\n<VTKFile type="UnstructuredGrid"></VTKFile>\n')
+    with pytest.raises(NotImplementedError, match="ReadVTK"):
+        rvf.load_mesh(str(f))
+    g = tmp_path / "xml.vtk"
+    g.write_text('<VTKFile type="UnstructuredGrid"></VTKFile>\n')
+    assert rvf.meshio.is_xml_vtk(str(g)) and not rvf.meshio.is_xml_vtk(str(PLATE))
+    with pytest.raises(NotImplementedError):
+        rvf.plot_mesh_normals(None)
+
+
 def test_load_errors(rvf, tmp_path):
     with pytest.raises(FileNotFoundError):
         rvf.load_mesh(str(tmp_path / "missing.msh"))
