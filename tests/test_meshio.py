@@ -122,6 +122,19 @@ def test_line_elements_turned_toward_the_surface(rvf, tmp_path, capsys):
     assert "Reoriented 2 Line3 element(s)" in capsys.readouterr().out
 
 
+def test_parametric_node_block(rvf, tmp_path):
+    """A 4.1 node block flagged parametric carries the curve parameter after
+    x y z on each coordinate line; the reader keeps x y z."""
+    text = PLATE.read_text().replace("1 1 0 3\n5\n6\n7\n0.25 0 0\n0.5 0 0\n0.75 0 0\n",
+                                     "1 1 1 3\n5\n6\n7\n0.25 0 0 0.25\n0.5 0 0 0.5\n0.75 0 0 0.75\n")
+    assert text != PLATE.read_text()
+    f = tmp_path / "parametric.msh"
+    f.write_text(text)
+    a = rvf.load_mesh(str(PLATE), verbose=False)
+    b = rvf.load_mesh(str(f), verbose=False)
+    assert np.array_equal(a.coords, b.coords) and np.array_equal(a.elem_nodes, b.elem_nodes)
+
+
 def test_reverse_normals_follows_the_reference(rvf):
     md = rvf.load_mesh(str(PLATE), reverse_normals=True, verbose=False)
     # Quad8: corners 1<->3 and mid-side nodes 5<->7, as src/MeshIO.jl:624-626 swaps them
