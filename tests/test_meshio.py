@@ -197,7 +197,10 @@ def test_xml_vtk_is_routed_to_load_vtu(rvf, tmp_path):
         rvf.load_mesh(str(f))
     g = tmp_path / "xml.vtk"
     g.write_text('<VTKFile type="UnstructuredGrid"></VTKFile>\n')
+    legacy = tmp_path / "legacy.vtk"
+    legacy.write_text("# vtk DataFile Version 3.0\nmesh\nASCII\n")
     assert rvf.meshio.is_xml_vtk(str(g)) and not rvf.meshio.is_xml_vtk(str(PLATE))
+    assert not rvf.meshio.is_xml_vtk(str(legacy))  # test/runtests.jl:453-456
     with pytest.raises(NotImplementedError):
         rvf.plot_mesh_normals(None)
 
