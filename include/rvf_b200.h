@@ -277,15 +277,20 @@ int rvf_server_stats_get(rvf_server* sv, rvf_server_stats* st);
  * reference).  For callers that cannot call cudaMalloc -- code under an
  * allocator that owns all device memory, memory-capped services, hosts that
  * hand the library pre-placed buffers only.  Inputs and outputs are the
- * caller's device pointers: coords (3 x n_nodes column-major), elem_family
+ * caller's device pointers, all on the current device (each is checked with
+ * cudaPointerGetAttributes; host memory or another device's buffer is
+ * RVF_EINVAL): coords (3 x n_nodes column-major), elem_family
  * (RVF_QUAD8..RVF_LINE2), elem_nodes (n_elems x 8 element-major, 1-based node
  * ids, zero padded), elem_group; outputs F (n_elems^2 column-major, F[i,j] =
  * raw/A_i as rvf_solve) and A (n_elems).  No obstruction, no group sums.
  * Scratch lives in one fixed 16 MiB __device__ array inside the library
  * (held by every GPU that loads the library until exit); a mesh whose tables
  * need more (about 90 B per element + 1792 B per 32 elements per quadrature
- * point) is rejected with RVF_EINVAL.  The first call on a device looks up
- * that array's device address, so make it before any stream capture.  Calls
+ * point; at most 114,900 elements) is rejected with RVF_EINVAL, and nquad
+ * above 8 (surfaces) or 64 (curves) with RVF_EUNSUPPORTED.  The first call on
+ * a device (and again after the device's context changes, e.g. after
+ * cudaDeviceReset) looks up that array's device address, so make it before
+ * any stream capture.  Calls
  * share the array; they take a process-wide lock and synchronise `stream`
  * (a cudaStream_t, NULL = legacy default stream) before returning, because
  * calls that overlapped on the GPU would race on it. */

@@ -28,9 +28,47 @@ namespace {
 constexpr size_t kNoAllocScratchBytes = size_t(16) << 20;
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
+// Device addresses of the scratch array, one per (device, context): a device
+// reset or a new primary context can load the array at a new address, so the
+// address is looked up again whenever the current context changes.
 constexpr int kMaxDevices = 64;
 std::mutex g_noalloc_mu;
-unsigned char* g_noalloc_addr[kMaxDevices] = {};
+struct ScratchAddr {
+  void* ctx = nullptr;
+  unsigned char* addr = nullptr;
+};
+ScratchAddr g_noalloc_addr[kMaxDevices];
+
+// cuCtxGetCurrent through the runtime's driver entry-point table (no libcuda
+// link); returns the current context handle, or null when it is unavailable.
+void* current_context() {
+  using Fn = int (*)(void**);
+  static Fn fn = [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      f = nullptr;
+    return reinterpret_cast<Fn>(f);
+  }();
+  void* ctx = nullptr;
+  if (!fn || fn(&ctx) != 0) return nullptr;
+  return ctx;
+}
+
+// True when p is device (or managed) memory that device `dev` owns.
+bool on_device(const void* p, int dev) {
+  cudaPointerAttributes at{};
+  if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+    cudaGetLastError();  // clear the sticky-free error of an unknown pointer
+    return false;
+  }
+  return (at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged) && at.device == dev;
+}
+
+// Largest mesh the array can hold: about 90 bytes of per-element data plus
+// at least 1 quadrature point's table (56 bytes) per element.
+constexpr int64_t kNoAllocMaxElems = (int64_t)(kNoAllocScratchBytes / 146);
 
 size_t align256(size_t n) { return (n + 255) & ~size_t(255); }
 
@@ -63,11 +101,20 @@ using namespace rvf;
 
 extern "C" int rvf_solve_fp64_noalloc(const double* coords, int64_t n_nodes, const int8_t* elem_family,
                                       const int32_t* elem_nodes, const int32_t* elem_group, int64_t n_elems,
-                                      int32_t mesh_dim, int32_t nquad, double* F, double* A, void* stream) {
+                                      int32_t mesh_dim, int32_t nquad, double* F, double* A, void* stream) try {
   if (n_elems < 0 || n_nodes < 0) return set_err(RVF_EINVAL, "negative sizes");
   if (mesh_dim != 1 && mesh_dim != 2) return set_err(RVF_EINVAL, "mesh_dim must be 1 or 2, got %d", mesh_dim);
   if (nquad < 1) return set_err(RVF_EINVAL, "nquad must be >= 1, got %d", nquad);
+  // surfaces: nquad^2 Gauss-Legendre points (at most kMaxPts = 64); curves: nquad points
+  const int nq_max = mesh_dim == 2 ? 8 : kMaxPts;
+  if (nquad > nq_max)
+    return set_err(RVF_EUNSUPPORTED, "nquad=%d: at most %d is supported for mesh_dim %d", nquad, nq_max, mesh_dim);
   if (n_elems == 0) return RVF_OK;
+  if (n_elems > kNoAllocMaxElems)
+    return set_err(RVF_EINVAL,
+                   "rvf_solve_fp64_noalloc: %lld elements exceed the fixed scratch array (%zu bytes, at most %lld "
+                   "elements)",
+                   (long long)n_elems, kNoAllocScratchBytes, (long long)kNoAllocMaxElems);
   if (!coords || !elem_family || !elem_nodes || !elem_group || !F || !A)
     return set_err(RVF_EINVAL, "null device pointer");
   const cudaStream_t st = static_cast<cudaStream_t>(stream);
@@ -76,13 +123,25 @@ extern "C" int rvf_solve_fp64_noalloc(const double* coords, int64_t n_nodes, con
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return cuda_err(e, "cudaGetDevice");
   if (dev < 0 || dev >= kMaxDevices) return set_err(RVF_ENODEV, "device ordinal %d out of range", dev);
-  if (!g_noalloc_addr[dev]) {  // once per device, with that device current
+  {
+    const void* ptrs[6] = {coords, elem_family, elem_nodes, elem_group, F, A};
+    const char* names[6] = {"coords", "elem_family", "elem_nodes", "elem_group", "F", "A"};
+    for (int k = 0; k < 6; ++k)
+      if (!on_device(ptrs[k], dev))
+        return set_err(RVF_EINVAL, "rvf_solve_fp64_noalloc: %s is not device memory of the current device %d",
+                       names[k], dev);
+  }
+  // once per device and context, with that device current
+  void* ctx = current_context();
+  ScratchAddr& sa = g_noalloc_addr[dev];
+  if (!sa.addr || !ctx || sa.ctx != ctx) {
     void* p = nullptr;
     e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
     if (e != cudaSuccess) return cuda_err(e, "cudaGetSymbolAddress(scratch)");
-    g_noalloc_addr[dev] = static_cast<unsigned char*>(p);
+    sa.addr = static_cast<unsigned char*>(p);
+    sa.ctx = ctx;
   }
-  unsigned char* base = g_noalloc_addr[dev];
+  unsigned char* base = sa.addr;
   int sm_count = 0;
   if ((e = cudaDeviceGetAttribute(&sm_count, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess)
     return cuda_err(e, "cudaDeviceGetAttribute");
@@ -182,4 +241,6 @@ extern "C" int rvf_solve_fp64_noalloc(const double* coords, int64_t n_nodes, con
   if (herr & kErrWaitTimeout) return set_err(RVF_ETIMEDOUT, "a bounded device wait gave up");
   if (herr & kErrBadInput) return set_err(RVF_EINVAL, "mesh holds a degenerate element");
   return RVF_OK;
+} catch (...) {
+  return exception_status();
 }

@@ -19,17 +19,24 @@ pytestmark = pytest.mark.gpu
 RTOL = 1e-10
 
 
-def _existing_entry_point(rvf, session, md, nquad):
+def _existing_entry_point(rvf, session, md, nquad, obstruction_groups=()):
     from rvf_b200 import _abi
-    dm = _abi.DeviceMesh(session, rvf.mesh_desc_arrays(md, ()))
+    dm = _abi.DeviceMesh(session, rvf.mesh_desc_arrays(md, obstruction_groups))
     try:
         N = md.n_elems
         F = np.empty((N, N), order="F")
         A = np.empty(N)
-        dm.solve(rvf.make_options(nquad, seed=0), F, A)
+        dm.solve(rvf.make_options(nquad, seed=0, occlusion=False), F, A)
         return F, A
     finally:
         dm.release()
+
+
+def _oracle(orc, md, nquad):
+    """The oracle's plain FP64 assembly without obstructions."""
+    m = orc.Mesh(md)
+    raw, area, _, _ = orc.solve_plain(m, nquad)
+    return orc.f_from_raw(raw, area), area
 
 
 def _noalloc(rvf, md, nquad):
@@ -56,7 +63,7 @@ def _assert_rel(a, b):
     assert not bad.any(), f"{int(bad.sum())} entries differ beyond rtol={RTOL}"
 
 
-def test_noalloc_matches_rvf_solve_on_two_calls(rvf, session):
+def test_noalloc_matches_rvf_solve_on_two_calls(rvf, orc, session):
     first = rvf.meshes.parallel_plates(10, "quad")        # 200 Quad8, nquad 4 (16 points)
     second = rvf.meshes.cube_enclosure(3, box=False)      # 108 Tri3, nquad 3 (7 points)
     for md, nq in ((first, 4), (second, 3)):
@@ -65,6 +72,47 @@ def test_noalloc_matches_rvf_solve_on_two_calls(rvf, session):
         assert rc == 0, rvf._abi.last_error()
         _assert_rel(A, A_ref)
         _assert_rel(F, F_ref)
+        F_orc, A_orc = _oracle(orc, md, nq)
+        _assert_rel(A, A_orc)
+        _assert_rel(F, F_orc)
+
+
+def test_noalloc_ignores_obstructions(rvf, session):
+    """No obstruction: on a cube with an obstructing box (and faces that hide
+    one another behind it) the result equals rvf_solve with occlusion off."""
+    md = rvf.meshes.cube_enclosure(4, box_m=2)
+    F_ref, A_ref = _existing_entry_point(rvf, session, md, 3, obstruction_groups=[7])
+    rc, F, A = _noalloc(rvf, md, 3)
+    assert rc == 0, rvf._abi.last_error()
+    _assert_rel(A, A_ref)
+    _assert_rel(F, F_ref)
+
+
+def test_noalloc_rejects_unsupported_nquad(rvf, session):
+    md = rvf.meshes.parallel_plates(2, "quad4")
+    rc, _, _ = _noalloc(rvf, md, 100000)
+    assert rc == -7  # RVF_EUNSUPPORTED, before any rule is built
+    assert "nquad" in rvf._abi.last_error()
+
+
+def test_noalloc_rejects_host_pointers(rvf, session):
+    import torch
+    from rvf_b200 import _abi
+    lib = _abi.load_library()
+    md = rvf.meshes.parallel_plates(2, "quad4")
+    N = md.n_elems
+    dev = torch.device("cuda:0")
+    coords_host = np.asfortranarray(md.coords).ravel(order="F").copy()
+    fam = torch.from_numpy(np.ascontiguousarray(md.elem_family, dtype=np.int8)).to(dev)
+    nodes = torch.from_numpy(np.ascontiguousarray(md.elem_nodes, dtype=np.int32)).to(dev)
+    grp = torch.from_numpy(np.ascontiguousarray(md.elem_group, dtype=np.int32)).to(dev)
+    F = torch.zeros(N * N, dtype=torch.float64, device=dev)
+    A = torch.zeros(N, dtype=torch.float64, device=dev)
+    torch.cuda.synchronize()
+    rc = lib.rvf_solve_fp64_noalloc(coords_host.ctypes.data, md.coords.shape[1], fam.data_ptr(), nodes.data_ptr(),
+                                    grp.data_ptr(), N, md.mesh_dim, 2, F.data_ptr(), A.data_ptr(), None)
+    assert rc == -1
+    assert "coords" in _abi.last_error()
 
 
 def test_noalloc_rejects_meshes_beyond_its_scratch(rvf, session):
