@@ -112,7 +112,9 @@ typedef struct {
   int32_t disable_pair_lists; /* 3-D occlusion: 1 = every ray walks the tree (same results; for testing) */
   int32_t self_vf;            /* 1: also integrate the pairs (i, i) -- concave elements see themselves
                                  (src/Assembly.jl:173,193, j_start = self_vf ? i : i + 1); quadrature only */
-  int32_t reserved[6];
+  int32_t disable_tile_cull;  /* 1: no tile classification -- every shadow ray goes through the ray pipeline
+                                 and every tile through its generation loop (same view factors; for testing) */
+  int32_t reserved[5];
 } rvf_options;
 
 typedef struct {
@@ -147,7 +149,10 @@ typedef struct {
   int64_t n_list_pairs;   /* 3-D occlusion: pending pairs whose rays test a per-pair triangle list */
   int64_t n_walk_pairs;   /*   ... whose list overflowed (their rays walk the tree) */
   double ms_lists;        /*   building the per-pair lists (part of ms_trace) */
-  int64_t reserved[5];
+  int64_t n_tiles_culled; /* 3-D occlusion: tiles none of whose shadow rays can be blocked (no ray work) */
+  int64_t n_pairs_masked; /*   pairs whose rays may be blocked (the only ones through the ray pipeline) */
+  double ms_cull;         /* tile classification before the pair pipeline */
+  int64_t reserved[2];
 } rvf_stats;
 
 const char* rvf_version(void);

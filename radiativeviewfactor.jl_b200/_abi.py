@@ -47,7 +47,7 @@ class Options(C.Structure):
                 ("seed", C.c_uint64), ("precision", C.c_int32), ("occlusion", C.c_int32),
                 ("geometric_soup", C.c_int32), ("mc_exclude_groups", C.c_int32), ("near_field_factor", C.c_double),
                 ("ray_log", _pu8), ("ray_log_pm", C.c_int32), ("disable_pair_lists", C.c_int32),
-                ("self_vf", C.c_int32), ("reserved", C.c_int32 * 6)]
+                ("self_vf", C.c_int32), ("disable_tile_cull", C.c_int32), ("reserved", C.c_int32 * 5)]
 
 
 class Stats(C.Structure):
@@ -61,7 +61,8 @@ class Stats(C.Structure):
                 ("n_unsure_prim", C.c_int64), ("n_unsure_dir", C.c_int64), ("n_rays_traced", C.c_int64),
                 ("n_chunks", C.c_int64), ("ms_gen", C.c_double), ("ms_trace", C.c_double),
                 ("ms_trace_fp64", C.c_double), ("ms_resolve", C.c_double), ("n_list_pairs", C.c_int64),
-                ("n_walk_pairs", C.c_int64), ("ms_lists", C.c_double), ("reserved", C.c_int64 * 5)]
+                ("n_walk_pairs", C.c_int64), ("ms_lists", C.c_double), ("n_tiles_culled", C.c_int64),
+                ("n_pairs_masked", C.c_int64), ("ms_cull", C.c_double), ("reserved", C.c_int64 * 2)]
 
     def as_dict(self):
         d = {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}

@@ -146,14 +146,20 @@ __device__ __forceinline__ void eval_line(const double* __restrict__ coords, con
 // Reference formula (src/GPUKernels.jl:204-215 / src/ViewFactorKernel.jl:169-180),
 // bit for bit.  dim3: cos*cos/(pi r^2); otherwise cos*cos/(2 r).
 template <bool DIM3>
-__device__ __noinline__ double k_reference(double rx, double ry, double rz, double r2, const double* ni,
-                                           const double* nj) {
+__device__ __forceinline__ double k_reference_inl(double rx, double ry, double rz, double r2, const double* ni,
+                                                  const double* nj) {
   double r = sqrt(r2);
   double hx = rx / r, hy = ry / r, hz = rz / r;
   double ci = (ni[0] * hx + ni[1] * hy) + ni[2] * hz;
   double cj = (nj[0] * (-hx) + nj[1] * (-hy)) + nj[2] * (-hz);
   if (ci <= 0.0 || cj <= 0.0) return 0.0;
   return DIM3 ? (ci * cj) / (kPiD * r2) : (ci * cj) / (2.0 * r);
+}
+// out of line where the caller keeps many registers live across it
+template <bool DIM3>
+__device__ __noinline__ double k_reference(double rx, double ry, double rz, double r2, const double* ni,
+                                           const double* nj) {
+  return k_reference_inl<DIM3>(rx, ry, rz, r2, ni, nj);
 }
 
 // Fast evaluation with the same K > 0 decision as the reference.

@@ -44,6 +44,39 @@ struct PairList {
   int32_t off;
 };
 
+// Tile classes (kernels_cull.cu): per 32 x 32 tile of the upper triangle a
+// class byte and, for kClsSlow tiles, 32 mask words (row li of the tile ->
+// bit lj set when some shadow ray of the pair may be blocked).
+enum : uint8_t {
+  kClsSlow = 1,  // some pair's rays may be blocked: the ray pipeline, with the mask
+  kClsNear = 2,  // some pair is near field (mixed precision integrates it in FP64)
+  kClsTiny = 4,  // some pair's points may nearly coincide (mixed precision: FP64)
+};
+constexpr int kTileLeaves = 128;  // candidate leaves of a tile's walk
+constexpr int kTileTris = 1024;   // listed triangles of a tile (more: every pair keeps its rays)
+
+struct TileClassArgs {
+  int64_t N, nT, n_tiles;
+  const double* cen;
+  const double* rad;
+  const double* diam;
+  const int32_t* group;
+  double near_factor;  // < 0: no near-field classification
+  double tiny_gap;     // pairs closer than rad_i + rad_j + tiny_gap are kClsTiny
+  double cull_margin;
+  bool occ, dim3;
+  const NodeF* nodesf;
+  int n_nodes;
+  const int32_t* frontier;
+  int n_frontier;
+  const int32_t* leaf_of;
+  const float4* sat;
+  float sat_em;
+  uint8_t* cls;    // n_tiles
+  uint32_t* mask;  // n_tiles x 32
+  unsigned long long* counters;  // [culled tiles, masked pairs]
+};
+
 struct WaveQ {
   uint64_t* rec64;  // FP64 ray queue
   uint64_t* rec32;  // FP32 ray queue (mixed precision)
@@ -111,6 +144,8 @@ struct PairArgs {
   int log_pm;
   WaveQ q;                       // wavefront queues (the fused kernel ignores them)
   int64_t tile0;                 // batched generation: first tile of this request in the launch
+  const uint8_t* tcls;           // tile classes and masks (kernels_cull.cu), or null
+  const uint32_t* tmask;
 };
 
 struct RedArgs {
@@ -168,6 +203,8 @@ struct MixedArgs {
   int log_pm;
   WaveQ q;
   int64_t tile0;
+  const uint8_t* tcls;  // tile classes and masks (kernels_cull.cu), or null
+  const uint32_t* tmask;
 };
 
 struct TraceArgs {
@@ -273,6 +310,8 @@ cudaError_t launch_trace(const WaveShape& sh, const TraceBatch* t, bool fp32, in
 cudaError_t launch_resolve(const WaveShape& sh, const ResolveBatch* r, int sm_count, cudaStream_t st);
 // Pair lists of the chunk's pending pairs (3-D triangles with occlusion).
 cudaError_t launch_plist(const TraceBatch* t, int sm_count, cudaStream_t st);
+// Tile classes and masks of one request (before its first chunk).
+cudaError_t launch_tile_class(const TileClassArgs& a, int sm_count, cudaStream_t st);
 
 // A Quad8 pair sharing corner nodes (src/DuffyKernel.jl:95-115), i < j in the
 // caller's order (the reference integrates with elem_i = the lower index).

@@ -29,6 +29,7 @@
 
 #include <cstdint>
 
+#include "device_lists.cuh"
 #include "device_trace.cuh"
 #include "kernels.h"
 
@@ -225,10 +226,233 @@ __device__ __forceinline__ int find_req(const int64_t* tile_base, int n_req, int
 }  // namespace
 
 // ---------------------------------------------------------------------------
+// 1a. Generation of a tile without shadow-ray work (the tile classification
+// found no pair whose rays may be blocked, or the mesh has no obstruction):
+// the quadrature alone, register-blocked.  Lane l owns destination
+// j = 32 bj + l and holds QB of its points in registers; the warp walks the
+// source element's points p, read once per QB point pairs from the staged
+// block in shared memory (broadcast), so each point pair costs the kernel's
+// arithmetic and about 7/QB shared loads.  Sums run in the pipeline's order
+// (over p inside, then w_q * inner over q), so an FP64 fast tile is bit for
+// bit what the ray pipeline gives for pairs whose rays are all visible.
+// Out of line: their registers are allocated apart from the ray pipeline's.
+// ---------------------------------------------------------------------------
+template <bool DIM3, bool OCC, int QB>
+__device__ __noinline__ void gen_fast_fp64(const PairArgs& a, const double* iblk, int64_t bi, int64_t bj, int warp,
+                                           int lane, uint32_t& n_pp, uint32_t& n_rays) {
+  const int64_t N = a.N;
+  const int pm = a.pmax;
+  const int64_t j = bj * kTile + lane;
+  const bool jok = j < N;
+  const int64_t oj = jok ? (a.orig ? (int64_t)a.orig[j] : j) : 0;
+  const int npj0 = jok ? a.np[j] : 0;
+  const double* jb = a.tab + bj * kComp * pm * kTile + lane;
+  for (int rr = 0; rr < kTile / 8; ++rr) {
+    const int li = warp + 8 * rr;
+    const int64_t i = bi * kTile + li;
+    if (i >= N) break;  // warp-uniform; later rows are further out
+    const bool valid = jok && i < j;
+    const int64_t oi = a.orig ? (int64_t)a.orig[i] : i;
+    const int npi = a.np[i];
+    int npj = valid ? npj0 : 0;
+    if (valid && a.flat[i] && a.flat[j] && a.nrm[3 * i] == a.nrm[3 * j] && a.nrm[3 * i + 1] == a.nrm[3 * j + 1] &&
+        a.nrm[3 * i + 2] == a.nrm[3 * j + 2])
+      npj = 0;
+    const int qmax = __reduce_max_sync(kFull, npj);
+    const double* ib = iblk + li;
+    double acc = 0.0;
+    for (int q0 = 0; q0 < qmax; q0 += QB) {
+      double xq[QB][3], nq[QB][3], wq[QB];
+#pragma unroll
+      for (int u = 0; u < QB; ++u) {
+        const int q = q0 + u;
+        const bool lq = q < npj;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          xq[u][c] = lq ? jb[(c * pm + q) * kTile] : 0.0;
+          nq[u][c] = lq ? jb[((3 + c) * pm + q) * kTile] : 0.0;
+        }
+        wq[u] = lq ? jb[(6 * pm + q) * kTile] : 0.0;
+      }
+      double inner[QB];
+#pragma unroll
+      for (int u = 0; u < QB; ++u) inner[u] = 0.0;
+      // k_fast with its grazing branch taken out of the loop: a lane that
+      // meets a grazing point pair (either |cos| within 1e-5 of zero) forms
+      // the chunk again below with k_fast's own arithmetic
+      bool graze = false;
+      uint32_t cast = 0;
+      for (int p = 0; p < npi; ++p) {
+        double xi[3], ni[3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          xi[c] = ib[(c * pm + p) * kTile];
+          ni[c] = ib[((3 + c) * pm + p) * kTile];
+        }
+        const double wi = ib[(6 * pm + p) * kTile];
+#pragma unroll
+        for (int u = 0; u < QB; ++u) {
+          if (q0 + u < npj) {
+            const double rx = xq[u][0] - xi[0], ry = xq[u][1] - xi[1], rz = xq[u][2] - xi[2];
+            const double r2 = (rx * rx + ry * ry) + rz * rz;
+            const double di = fma(ni[0], rx, fma(ni[1], ry, ni[2] * rz));
+            const double dj = -fma(nq[u][0], rx, fma(nq[u][1], ry, nq[u][2] * rz));
+            const double thr = 1e-10 * r2;
+            const bool big = !(r2 < 1e-30);
+            graze = graze || (big && (di * di <= thr || dj * dj <= thr));
+            double K = 0.0;
+            if (big && di > 0.0 && dj > 0.0)
+              K = DIM3 ? (di * dj) * rcp_nr(kPiD * (r2 * r2)) : (di * dj) * rcp_nr(2.0 * (r2 * sqrt(r2)));
+            cast += K > 0.0 ? 1 : 0;
+            inner[u] = fma(wi, K, inner[u]);
+          }
+        }
+      }
+      if (__any_sync(kFull, graze) && graze) {  // rare: the chunk again, exactly as the ray pipeline forms it
+        cast = 0;
+#pragma unroll
+        for (int u = 0; u < QB; ++u) inner[u] = 0.0;
+        for (int p = 0; p < npi; ++p) {
+          double xi[3], ni[3];
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            xi[c] = ib[(c * pm + p) * kTile];
+            ni[c] = ib[((3 + c) * pm + p) * kTile];
+          }
+          const double wi = ib[(6 * pm + p) * kTile];
+#pragma unroll
+          for (int u = 0; u < QB; ++u) {
+            if (q0 + u < npj) {
+              const double rx = xq[u][0] - xi[0], ry = xq[u][1] - xi[1], rz = xq[u][2] - xi[2];
+              const double r2 = (rx * rx + ry * ry) + rz * rz;
+              // k_fast, with the reference formula in line
+              double K = 0.0;
+              if (!(r2 < 1e-30)) {
+                const double di = fma(ni[0], rx, fma(ni[1], ry, ni[2] * rz));
+                const double dj = -fma(nq[u][0], rx, fma(nq[u][1], ry, nq[u][2] * rz));
+                const double thr = 1e-10 * r2;
+                if (di * di <= thr || dj * dj <= thr) K = k_reference_inl<DIM3>(rx, ry, rz, r2, ni, nq[u]);
+                else if (di > 0.0 && dj > 0.0)
+                  K = DIM3 ? (di * dj) * rcp_nr(kPiD * (r2 * r2)) : (di * dj) * rcp_nr(2.0 * (r2 * sqrt(r2)));
+              }
+              cast += K > 0.0 ? 1 : 0;
+              inner[u] = fma(wi, K, inner[u]);
+            }
+          }
+        }
+      }
+      if (OCC) n_rays += cast;
+#pragma unroll
+      for (int u = 0; u < QB; ++u)
+        if (q0 + u < npj) acc = fma(wq[u], inner[u], acc);
+    }
+    n_pp += (uint32_t)(npi * npj);
+    if (valid) {
+      a.F[oi + oj * N] = acc / a.area[i];
+      a.F[oj + oi * N] = acc / a.area[j];
+    } else if (j == i) {
+      a.F[oi + oi * N] = 0.0 / a.area[i];
+    }
+  }
+}
+
+// Mixed precision: the FP32 far-field arithmetic of k_gen_mixed (offsets
+// from the element centroids, FP32 per-pair sums), for tiles with neither
+// near-field nor nearly coincident pairs.  Grazing point pairs stay in FP32
+// here: no ray depends on the sign of their K, and their FP32 error is that
+// of any other far-field term.
+template <bool OCC, int QB>
+__device__ __noinline__ void gen_fast_mixed(const MixedArgs& a, const float* iblk, int64_t bi, int64_t bj, int warp,
+                                            int lane, uint32_t& n_pp, uint32_t& n_rays) {
+  const int64_t N = a.N;
+  const int pm = a.pmax;
+  const int64_t j = bj * kTile + lane;
+  const bool jok = j < N;
+  const int64_t oj = jok ? (a.orig ? (int64_t)a.orig[j] : j) : 0;
+  const int npj0 = jok ? a.np[j] : 0;
+  const float* jbf = a.tabf + bj * kComp * pm * kTile + lane;
+  const double cj0 = jok ? a.cen[3 * j] : 0.0, cj1 = jok ? a.cen[3 * j + 1] : 0.0, cj2 = jok ? a.cen[3 * j + 2] : 0.0;
+  for (int rr = 0; rr < kTile / 8; ++rr) {
+    const int li = warp + 8 * rr;
+    const int64_t i = bi * kTile + li;
+    if (i >= N) break;  // warp-uniform
+    const bool valid = jok && i < j;
+    const int64_t oi = a.orig ? (int64_t)a.orig[i] : i;
+    const int npi = a.np[i];
+    int npj = valid ? npj0 : 0;
+    if (valid && a.flat[i] && a.flat[j] && a.nrm[3 * i] == a.nrm[3 * j] && a.nrm[3 * i + 1] == a.nrm[3 * j + 1] &&
+        a.nrm[3 * i + 2] == a.nrm[3 * j + 2])
+      npj = 0;
+    const int qmax = __reduce_max_sync(kFull, npj);
+    const float d0 = (float)(cj0 - a.cen[3 * i]), d1 = (float)(cj1 - a.cen[3 * i + 1]),
+                d2 = (float)(cj2 - a.cen[3 * i + 2]);
+    const float* ibf = iblk + li;
+    float acc32 = 0.0f;
+    uint32_t cast = 0;
+    for (int q0 = 0; q0 < qmax; q0 += QB) {
+      float oq[QB][3], nq[QB][3], wq[QB];
+#pragma unroll
+      for (int u = 0; u < QB; ++u) {
+        const int q = q0 + u;
+        const bool lq = q < npj;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          oq[u][c] = lq ? jbf[(c * pm + q) * kTile] : 0.0f;
+          nq[u][c] = lq ? jbf[((3 + c) * pm + q) * kTile] : 0.0f;
+        }
+        wq[u] = lq ? jbf[(6 * pm + q) * kTile] : 0.0f;
+      }
+      float inner[QB];
+#pragma unroll
+      for (int u = 0; u < QB; ++u) inner[u] = 0.0f;
+      for (int p = 0; p < npi; ++p) {
+        const float op0 = ibf[(0 * pm + p) * kTile], op1 = ibf[(1 * pm + p) * kTile], op2 = ibf[(2 * pm + p) * kTile];
+        const float np0 = ibf[(3 * pm + p) * kTile], np1 = ibf[(4 * pm + p) * kTile], np2 = ibf[(5 * pm + p) * kTile];
+        const float wp = ibf[(6 * pm + p) * kTile];
+#pragma unroll
+        for (int u = 0; u < QB; ++u) {
+          if (q0 + u < npj) {
+            const float rx = d0 + (oq[u][0] - op0), ry = d1 + (oq[u][1] - op1), rz = d2 + (oq[u][2] - op2);
+            const float r2 = fmaf(rx, rx, fmaf(ry, ry, rz * rz));
+            const float di = fmaf(np0, rx, fmaf(np1, ry, np2 * rz));
+            const float dj = -fmaf(nq[u][0], rx, fmaf(nq[u][1], ry, nq[u][2] * rz));
+            const float K32 = (di > 0.0f && dj > 0.0f) ? (di * dj) * rcp_approx(3.14159265f * (r2 * r2)) : 0.0f;
+            cast += K32 > 0.0f ? 1 : 0;
+            inner[u] = fmaf(wp, K32, inner[u]);
+          }
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < QB; ++u)
+        if (q0 + u < npj) acc32 = fmaf(wq[u], inner[u], acc32);
+    }
+    if (OCC) n_rays += cast;
+    n_pp += (uint32_t)(npi * npj);
+    const double raw = 0.0 + (double)acc32;
+    if (valid) {
+      a.F[oi + oj * N] = raw / a.area[i];
+      a.F[oj + oi * N] = raw / a.area[j];
+    } else if (j == i) {
+      a.F[oi + oi * N] = 0.0 / a.area[i];
+    }
+  }
+}
+
+// Tile class of request-local tile t (kernels_cull.cu) and the mask words of
+// its rows in shared memory; without classes every pair keeps its rays.
+__device__ __forceinline__ uint8_t load_tile_class(const uint8_t* tcls, const uint32_t* tmask, int64_t t,
+                                                   uint32_t* s_mask) {
+  const uint8_t cls = tcls ? tcls[t] : (uint8_t)kClsSlow;
+  if (threadIdx.x < kTile)
+    s_mask[threadIdx.x] = !tcls ? 0xffffffffu : (cls & kClsSlow) ? tmask[t * kTile + threadIdx.x] : 0u;
+  return cls;
+}
+
+// ---------------------------------------------------------------------------
 // 1. Generation, FP64 (surfaces and curves).
 // ---------------------------------------------------------------------------
 template <bool DIM3, bool OCC>
-__global__ void __launch_bounds__(256, 3) k_gen_fp64(const GenBatch* __restrict__ Lp) {
+__global__ void __launch_bounds__(256, 2) k_gen_fp64(const GenBatch* __restrict__ Lp) {
   extern __shared__ __align__(128) unsigned char smem[];
   const GenBatch& L = *Lp;
   const int pmL = L.pmax_max;
@@ -239,6 +463,7 @@ __global__ void __launch_bounds__(256, 3) k_gen_fp64(const GenBatch* __restrict_
   __shared__ int s_req;
   __shared__ unsigned long long s_used, s_slots;
   __shared__ NodeD s_root;  // the request's root box: the only node the generation tests
+  __shared__ uint32_t s_mask[kTile];  // pairs of the tile whose rays may be blocked (row -> lanes)
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (threadIdx.x == 0) mbar_init(bar, 1);
@@ -275,6 +500,7 @@ __global__ void __launch_bounds__(256, 3) k_gen_fp64(const GenBatch* __restrict_
     const int pm = a.pmax;
     int64_t bi, bj;
     tile_coords(t, a.nT, bi, bj);
+    const uint8_t cls = load_tile_class(a.tcls, a.tmask, t, s_mask);
     const bool ok = mbar_wait_bounded(bar, phase);
     if (__syncthreads_or(!ok)) {
       if (threadIdx.x == 0) {
@@ -285,6 +511,13 @@ __global__ void __launch_bounds__(256, 3) k_gen_fp64(const GenBatch* __restrict_
     }
     phase ^= 1u;
 
+    if (a.tcls && !(cls & kClsSlow) && !a.ray_log) {  // block-uniform: no ray of the tile can be blocked
+      if (pm <= 3) gen_fast_fp64<DIM3, OCC, 3>(a, iblk, bi, bj, warp, lane, n_pp, n_rays);
+      else gen_fast_fp64<DIM3, OCC, 4>(a, iblk, bi, bj, warp, lane, n_pp, n_rays);
+      __syncthreads();
+      if (OCC && threadIdx.x == 0) resv_release(Q, need, need_s);
+      continue;
+    }
     const int64_t N = a.N;
     const int64_t j = bj * kTile + lane;
     const int64_t oj = (j < N) ? (a.orig ? (int64_t)a.orig[j] : j) : 0;
@@ -309,9 +542,10 @@ __global__ void __launch_bounds__(256, 3) k_gen_fp64(const GenBatch* __restrict_
                           ? a.ray_log + ((uint64_t)(sw ? oj : oi) * N + (sw ? oi : oj)) * a.log_pm * a.log_pm
                           : nullptr;
       // pairs whose rays all certainly miss the root box need no ray at all
-      const bool cullp = OCC && npj > 0 && a.rad &&
-                         pair_misses_box<DIM3>(a.cen + 3 * i, a.cen + 3 * j, fmax(a.rad[i], a.rad[j]) + a.cull_margin,
-                                               s_root);
+      const bool cullp = OCC && npj > 0 &&
+                         (!((s_mask[li] >> lane) & 1u) ||
+                          (a.rad && pair_misses_box<DIM3>(a.cen + 3 * i, a.cen + 3 * j,
+                                                          fmax(a.rad[i], a.rad[j]) + a.cull_margin, s_root)));
       double acc = 0.0;
       int64_t slot = -1;
       int nr = 0;
@@ -467,6 +701,7 @@ __global__ void __launch_bounds__(256, 2) k_gen_mixed(const GenBatch* __restrict
   __shared__ unsigned long long s_used, s_slots;
   __shared__ NodeF s_rootf;  // the request's root box, FP32 and FP64
   __shared__ NodeD s_root;
+  __shared__ uint32_t s_mask[kTile];  // pairs of the tile whose rays may be blocked (row -> lanes)
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   uint64_t* st64 = stage_all + warp * 64;
@@ -507,6 +742,7 @@ __global__ void __launch_bounds__(256, 2) k_gen_mixed(const GenBatch* __restrict
     const int pm = a.pmax;
     int64_t bi, bj;
     tile_coords(t, a.nT, bi, bj);
+    const uint8_t cls = load_tile_class(a.tcls, a.tmask, t, s_mask);
     const bool ok = mbar_wait_bounded(bar, phase);
     if (__syncthreads_or(!ok)) {
       if (threadIdx.x == 0) {
@@ -516,6 +752,16 @@ __global__ void __launch_bounds__(256, 2) k_gen_mixed(const GenBatch* __restrict
       break;
     }
     phase ^= 1u;
+
+    if (a.tcls && !(cls & (kClsSlow | kClsNear | kClsTiny)) && !a.ray_log) {  // block-uniform
+      if (pm == 7 || pm == 13 || pm == 49) gen_fast_mixed<OCC, 7>(a, iblk, bi, bj, warp, lane, n_pp, n_rays);
+      else if (pm == 5 || pm == 25) gen_fast_mixed<OCC, 5>(a, iblk, bi, bj, warp, lane, n_pp, n_rays);
+      else if (pm == 3 || pm == 9) gen_fast_mixed<OCC, 3>(a, iblk, bi, bj, warp, lane, n_pp, n_rays);
+      else gen_fast_mixed<OCC, 8>(a, iblk, bi, bj, warp, lane, n_pp, n_rays);
+      __syncthreads();
+      if (OCC && threadIdx.x == 0) resv_release(Q, need, need_s);
+      continue;
+    }
 
     const int64_t N = a.N;
     const int64_t j = bj * kTile + lane;
@@ -550,9 +796,10 @@ __global__ void __launch_bounds__(256, 2) k_gen_mixed(const GenBatch* __restrict
                   an2 = (float)(ci2 + (sw ? dc2 : 0.0));
       const float* ibf = iblk + li;
       const double* it64 = a.tab + bi * kComp * pm * kTile + li;
-      const bool cullp = OCC && npj > 0 && a.rad &&
-                         pair_misses_box<true>(a.cen + 3 * i, a.cen + 3 * j, fmax(a.rad[i], a.rad[j]) + a.cull_margin,
-                                               s_root);
+      const bool cullp = OCC && npj > 0 &&
+                         (!((s_mask[li] >> lane) & 1u) ||
+                          (a.rad && pair_misses_box<true>(a.cen + 3 * i, a.cen + 3 * j,
+                                                          fmax(a.rad[i], a.rad[j]) + a.cull_margin, s_root)));
       uint8_t* logp = (a.ray_log && valid)
                           ? a.ray_log + ((uint64_t)(sw ? oj : oi) * N + (sw ? oi : oj)) * a.log_pm * a.log_pm
                           : nullptr;
@@ -692,74 +939,6 @@ __device__ __forceinline__ void log_ray(const TraceArgs& a, int64_t i, int64_t j
 // means the reference's walk reaches the leaf.  A pair with more than
 // kListMax triangles keeps n = -1 and its rays walk the tree.
 // ---------------------------------------------------------------------------
-// Separation of the centroid segment (a, b) and the triangle (p0, p1, p2)
-// along w, in FP32: true when the gap exceeds rm |w|.  Squares avoid the
-// square root (rm > 0).
-__device__ __forceinline__ bool axis_separates(const float* a, const float* b, const float4& p0, const float4& p1,
-                                               const float4& p2, float wx, float wy, float wz, float rm) {
-  const float sa = fmaf(a[0], wx, fmaf(a[1], wy, a[2] * wz)), sb = fmaf(b[0], wx, fmaf(b[1], wy, b[2] * wz));
-  const float q0 = fmaf(p0.x, wx, fmaf(p0.y, wy, p0.z * wz));
-  const float q1 = fmaf(p1.x, wx, fmaf(p1.y, wy, p1.z * wz));
-  const float q2 = fmaf(p2.x, wx, fmaf(p2.y, wy, p2.z * wz));
-  const float gap = fmaxf(fminf(q0, fminf(q1, q2)) - fmaxf(sa, sb), fminf(sa, sb) - fmaxf(q0, fmaxf(q1, q2)));
-  return gap > 0.0f && gap * gap > rm * rm * fmaf(wx, wx, fmaf(wy, wy, wz * wz));
-}
-
-// True when no ray of the pair (segments within R of the centroid segment
-// a -> b, direction d) can be a hit of the reference's test of the triangle
-// with corners p0, p1, p2 (FP32) and rounding margin p0.w.  em absorbs the
-// FP32 rounding of the corners and of this test (a few 2^-24 of the
-// coordinates' magnitude, against em = S 2^-16).
-__device__ __forceinline__ bool pair_misses_tri(const float* a, const float* b, const float* d, float R, float em,
-                                                const float4& p0, const float4& p1, const float4& p2) {
-  const float rm = R + p0.w + em;
-  const float f1[3] = {p1.x - p0.x, p1.y - p0.y, p1.z - p0.z};
-  const float f2[3] = {p2.x - p0.x, p2.y - p0.y, p2.z - p0.z};
-  const float f3[3] = {p2.x - p1.x, p2.y - p1.y, p2.z - p1.z};
-  // the segment direction crossed with each edge, then the triangle's normal
-  if (axis_separates(a, b, p0, p1, p2, d[1] * f1[2] - d[2] * f1[1], d[2] * f1[0] - d[0] * f1[2],
-                     d[0] * f1[1] - d[1] * f1[0], rm))
-    return true;
-  if (axis_separates(a, b, p0, p1, p2, d[1] * f2[2] - d[2] * f2[1], d[2] * f2[0] - d[0] * f2[2],
-                     d[0] * f2[1] - d[1] * f2[0], rm))
-    return true;
-  if (axis_separates(a, b, p0, p1, p2, d[1] * f3[2] - d[2] * f3[1], d[2] * f3[0] - d[0] * f3[2],
-                     d[0] * f3[1] - d[1] * f3[0], rm))
-    return true;
-  return axis_separates(a, b, p0, p1, p2, f1[1] * f2[2] - f1[2] * f2[1], f1[2] * f2[0] - f1[0] * f2[2],
-                        f1[0] * f2[1] - f1[1] * f2[0], rm);
-}
-
-// The pair's capsule for the list walk, in FP32: the centroid segment's
-// start A and direction reciprocals (from FP64, rounded once), and the radius
-// grown by em.  A box test in FP32 (capsule_misses_box) then only reports a
-// miss when the FP64 test with the ungrown radius would: every rounding of
-// the test (the nodes' and A's FP32 copies, the subtraction, 1/d) moves a
-// slab parameter by a few 2^-24 S |1/d|, the growth by em = 2^-16 S moves it
-// by em |1/d|.  Components of d that are exactly zero use the containment
-// test, as pair_misses_box does.
-struct CapsuleF {
-  float A[3], inv[3];
-  bool zero[3];
-  float R;
-};
-
-__device__ __forceinline__ bool capsule_misses_box(const CapsuleF& c, const NodeF& nd) {
-  float te = 0.0f, tx = 1.0f;
-#pragma unroll
-  for (int k = 0; k < 3; ++k) {
-    const float lo = nd.lo[k] - c.R, hi = nd.hi[k] + c.R;
-    if (c.zero[k]) {
-      if (c.A[k] < lo || c.A[k] > hi) return true;
-      continue;
-    }
-    const float t1 = (lo - c.A[k]) * c.inv[k], t2 = (hi - c.A[k]) * c.inv[k];
-    te = fmaxf(te, fminf(t1, t2));
-    tx = fminf(tx, fmaxf(t1, t2));
-  }
-  return te > tx;
-}
-
 // The list of one pending pair, built by its warp: a breadth-first walk of
 // the tree with the capsule test from the precomputed start nodes (one node
 // per lane; every start node's box lies inside its ancestors', so skipping

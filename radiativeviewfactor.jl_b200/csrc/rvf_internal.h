@@ -53,6 +53,7 @@ struct Tables {
   DevBuf rules, tab, area, np, flat, nrm, cen, diam, rad;  // internal element order
   DevBuf area_orig;                                   // areas in the caller's element order
   DevBuf tabf;  // FP32 table, built on the first mixed-precision solve
+  DevBuf tcls, tmask;  // tile classes and masks of the last solve (kernels_cull.cu)
 };
 
 }  // namespace rvf

@@ -479,7 +479,11 @@ int rvf_solve(rvf_session* s, rvf_mesh* m, const rvf_options* o, double* F_elem,
     }
     cudaError_t e = cudaSuccess;
     WaveReq w;
-    if ((rc = wave_prepare(s, m, T, o, o->ray_log ? log.as<uint8_t>() : nullptr, w, &n_kernels))) return rc;
+    {
+      EvTimer tc(s->stream);
+      if ((rc = wave_prepare(s, m, T, o, o->ray_log ? log.as<uint8_t>() : nullptr, w, &n_kernels))) return rc;
+      S.ms_cull = tc.stop();
+    }
     // Duffy and self pairs overwrite F after the pipeline: no early columns then
     if (F_elem && N > 1 && !(o->use_duffy && m->dim == 2) && !o->self_vf) {
       dl.s = s;
@@ -601,6 +605,8 @@ int rvf_solve(rvf_session* s, rvf_mesh* m, const rvf_options* o, double* F_elem,
     S.n_unsure_dir = mixed ? (int64_t)c[10] : 0;
     S.n_list_pairs = (int64_t)c[11];
     S.n_walk_pairs = (int64_t)c[12];
+    S.n_tiles_culled = (int64_t)c[13];
+    S.n_pairs_masked = (int64_t)c[14];
     if (N > 0 && m->G > 0) {
       std::vector<double> rs(N);
       cudaMemcpy(rs.data(), m->rowsum.ptr, sizeof(double) * N, cudaMemcpyDeviceToHost);

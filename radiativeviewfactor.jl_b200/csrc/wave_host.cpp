@@ -133,6 +133,47 @@ int wave_prepare(Session* s, rvf_mesh* m, Tables* T, const rvf_options* o, uint8
     x.delta = (float)std::ldexp(m->extent, -20);
     x.ray_log = a.ray_log; x.log_pm = a.log_pm;
   }
+  // Tile classes: which pairs' shadow rays may be blocked, which tiles are
+  // near field (kernels_cull.cu); recomputed by every solve.
+  if (!o->disable_tile_cull && N > 0) {
+    int rc = 0;
+    const size_t nt = (size_t)a.n_tiles;
+    if (T->tcls.bytes < nt && (rc = T->tcls.alloc(s, nt))) return rc;
+    if (T->tmask.bytes < nt * kTile * sizeof(uint32_t) && (rc = T->tmask.alloc(s, nt * kTile * sizeof(uint32_t))))
+      return rc;
+    TileClassArgs c{};
+    c.N = N;
+    c.nT = a.nT;
+    c.n_tiles = a.n_tiles;
+    c.cen = a.cen;
+    c.rad = a.rad;
+    c.diam = T->diam.as<double>();
+    c.group = a.group;
+    c.near_factor = w.mixed ? o->near_field_factor : -1.0;
+    c.tiny_gap = std::ldexp(m->extent, -16);
+    c.cull_margin = a.cull_margin;
+    c.occ = occ;
+    c.dim3 = w.dim3;
+    if (occ && w.dim3) {
+      c.nodesf = m->nodesf.as<NodeF>();
+      c.n_nodes = m->n_nodes;
+      c.frontier = m->frontier.as<int32_t>();
+      c.n_frontier = m->n_frontier;
+      c.leaf_of = m->leaf_of.as<int32_t>();
+      c.sat = o->geometric_soup ? m->sat_geo.as<float4>() : m->sat_ref.as<float4>();
+      c.sat_em = m->sat_em;
+    }
+    c.cls = T->tcls.as<uint8_t>();
+    c.mask = T->tmask.as<uint32_t>();
+    c.counters = s->counters.as<unsigned long long>() + 13;
+    const cudaError_t e = launch_tile_class(c, s->sm_count, s->stream);
+    if (e != cudaSuccess) return cuda_err(e, "tile classification launch");
+    if (n_kernels) *n_kernels += 1;
+    a.tcls = c.cls;
+    a.tmask = c.mask;
+    w.ma.tcls = c.cls;
+    w.ma.tmask = c.mask;
+  }
   TraceArgs& ta = w.ta;
   ta.N = N; ta.pmax = a.pmax; ta.dim3 = a.dim3; ta.tab = a.tab; ta.tabf = w.ma.tabf; ta.cen = a.cen;
   ta.group = a.group; ta.orig = a.orig; ta.nodes = a.nodes; ta.nodesf = occ ? m->nodesf.as<NodeF>() : nullptr; ta.n_nodes = a.n_nodes;
