@@ -244,15 +244,22 @@ def run_reference(args):
     rvf = load_pkg()
     W = workload(rvf, args.size)
     md, desc = W.md, W.desc
-    samples = []
+    # each step is a bounded row sample, sized so that the whole run (warm-up
+    # included) takes about ref_total seconds
+    per_step = min(args.ref_seconds, args.ref_total / max(1, args.warmup + args.steps))
+    samples, step_s = [], []
     for k in range(args.warmup + args.steps):
-        r = cpu_baseline(rvf, W, args.ref_seconds, offset=k * 7919)
+        t0 = time.perf_counter()
+        r = cpu_baseline(rvf, W, per_step, offset=k * 7919)
         if k >= args.warmup:
             samples.append(r)
+            step_s.append(time.perf_counter() - t0)
     v = statistics.median(s["value"] for s in samples)
     N = md.n_elems
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * (N * (N - 1) / 2) / v,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * statistics.mean(step_s),
+            "step": "one bounded row sample of the workload (calibration rows, then the timed rows)",
+            "ms_full_workload_projected": 1000.0 * (N * (N - 1) / 2) / v,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": desc, "n_elems": N, "nquad": W.nquad},
             "cpu_baseline": {**samples[-1], "value": v},
@@ -336,13 +343,11 @@ def roof_for(W: Workload, stats, prec, size, peak64, peak32):
 
 
 def phases(stats):
-    keys = ("ms_gen", "ms_trace", "ms_lists", "ms_trace_fp64", "ms_resolve", "ms_duffy", "ms_pairs", "ms_prep",
-            "ms_reduce")
+    keys = ("ms_cull", "ms_gen", "ms_trace", "ms_lists", "ms_trace_fp64", "ms_resolve", "ms_duffy", "ms_pairs",
+            "ms_prep", "ms_reduce")
     d = {k: statistics.mean(s[k] for s in stats) for k in keys}
-    d["n_chunks"] = int(stats[-1]["n_chunks"])
-    d["n_rays_traced"] = int(stats[-1]["n_rays_traced"])
-    d["n_list_pairs"] = int(stats[-1]["n_list_pairs"])
-    d["n_walk_pairs"] = int(stats[-1]["n_walk_pairs"])
+    for k in ("n_chunks", "n_rays_traced", "n_list_pairs", "n_walk_pairs", "n_tiles_culled", "n_pairs_masked"):
+        d[k] = int(stats[-1][k])
     return d
 
 
@@ -538,6 +543,88 @@ def run_serve(rvf, sess, size: str, local: int):
     }
 
 
+class _DeviceMatrix:
+    """A column-major N x N FP64 matrix at a device address, seen by torch
+    through the CUDA array interface (no copy)."""
+
+    def __init__(self, ptr: int, n: int):
+        self.__cuda_array_interface__ = {"shape": (n, n), "typestr": "<f8", "data": (int(ptr), True),
+                                         "version": 3, "strides": (8, 8 * n)}
+
+
+def device_rows_cols(ptr, N, idx, local):
+    """Rows F[i, :] and columns F[:, i] of the device F for the sampled i."""
+    import ctypes
+    import torch
+    addr = ctypes.cast(ptr, ctypes.c_void_p).value
+    F = torch.as_tensor(_DeviceMatrix(addr, N), device=f"cuda:{local}")
+    ii = torch.as_tensor(idx, dtype=torch.int64, device=f"cuda:{local}")
+    rows = F.index_select(0, ii).cpu().numpy()
+    cols = F.index_select(1, ii).cpu().numpy().T.copy()
+    return rows, cols
+
+
+def oracle_sample(W: Workload, stride: int):
+    """The oracle's raw values on sampled rows of the workload (the rows
+    i = 0, stride, 2 stride, ...): (rows, raw[rows, :] as rows x N, areas,
+    seconds).  Quadrature: every pair of the row as the reference's GPU path
+    integrates it, Duffy pairs replaced by the oracle's Sauter-Schwab
+    integrals; Monte Carlo: the reference's streams for the pairs (i, j > i)."""
+    import numpy as np
+    if str(ROOT) not in sys.path:
+        sys.path.insert(0, str(ROOT))
+    from oracle import pyoracle as orc
+    m = orc.Mesh(W.md, W.obs)
+    N = W.md.n_elems
+    rows = np.arange(0, N, stride, dtype=np.int64)
+    t0 = time.perf_counter()
+    if W.method == "mc":
+        raw, area, _, _ = orc.solve_mc(m, W.n_samples, W.seed, row_stride=stride, threads=os.cpu_count() or 1)
+        out = raw[rows, :].copy()
+        del raw
+    else:
+        out, area, _ = orc.solve_rows(m, W.nquad, rows, threads=os.cpu_count() or 1)
+        if W.use_duffy:
+            for r, i in enumerate(rows):
+                for j in range(N):
+                    if j == i:
+                        continue
+                    a, b = (int(i), j) if i < j else (j, int(i))
+                    if orc.singularity_type(m, a, b)[0] > 0:
+                        out[r, j] = orc.pair_duffy(m, a, b, W.nquad, None, gpu_semantics=True)[0]
+    return rows, out, area, time.perf_counter() - t0
+
+
+def compare_with_oracle(rows, raw, area, Frows, Fcols, mc):
+    """The device F against the oracle on the sampled rows (F[i, :] = raw / A_i)
+    and columns (F[:, i] = raw / A_j): largest absolute and relative element
+    difference, whether they are identical, the row-sum deviation and the
+    reciprocity A_i F_ij = A_j F_ji."""
+    import numpy as np
+    N = raw.shape[1]
+    with np.errstate(invalid="ignore", divide="ignore"):
+        Fo_r = raw / area[rows][:, None]
+        Fo_c = raw / area[None, :]
+    if mc:  # Monte Carlo rows hold the pairs j > i only
+        mask = np.arange(N)[None, :] > rows[:, None]
+    else:
+        mask = np.arange(N)[None, :] != rows[:, None]
+    d_r = np.abs(Frows - Fo_r)[mask]
+    d_c = np.abs(Fcols - Fo_c)[mask]
+    ref_r = np.abs(Fo_r)[mask]
+    ref_c = np.abs(Fo_c)[mask]
+    rel = max(float(np.max(d_r / np.maximum(ref_r, 1e-300))), float(np.max(d_c / np.maximum(ref_c, 1e-300))))
+    out = {"max_abs_dF": max(float(d_r.max()), float(d_c.max())), "max_rel_dF": rel,
+           "identical": bool(np.array_equal(Frows[mask], Fo_r[mask]) and np.array_equal(Fcols[mask], Fo_c[mask]))}
+    if not mc:
+        out["max_row_sum_dev"] = float(np.max(np.abs(np.where(mask, Frows, 0.0).sum(axis=1) -
+                                                     np.where(mask, Fo_r, 0.0).sum(axis=1))))
+        lhs, rhs = area[rows][:, None] * Frows, area[None, :] * Fcols
+        rec = np.abs(lhs - rhs)[mask] / np.maximum(np.abs(lhs)[mask], 1e-30)
+        out["max_reciprocity_err"] = float(rec.max())
+    return out
+
+
 def run_ours(args):
     ws, rank, local = dist_setup()
     rvf = load_pkg()
@@ -578,6 +665,19 @@ def run_ours(args):
                     "unsure_rays": {k: runs["mixed"]["stats"][-1][k] for k in
                                     ("unsure_rays", "unsure_slab", "unsure_prim", "unsure_direction")},
                     "graze_point_pairs": runs["mixed"]["stats"][-1]["graze_point_pairs"]}
+    vs_oracle = None
+    if rank == 0 and args.oracle_stride > 0:
+        stride = args.oracle_stride if args.size == "full" else max(1, min(args.oracle_stride, N // 32))
+        rows, raw, area, t_orc = oracle_sample(W, stride)
+        vs_oracle = {"rows": int(rows.size), "row_stride": int(stride), "oracle_s": t_orc,
+                     "pairs_checked": int(sum(N - 1 - i for i in rows) if W.method == "mc" else rows.size * (N - 1)),
+                     "what": "every stride-th row and column of the device F against the oracle's restatement of "
+                             "the reference's GPU path (Duffy pairs: its Sauter-Schwab integrals; Monte Carlo: "
+                             "its streams, pairs j > i)"}
+        for prec, dm in meshes.items():
+            Fr, Fc = device_rows_cols(dm.result_device(), N, rows, local)
+            vs_oracle[prec] = compare_with_oracle(rows, raw, area, Fr, Fc, W.method == "mc")
+        del raw
     for dm in meshes.values():
         dm.release()
     peak64 = _abi.fma_peak(local, True)
@@ -585,10 +685,9 @@ def run_ours(args):
     H = runs[head]
     roof = roof_for(W, H["stats"], head, args.size, peak64, peak32)
 
-    # ---- e2e: through the C ABI with host buffers ----
-    e2e = None
+    # ---- e2e: through the C ABI with host buffers, every precision ----
+    e2e_all = {}
     if not args.no_e2e:
-        opts = W.options(rvf, head)
         h2d = sum(a.nbytes for k, a in arrays.items() if hasattr(a, "nbytes")) + sum(t.nbytes for t in arrays["nodes"])
         d2h = 8 * (N * N + N + G * G + G)
         try:
@@ -599,22 +698,26 @@ def run_ours(args):
         A = np.empty(N)
         Fg = np.empty((G, G), order="F")
         Ag = np.empty(G)
-        times = []
-        for k in range(args.e2e_warmup + args.e2e_steps):
-            barrier(ws)
-            t0 = time.perf_counter()
-            d = _abi.DeviceMesh(sess, rvf.mesh_desc_arrays(md, W.obs))
-            d.solve(opts, F, A, Fg, Ag)
-            d.release()
-            t1 = time.perf_counter()
-            if k >= args.e2e_warmup:
-                times.append(t1 - t0)
-        t = allreduce_max(sum(times), ws)
-        e2e = {"value": job_rate(pairs * len(times), t, ws), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
-               "d2h_bytes_per_step": int(d2h), "host_buffer": "pinned" if pinned else "pageable",
-               "steps": len(times), "s_per_step": t / len(times), "precision": head}
+        for prec in precisions:
+            opts = W.options(rvf, prec)
+            times = []
+            for k in range(args.e2e_warmup + args.e2e_steps):
+                barrier(ws)
+                t0 = time.perf_counter()
+                d = _abi.DeviceMesh(sess, rvf.mesh_desc_arrays(md, W.obs))
+                d.solve(opts, F, A, Fg, Ag)
+                d.release()
+                t1 = time.perf_counter()
+                if k >= args.e2e_warmup:
+                    times.append(t1 - t0)
+            t = allreduce_max(sum(times), ws)
+            e2e_all[prec] = {"value": job_rate(pairs * len(times), t, ws), "unit": UNIT,
+                             "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+                             "host_buffer": "pinned" if pinned else "pageable", "steps": len(times),
+                             "s_per_step": t / len(times), "precision": prec}
         if pinned:
             Fh.free()
+    e2e = e2e_all.get(head)
 
     s0 = H["stats"][-1]
     line = {"metric": METRIC, "value": H["value"], "unit": UNIT, "n_gpus": ws, "steps": args.steps,
@@ -635,11 +738,14 @@ def run_ours(args):
                                           "prim_tests", "n_rays_traced")}}
     if len(precisions) == 2:
         line["fp64"] = {"value": runs["fp64"]["value"], "ms_per_step": runs["fp64"]["ms"],
+                        "e2e": e2e_all.get("fp64"),
                         "roofline": roof_for(W, runs["fp64"]["stats"], "fp64", args.size, peak64, peak32),
                         "phases": phases(runs["fp64"]["stats"]),
                         "clocks": runs["fp64"]["clocks"]}
         line["mixed_over_fp64"] = runs["mixed"]["value"] / runs["fp64"]["value"]
         line["accuracy"] = accuracy
+    if vs_oracle is not None:
+        line["accuracy"] = dict(line.get("accuracy") or {}, vs_oracle=vs_oracle)
     if rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(rvf, W, args.ref_seconds)
     if rank == 0 and args.serve != "none":
@@ -665,10 +771,14 @@ def main():
                          "c3: cylinder with Duffy pairs; c4: 2-D Monte Carlo cavity; medium / small: the headline "
                          "shape at m = 24 / 12")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--e2e-warmup", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ref-seconds", type=float, default=15.0)
+    ap.add_argument("--ref-total", type=float, default=150.0,
+                    help="--impl reference: seconds for the whole run (warm-up and timed samples)")
+    ap.add_argument("--oracle-stride", type=int, default=97,
+                    help="compare every stride-th row and column of the device F with the oracle (0: off)")
     ap.add_argument("--serve", choices=["none", "small", "medium", "full"], default="small",
                     help="serving stream reported beside the main line (small: 32 requests, 2k-8k elements; "
                          "medium: 128, 2k-20k; full: 512, 2k-40k)")

@@ -52,6 +52,7 @@ _SIG = {
     "orc_is_visible_cpu": (C.c_int, [_p, _pd, _pd, C.c_int]),
     "orc_solve_plain": (C.c_int, [C.POINTER(OrcMesh), C.c_int, C.c_int, C.c_int64, C.c_int64, C.c_int64, C.c_int,
                                   _pd, _pd, _pu8, C.c_int32, _pi64]),
+    "orc_solve_rows": (C.c_int, [C.POINTER(OrcMesh), C.c_int, C.c_int, _pi64, C.c_int64, C.c_int, _pd, _pd, _pi64]),
     "orc_self_gpu": (C.c_int, [C.POINTER(OrcMesh), C.c_int, C.c_int, _pd, _pd]),
     "orc_solve_mc": (C.c_int, [C.POINTER(OrcMesh), C.c_int, C.c_uint64, C.c_int, C.c_int, C.c_int64, C.c_int64,
                                C.c_int64, C.c_int, _pd, _pd, _pu8, _pi64]),
@@ -231,6 +232,19 @@ def solve_plain(mesh: Mesh, nquad, geometric=False, row_begin=0, row_end=None, r
                           row_stride, threads, _d(raw), _d(area),
                           None if log is None else log.ctypes.data_as(_pu8), pm, cnt.ctypes.data_as(_pi64))
     return raw, area, log, cnt
+
+
+def solve_rows(mesh: Mesh, nquad, rows, geometric=False, threads=0):
+    """raw[i, :] for each sampled element i (both i < j and j < i pairs, as
+    solve_plain integrates them) without the N x N matrix: (rows x N, area)."""
+    rows = np.ascontiguousarray(np.asarray(rows, dtype=np.int64))
+    N = mesh.N
+    out = np.zeros((rows.size, N))
+    area = np.zeros(N)
+    cnt = np.zeros(4, dtype=np.int64)
+    lib().orc_solve_rows(mesh.ref(), nquad, int(geometric), rows.ctypes.data_as(_pi64), rows.size, threads,
+                         _d(out), _d(area), cnt.ctypes.data_as(_pi64))
+    return out, area, cnt
 
 
 def self_gpu(mesh: Mesh, nquad, geometric=False):

@@ -28,6 +28,7 @@
 #include <cstring>
 #include <map>
 #include <mutex>
+#include <memory>
 #include <vector>
 #ifdef _OPENMP
 #include <omp.h>
@@ -346,6 +347,20 @@ double vf_kernel_2d(const double* xi, const double* ni, const double* xj, const 
 struct Pts {
   int np = 0;
   double x[256][3], n[256][3], dA[256], w[256];  // up to nquad = 16 (256 points)
+  const double* X(int p) const { return x[p]; }
+  const double* Nn(int p) const { return n[p]; }
+  double W(int p) const { return w[p]; }
+  double DA(int p) const { return dA[p]; }
+};
+// The same points of one element inside compact per-mesh arrays
+// (x, n: 3 per point; w, dA: 1 per point).
+struct PtsView {
+  int np = 0;
+  const double *x = nullptr, *n = nullptr, *w = nullptr, *dA = nullptr;
+  const double* X(int p) const { return x + 3 * p; }
+  const double* Nn(int p) const { return n + 3 * p; }
+  double W(int p) const { return w[p]; }
+  double DA(int p) const { return dA[p]; }
 };
 struct Rules {
   std::vector<double> qx, qe, qw, tx, te, tw, lx, lw;
@@ -739,6 +754,46 @@ inline int ray_blocked_gpu(const orc_bvh* bvh, const int32_t* pg, const double* 
   return orc_intersect_flat(bvh, pg, o, d, rlen, gi, gj, geometric, cnt);
 }
 
+// One pair i < j of src/GPUKernels.jl:276-310 (the double quadrature loop
+// with the shadow ray of each point pair with K > 0), or of
+// src/ViewFactorKernel.jl:199-241 on curve meshes; c: counters as in
+// orc_solve_plain; lg_pair (optional): the pair's ray log, stride pm.
+template <class PT>
+double pair_plain(const orc_mesh* m, const orc_bvh* bvh, const PT& Pi, const PT& Pj, int32_t gi, int32_t gj,
+                  int geometric, int64_t* c, uint8_t* lg_pair, int32_t pm) {
+  const bool two_d = (m->mesh_dim == 1);
+  double Fij = 0.0;
+  for (int p = 0; p < Pi.np; ++p) {
+    double inner = 0.0;
+    for (int q = 0; q < Pj.np; ++q) {
+      c[0]++;
+      uint8_t lg = 0;
+      double K;
+      if (two_d) {
+        K = vf_kernel_2d(Pi.X(p), Pi.Nn(p), Pj.X(q), Pj.Nn(q));
+        if (K > 0.0 && bvh) {
+          c[1]++;
+          int blk = orc_intersect_seg(bvh, m->obs_group, Pi.X(p), Pj.X(q), gi, gj);
+          lg = blk ? 2 : 1;
+          if (blk) K = 0.0;
+        }
+      } else {
+        K = vf_kernel(Pi.X(p), Pi.Nn(p), Pj.X(q), Pj.Nn(q));
+        if (bvh && K > 0.0) {
+          int64_t before = c[1];
+          int blk = ray_blocked_gpu(bvh, m->obs_group, Pi.X(p), Pj.X(q), gi, gj, geometric, c);
+          if (c[1] != before) lg = blk ? 2 : 1;
+          if (blk) K = 0.0;
+        }
+      }
+      if (lg_pair) lg_pair[p * pm + q] = lg;
+      inner += (Pj.W(q) * K) * Pj.DA(q);
+    }
+    Fij += (Pi.W(p) * inner) * Pi.DA(p);
+  }
+  return Fij;
+}
+
 }  // namespace
 
 extern "C" {
@@ -758,7 +813,6 @@ int orc_solve_plain(const orc_mesh* m, int nquad, int geometric, int64_t row_beg
     area[e] = (N >= 2) ? A : 0.0;  // area is only written by pair threads
   }
   orc_bvh* bvh = (m->n_obs > 0) ? orc_bvh_build(m->obs_soup, m->obs_nv, m->n_obs) : nullptr;
-  const bool two_d = (m->mesh_dim == 1);
   if (row_stride < 1) row_stride = 1;
   if (row_end > N) row_end = N;
   std::vector<int64_t> rows;
@@ -777,37 +831,85 @@ int orc_solve_plain(const orc_mesh* m, int nquad, int geometric, int64_t row_beg
       for (int64_t j = i + 1; j < N; ++j) {
         const Pts& Pj = P[j];
         int32_t gj = m->elem_group[j];
-        double Fij = 0.0;
-        for (int p = 0; p < Pi.np; ++p) {
-          double inner = 0.0;
-          for (int q = 0; q < Pj.np; ++q) {
-            c[0]++;
-            uint8_t lg = 0;
-            double K;
-            if (two_d) {
-              K = vf_kernel_2d(Pi.x[p], Pi.n[p], Pj.x[q], Pj.n[q]);
-              if (K > 0.0 && bvh) {
-                c[1]++;
-                int blk = orc_intersect_seg(bvh, m->obs_group, Pi.x[p], Pj.x[q], gi, gj);
-                lg = blk ? 2 : 1;
-                if (blk) K = 0.0;
-              }
-            } else {
-              K = vf_kernel(Pi.x[p], Pi.n[p], Pj.x[q], Pj.n[q]);
-              if (bvh && K > 0.0) {
-                int64_t before = c[1];
-                int blk = ray_blocked_gpu(bvh, m->obs_group, Pi.x[p], Pj.x[q], gi, gj, geometric, c);
-                if (c[1] != before) lg = blk ? 2 : 1;
-                if (blk) K = 0.0;
-              }
-            }
-            if (ray_log) ray_log[((i * N + j) * pm + p) * pm + q] = lg;
-            inner += (Pj.w[q] * K) * Pj.dA[q];
-          }
-          Fij += (Pi.w[p] * inner) * Pi.dA[p];
-        }
+        uint8_t* lg = ray_log ? ray_log + (i * N + j) * pm * pm : nullptr;
+        const double Fij = pair_plain(m, bvh, Pi, Pj, gi, gj, geometric, c, lg, pm);
         raw[i + j * N] = Fij;
         raw[j + i * N] = Fij;
+      }
+    }
+    std::lock_guard<std::mutex> lk(mu);
+    for (int k = 0; k < 4; ++k) tot[k] += c[k];
+  }
+  if (counters) for (int k = 0; k < 4; ++k) counters[k] = tot[k];
+  orc_bvh_free(bvh);
+  return 0;
+}
+
+// Whole rows of raw for the sampled elements rows[0..n_rows): out[r*N + j] =
+// raw[rows[r], j] (0 on the diagonal), each pair integrated as
+// orc_solve_plain integrates it (lower index first); the points live in
+// compact arrays, so large meshes fit.
+int orc_solve_rows(const orc_mesh* m, int nquad, int geometric, const int64_t* rows, int64_t n_rows, int n_threads,
+                   double* out, double* area, int64_t* counters) {
+  const int64_t N = m->n_elems;
+  Rules R = make_rules(nquad);
+  std::vector<int> npts(N);
+  std::vector<int64_t> off(N + 1, 0);
+  for (int64_t e = 0; e < N; ++e) {
+    const int f = m->family[e];
+    npts[e] = is_line_fam(f) ? (int)R.lx.size() : is_quad_fam(f) ? (int)R.qw.size() : (int)R.tw.size();
+    off[e + 1] = off[e] + npts[e];
+  }
+  std::vector<double> X(3 * off[N]), Nv(3 * off[N]), W(off[N]), DA(off[N]);
+  const int nt = threads_for(n_threads);
+#pragma omp parallel num_threads(nt)
+  {
+    std::unique_ptr<Pts> tmp(new Pts());
+#pragma omp for schedule(static)
+    for (int64_t e = 0; e < N; ++e) {
+      element_points(m, e, R, *tmp);
+      for (int p = 0; p < tmp->np; ++p) {
+        for (int k = 0; k < 3; ++k) {
+          X[3 * (off[e] + p) + k] = tmp->x[p][k];
+          Nv[3 * (off[e] + p) + k] = tmp->n[p][k];
+        }
+        W[off[e] + p] = tmp->w[p];
+        DA[off[e] + p] = tmp->dA[p];
+      }
+      double A = 0.0;
+      for (int p = 0; p < tmp->np; ++p) A += tmp->w[p] * tmp->dA[p];
+      area[e] = (N >= 2) ? A : 0.0;
+    }
+  }
+  auto view = [&](int64_t e) {
+    PtsView v;
+    v.np = npts[e];
+    v.x = X.data() + 3 * off[e];
+    v.n = Nv.data() + 3 * off[e];
+    v.w = W.data() + off[e];
+    v.dA = DA.data() + off[e];
+    return v;
+  };
+  orc_bvh* bvh = (m->n_obs > 0) ? orc_bvh_build(m->obs_soup, m->obs_nv, m->n_obs) : nullptr;
+  constexpr int64_t kBlock = 256;
+  const int64_t nb = (N + kBlock - 1) / kBlock;
+  int64_t tot[4] = {0, 0, 0, 0};
+  std::mutex mu;
+#pragma omp parallel num_threads(nt)
+  {
+    int64_t c[4] = {0, 0, 0, 0};
+#pragma omp for schedule(dynamic, 1)
+    for (int64_t w = 0; w < n_rows * nb; ++w) {
+      const int64_t r = w / nb, j0 = (w % nb) * kBlock, j1 = std::min<int64_t>(N, j0 + kBlock);
+      const int64_t i = rows[r];
+      for (int64_t j = j0; j < j1; ++j) {
+        if (j == i) {
+          out[r * N + j] = 0.0;
+          continue;
+        }
+        const int64_t a = std::min(i, j), b = std::max(i, j);
+        out[r * N + j] = pair_plain(m, bvh, view(a), view(b), m->elem_group[a], m->elem_group[b], geometric, c,
+                                    (uint8_t*)nullptr, 0);
       }
     }
     std::lock_guard<std::mutex> lk(mu);

@@ -103,6 +103,13 @@ int orc_solve_plain(const orc_mesh* m, int nquad, int geometric,
                     int64_t row_begin, int64_t row_end, int64_t row_stride, int n_threads,
                     double* raw, double* area, uint8_t* ray_log, int32_t pm, int64_t* counters);
 
+/* Whole rows of raw (both i < j and j < i pairs, each integrated as
+ * orc_solve_plain integrates it) for the sampled elements rows[0..n_rows):
+ * out[r*N + j] = raw[rows[r], j], 0 on the diagonal; area as orc_solve_plain.
+ * Points live in compact arrays (large meshes fit). */
+int orc_solve_rows(const orc_mesh* m, int nquad, int geometric, const int64_t* rows, int64_t n_rows,
+                   int n_threads, double* out, double* area, int64_t* counters);
+
 /* Self pairs (i, i), which the reference integrates on its CPU path only
  * (self_vf, src/Assembly.jl:173,193), with the GPU path's arithmetic of
  * orc_solve_plain: the same points, kernel, summation order and shadow rays

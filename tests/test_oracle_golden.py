@@ -222,3 +222,17 @@ def test_gpu_kernel_semantics_linear_families(orc):
     raw, area, _, _ = orc.solve_plain(m, 6)
     assert abs(area[0] - 1.0) < 1e-9
     assert abs(raw[0, 1] / area[0] - ANALYTIC_PLATES) < 2e-4
+
+
+@pytest.mark.parametrize("geometric", [False, True])
+def test_oracle_rows_equal_full_solve(rvf, orc, geometric):
+    """orc_solve_rows (the row sample the full-size parity checks use) equals
+    the full solve's rows bit for bit, for pairs below and above the row."""
+    md = rvf.meshes.cube_enclosure(6, box_m=3)
+    m = orc.Mesh(md, [7])
+    raw, area, _, _ = orc.solve_plain(m, 3, geometric=geometric)
+    rows = [0, 5, 77, 200, md.n_elems - 1]
+    out, area2, _ = orc.solve_rows(m, 3, rows, geometric=geometric)
+    assert np.array_equal(area, area2)
+    for r, i in enumerate(rows):
+        assert np.array_equal(out[r], raw[i]), i
