@@ -114,8 +114,14 @@ typedef struct {
                                  (src/Assembly.jl:173,193, j_start = self_vf ? i : i + 1); quadrature only */
   int32_t disable_tile_cull;  /* 1: no tile classification -- every shadow ray goes through the ray pipeline
                                  and every tile through its generation loop (same view factors; for testing) */
-  int32_t reserved[5];
+  int32_t fault_inject;       /* test hooks, 0 in production: RVF_FAULT_* bits */
+  int32_t reserved[4];
 } rvf_options;
+
+/* fault_inject bits (failure-path tests; each injects one host-visible failure
+ * and leaves the session usable for the next call) */
+#define RVF_FAULT_CLAIM 1 /* the pair pipeline's tile claims get no retries: every claim gives up -> RVF_ETIMEDOUT */
+#define RVF_FAULT_ALLOC 2 /* the first device allocation of this call fails -> RVF_ENOMEM */
 
 typedef struct {
   double ms_upload;       /* host->device of the mesh description */

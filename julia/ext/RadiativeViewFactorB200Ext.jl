@@ -66,7 +66,8 @@ struct RvfOptions
     disable_pair_lists::Int32
     self_vf::Int32
     disable_tile_cull::Int32
-    reserved::NTuple{5,Int32}
+    fault_inject::Int32
+    reserved::NTuple{4,Int32}
 end
 
 struct RvfStats

@@ -21,6 +21,7 @@ STATUS_NAMES = {0: "RVF_OK", -1: "RVF_EINVAL", -2: "RVF_ENOMEM", -3: "RVF_EBUDGE
 globals().update({name: code for code, name in STATUS_NAMES.items()})  # RVF_EINVAL, ...
 
 METHOD_QUADRATURE, METHOD_MONTE_CARLO = 0, 1
+FAULT_CLAIM, FAULT_ALLOC = 1, 2  # rvf_options.fault_inject test hooks
 PREC_FP64, PREC_MIXED = 0, 1
 
 _p = C.c_void_p
@@ -47,7 +48,8 @@ class Options(C.Structure):
                 ("seed", C.c_uint64), ("precision", C.c_int32), ("occlusion", C.c_int32),
                 ("geometric_soup", C.c_int32), ("mc_exclude_groups", C.c_int32), ("near_field_factor", C.c_double),
                 ("ray_log", _pu8), ("ray_log_pm", C.c_int32), ("disable_pair_lists", C.c_int32),
-                ("self_vf", C.c_int32), ("disable_tile_cull", C.c_int32), ("reserved", C.c_int32 * 5)]
+                ("self_vf", C.c_int32), ("disable_tile_cull", C.c_int32), ("fault_inject", C.c_int32),
+                ("reserved", C.c_int32 * 4)]
 
 
 class Stats(C.Structure):

@@ -86,6 +86,8 @@ int DevBuf::alloc(Session* s, size_t n) {
   if (s->used + n > s->budget)
     return set_err(RVF_EBUDGET, "HBM budget exceeded: need %zu more bytes, %zu of %zu in use", n, s->used,
                    s->budget);
+  if (s->fail_alloc_in > 0 && --s->fail_alloc_in == 0)
+    return set_err(RVF_ENOMEM, "cudaMalloc(%zu) failed: injected allocation failure (fault_inject)", n);
   cudaError_t e = cudaMalloc(&ptr, n);
   if (e != cudaSuccess) {
     cudaGetLastError();

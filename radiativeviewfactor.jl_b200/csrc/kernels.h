@@ -269,6 +269,7 @@ struct GenBatch {
   int n_req;
   int pmax_max;            // shared-memory layout and queue reservation
   int64_t total_tiles;
+  int claim_retries;       // compare-and-swap attempts of a tile claim before it gives up
   WaveQ q;
   unsigned long long* counters;
   int* err;

@@ -155,16 +155,22 @@ __device__ __forceinline__ void resv_release(const WaveQ& q, unsigned long long 
 // tile, or -1 when the chunk's queues have no room for another tile or every
 // tile is claimed.  The reservation is a compare-and-swap that only succeeds
 // when both capacities hold, so concurrent claims never over-reserve; the
-// retry loop is bounded (a block that keeps losing the race ends its chunk).
+// retry loop is bounded (a block that keeps losing the race ends its chunk
+// and raises kErrClaimGaveUp, which the host turns into RVF_ETIMEDOUT only
+// when a whole chunk claimed nothing).
 __device__ __forceinline__ int64_t claim_tile(const WaveQ& q, int64_t n_tiles, bool occ,
-                                              unsigned long long need, unsigned long long need_s) {
+                                              unsigned long long need, unsigned long long need_s, int retries,
+                                              int* err) {
   if (occ) {
     unsigned long long* c = q.ctr + kCtrResv;
     unsigned long long cur = *(volatile unsigned long long*)c;
-    bool ok = false;
-    for (int it = 0; it < 4096; ++it) {
+    bool ok = false, full = false;
+    for (int it = 0; it < retries; ++it) {
       const unsigned long long recs = cur & ((1ull << 38) - 1), slots = cur >> 38;
-      if (recs + need > (unsigned long long)q.cap || slots + need_s > (unsigned long long)q.scap) break;
+      if (recs + need > (unsigned long long)q.cap || slots + need_s > (unsigned long long)q.scap) {
+        full = true;
+        break;
+      }
       const unsigned long long prev = atomicCAS(c, cur, cur + resv_pack(need, need_s));
       if (prev == cur) {
         ok = true;
@@ -172,7 +178,10 @@ __device__ __forceinline__ int64_t claim_tile(const WaveQ& q, int64_t n_tiles, b
       }
       cur = prev;
     }
-    if (!ok) return -1;
+    if (!ok) {
+      if (!full) atomicOr(err, kErrClaimGaveUp);
+      return -1;
+    }
   }
   const int64_t t = (int64_t)atomicAdd(q.ctr + kCtrTile, 1ull);
   if (t >= n_tiles) {
@@ -475,7 +484,7 @@ __global__ void __launch_bounds__(256, 2) k_gen_fp64(const GenBatch* __restrict_
   uint32_t n_rays = 0, n_pp = 0;
   for (;;) {
     if (threadIdx.x == 0) {
-      const int64_t g = claim_tile(Q, L.total_tiles, OCC, need, need_s);
+      const int64_t g = claim_tile(Q, L.total_tiles, OCC, need, need_s, L.claim_retries, L.err);
       s_used = 0;
       s_slots = 0;
       s_tile = -1;
@@ -714,7 +723,7 @@ __global__ void __launch_bounds__(256, 2) k_gen_mixed(const GenBatch* __restrict
   uint32_t n_pp = 0, n_rays = 0, n_rays64 = 0, n_near = 0, n_graze = 0, n_baddir = 0;
   for (;;) {
     if (threadIdx.x == 0) {
-      const int64_t g = claim_tile(Q, L.total_tiles, OCC, need, need_s);
+      const int64_t g = claim_tile(Q, L.total_tiles, OCC, need, need_s, L.claim_retries, L.err);
       s_used = 0;
       s_slots = 0;
       s_tile = -1;

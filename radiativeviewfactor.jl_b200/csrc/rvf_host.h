@@ -39,6 +39,7 @@ HostBVH build_bvh(const double* soup, int nv, int64_t n_prims);
 // error flags raised by kernels (bit mask, read by the host after a launch)
 constexpr int kErrWaitTimeout = 1;
 constexpr int kErrBadInput = 2;
+constexpr int kErrClaimGaveUp = 4;  // a tile claim ran out of retries (not an error unless nothing progressed)
 
 constexpr int kTile = 32;      // elements per tile side
 constexpr int kComp = 7;       // x, y, z, nx, ny, nz, w*dA per quadrature point

@@ -63,6 +63,7 @@ struct rvf_session {
   cudaStream_t stream = nullptr;
   cudaStream_t copy_stream = nullptr;  // downloads of finished F columns while later chunks compute
   size_t budget = 0, used = 0;
+  int fail_alloc_in = 0;  // test hook: the n-th cudaMalloc from now fails once (0 = never)
   int sm_count = 0;
   size_t smem_optin = 0;
   std::mutex mu;
@@ -136,6 +137,7 @@ int ensure_tables(Session* s, rvf_mesh* m, int nquad, Tables** out);
 // solve.cpp helpers shared with the serving loop (callers hold s->mu)
 int read_err(Session* s);
 int validate_options(const rvf_mesh* m, const rvf_options* o);
+int no_progress(Session* s);
 int run_reduce(Session* s, rvf_mesh* m, const double* area);
 // The self pairs (i, i) of a quadrature solve with the pipeline's FP64
 // arguments, counted in the session's counters.

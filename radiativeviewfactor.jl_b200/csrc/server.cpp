@@ -327,7 +327,7 @@ void run_chunk(rvf_server* sv, std::vector<Req*>& batch) {
       }
     }
     if (!rc && pp == 0) {  // the queues could not take one tile: fail the batch rather than spin
-      rc = set_err(RVF_ENOMEM, "pair pipeline made no progress: ray queue too small for one tile");
+      rc = no_progress(s);
       for (Req* r : batch) {
         finish(sv, r, RVF_REQ_FAILED, rc);
         drop_device(sv, r);

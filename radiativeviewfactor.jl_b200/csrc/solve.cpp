@@ -52,6 +52,15 @@ int read_err(Session* s) {
   return RVF_OK;
 }
 
+// A chunk that claimed no tile: its claims either gave up after their
+// bounded retries (RVF_ETIMEDOUT) or found no queue room for one tile.
+int no_progress(Session* s) {
+  int herr = 0;
+  if (cudaMemcpy(&herr, s->err.ptr, sizeof(int), cudaMemcpyDeviceToHost) == cudaSuccess && (herr & kErrClaimGaveUp))
+    return set_err(RVF_ETIMEDOUT, "pair pipeline made no progress: every tile claim gave up after its bounded retries");
+  return set_err(RVF_ENOMEM, "pair pipeline made no progress: ray queue too small for one tile");
+}
+
 int validate_options(const rvf_mesh* m, const rvf_options* o) {
   if (o->nquad < 1) return set_err(RVF_EINVAL, "nquad must be >= 1, got %d", o->nquad);
   if (o->method != RVF_METHOD_QUADRATURE && o->method != RVF_METHOD_MONTE_CARLO)
@@ -63,6 +72,8 @@ int validate_options(const rvf_mesh* m, const rvf_options* o) {
   if (o->method == RVF_METHOD_MONTE_CARLO && o->n_samples < 1)
     return set_err(RVF_EINVAL, "n_samples must be >= 1");
   if (o->ray_log && o->ray_log_pm < 1) return set_err(RVF_EINVAL, "ray_log needs ray_log_pm >= 1");
+  if (o->fault_inject & ~(RVF_FAULT_CLAIM | RVF_FAULT_ALLOC))
+    return set_err(RVF_EINVAL, "unknown fault_inject bits 0x%x", o->fault_inject);
   if (o->self_vf != 0 && o->self_vf != 1) return set_err(RVF_EINVAL, "self_vf must be 0 or 1, got %d", o->self_vf);
   if (o->self_vf && o->method == RVF_METHOD_MONTE_CARLO)
     return set_err(RVF_EINVAL, "self_vf is supported with quadrature only");
@@ -419,6 +430,12 @@ int rvf_solve(rvf_session* s, rvf_mesh* m, const rvf_options* o, double* F_elem,
   cudaSetDevice(s->device);
   int rc = validate_options(m, o);
   if (rc) return rc;
+  // test hook: the first device allocation of this call fails; disarmed on return
+  struct FaultGuard {
+    Session* s;
+    ~FaultGuard() { s->fail_alloc_in = 0; }
+  } fault_guard{s};
+  s->fail_alloc_in = (o->fault_inject & RVF_FAULT_ALLOC) ? 1 : 0;
   const bool mc = (o->method == RVF_METHOD_MONTE_CARLO);
   // mixed precision covers quadrature on surface meshes; curve meshes and
   // Monte Carlo (which reproduces the reference's streams) run in FP64
@@ -516,7 +533,7 @@ int rvf_solve(rvf_session* s, rvf_mesh* m, const rvf_options* o, double* F_elem,
       S.ms_resolve += ci.ms_resolve;
       S.ms_lists += ci.ms_lists;
       S.n_rays_traced += ci.rays_traced;
-      if (w.claimed == before) return set_err(RVF_ENOMEM, "pair pipeline made no progress: ray queue too small for one tile");
+      if (w.claimed == before) return no_progress(s);
     }
     w_tiles = w.claimed;
     if (o->self_vf) {  // the pairs (i, i), before Duffy (which replaces the Quad8 ones)

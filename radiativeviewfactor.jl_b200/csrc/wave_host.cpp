@@ -86,6 +86,7 @@ int wave_prepare(Session* s, rvf_mesh* m, Tables* T, const rvf_options* o, uint8
   w.occ = occ;
   w.dim3 = (m->dim == 2);
   w.pmax = T->pmax;
+  if (o->fault_inject & RVF_FAULT_CLAIM) w.claim_retries = 0;
   PairArgs& a = w.pa;
   a.N = N;
   a.nT = (N + kTile - 1) / kTile;
@@ -319,6 +320,8 @@ int wave_chunk(Session* s, WaveReq* const* reqs_in, int n_in, bool use_graph, Ch
   g.n_req = n;
   g.pmax_max = sh.pmax_max;
   g.total_tiles = base[n];
+  g.claim_retries = reqs[0]->claim_retries;
+  for (int r = 1; r < n; ++r) g.claim_retries = std::min(g.claim_retries, reqs[r]->claim_retries);
   g.q = q;
   g.counters = s->counters.as<unsigned long long>();
   g.err = s->err.as<int>();

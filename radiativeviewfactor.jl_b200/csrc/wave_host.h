@@ -18,6 +18,7 @@ struct WaveReq {
   int pmax = 0;
   int64_t n_tiles = 0;  // upper-triangle tiles of the mesh
   int64_t claimed = 0;  // tiles integrated so far
+  int claim_retries = 4096;  // compare-and-swap attempts of a tile claim (0: every claim gives up)
   const NodeD* nodes_d = nullptr;
   const NodeF* nodes_f = nullptr;
   bool done() const { return claimed >= n_tiles; }
