@@ -369,6 +369,7 @@ struct McArgs {
   int n_nodes;
   const TriD* tris;
   const SegD* segs;
+  double cand_margin;  // curves: distance beyond which rounding cannot let a segment block a ray
   unsigned long long* tile_counter;
   unsigned long long* counters;
   uint8_t* ray_log;  // [(i*N + j) * n_samples + k] for caller indices i < j

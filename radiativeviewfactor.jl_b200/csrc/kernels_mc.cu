@@ -92,6 +92,127 @@ __device__ __forceinline__ void mc_coords(bool dim3, int k, int s, uint64_t& st,
   }
 }
 
+// ---------------------------------------------------------------------------
+// Curves with occlusion: per-pair candidate segments.
+//
+// The reference walks the whole segment tree for every sample ray, testing a
+// node when the ray's bounding box overlaps it (src/BVH.jl:285-322).  A
+// segment blocks a ray only if the computed test puts their intersection
+// inside both, which (rounding included) needs the segment within
+// cand_margin of the ray; and every ray of pair (i, j) lies within
+// R = max(r_i, r_j) of the segment between the elements' centres (each
+// element's points lie within r of its centre).  So one walk per pair with
+// that capsule finds every segment that can block any of the pair's rays;
+// each sample then tests only these, each behind the overlap test of its own
+// leaf (the walk's test at that leaf: the leaf box lies inside every
+// ancestor's, so the test passing there means the reference's walk reaches
+// it), with the reference's own segment test.  Decisions are identical to
+// the full walk's.  Pairs with more than kMcCand candidates walk the tree
+// for every sample as before.
+// ---------------------------------------------------------------------------
+constexpr int kMcCand = 24;
+
+// Centre and radius of a Line3 / Line2 element: the quadratic curve lies in
+// the triangle of its end nodes and its Bezier middle control point
+// 2 x_mid - (x_a + x_b) / 2; a Line2 between its ends.
+__device__ __forceinline__ void line_bounds(const double* coords, const int32_t* en, int f, double* c, double& r) {
+  const double* a = coords + 3 * (int64_t)en[0];
+  const double* b = coords + 3 * (int64_t)en[1];
+  double p[3][2];
+  int n = 2;
+  p[0][0] = a[0]; p[0][1] = a[1];
+  p[1][0] = b[0]; p[1][1] = b[1];
+  if (f == 4) {
+    const double* m = coords + 3 * (int64_t)en[2];
+    p[2][0] = 2.0 * m[0] - 0.5 * (a[0] + b[0]);
+    p[2][1] = 2.0 * m[1] - 0.5 * (a[1] + b[1]);
+    n = 3;
+  }
+  c[0] = c[1] = 0.0;
+  for (int k = 0; k < n; ++k) {
+    c[0] += p[k][0] / n;
+    c[1] += p[k][1] / n;
+  }
+  r = 0.0;
+  for (int k = 0; k < n; ++k) r = fmax(r, hypot(p[k][0] - c[0], p[k][1] - c[1]));
+  r *= 1.0 + 1e-12;
+}
+
+// True when the box, grown by R, certainly misses the segment a -> b (x, y).
+__device__ __forceinline__ bool capsule2_misses_box(const double* a, const double* b, double R, const NodeD& nd) {
+  double te = 0.0, tx = 1.0;
+#pragma unroll
+  for (int c = 0; c < 2; ++c) {
+    const double lo = nd.lo[c] - R, hi = nd.hi[c] + R;
+    const double d = b[c] - a[c];
+    if (d == 0.0) {
+      if (a[c] < lo || a[c] > hi) return true;
+      continue;
+    }
+    const double inv = 1.0 / d;
+    const double t1 = (lo - a[c]) * inv, t2 = (hi - a[c]) * inv;
+    te = fmax(te, fmin(t1, t2));
+    tx = fmin(tx, fmax(t1, t2));
+  }
+  return te > tx;
+}
+
+__device__ __forceinline__ double point_seg_dist2(double px, double py, double ax, double ay, double bx, double by) {
+  const double ex = bx - ax, ey = by - ay;
+  const double L2 = ex * ex + ey * ey;
+  double t = L2 > 0.0 ? ((px - ax) * ex + (py - ay) * ey) / L2 : 0.0;
+  t = fmin(1.0, fmax(0.0, t));
+  const double dx = ax + t * ex - px, dy = ay + t * ey - py;
+  return dx * dx + dy * dy;
+}
+
+// Distance between the segments a-b and c-d in the plane (0 when they cross).
+__device__ __forceinline__ double seg_seg_dist(const double* a, const double* b, const double* c, const double* d) {
+  const double o1 = (b[0] - a[0]) * (c[1] - a[1]) - (b[1] - a[1]) * (c[0] - a[0]);
+  const double o2 = (b[0] - a[0]) * (d[1] - a[1]) - (b[1] - a[1]) * (d[0] - a[0]);
+  const double o3 = (d[0] - c[0]) * (a[1] - c[1]) - (d[1] - c[1]) * (a[0] - c[0]);
+  const double o4 = (d[0] - c[0]) * (b[1] - c[1]) - (d[1] - c[1]) * (b[0] - c[0]);
+  if (((o1 <= 0.0 && o2 >= 0.0) || (o1 >= 0.0 && o2 <= 0.0)) && ((o3 <= 0.0 && o4 >= 0.0) || (o3 >= 0.0 && o4 <= 0.0)))
+    return 0.0;
+  double m = point_seg_dist2(a[0], a[1], c[0], c[1], d[0], d[1]);
+  m = fmin(m, point_seg_dist2(b[0], b[1], c[0], c[1], d[0], d[1]));
+  m = fmin(m, point_seg_dist2(c[0], c[1], a[0], a[1], b[0], b[1]));
+  m = fmin(m, point_seg_dist2(d[0], d[1], a[0], a[1], b[0], b[1]));
+  return sqrt(m);
+}
+
+// The pair's candidate segments (index and leaf), or -1 when there are more
+// than kMcCand (then every sample walks the tree).
+__device__ int mc_candidates(const McArgs& a, const double* ca, const double* cb, double R, int32_t gx, int32_t gy,
+                             int* cand_seg, int* cand_leaf, TravCount& tc) {
+  const double Rm = R + a.cand_margin;
+  int n = 0, node = 0;
+  while (node < a.n_nodes) {
+    const NodeD nd = a.nodes[node];
+    ++tc.nodes;
+    if (capsule2_misses_box(ca, cb, Rm, nd)) {
+      node = nd.miss;
+      continue;
+    }
+    if (nd.b == 0) {
+      node = node + 1;
+      continue;
+    }
+    for (int k = nd.a; k < nd.a + nd.b; ++k) {
+      const SegD sg = a.segs[k];
+      if (sg.group == gx || sg.group == gy) continue;
+      const double s0[2] = {sg.x0, sg.y0}, s1[2] = {sg.x1, sg.y1};
+      if (seg_seg_dist(ca, cb, s0, s1) > Rm) continue;
+      if (n == kMcCand) return -1;
+      cand_seg[n] = k;
+      cand_leaf[n] = node;
+      ++n;
+    }
+    node = nd.miss;
+  }
+  return n;
+}
+
 }  // namespace
 
 // Area rule: one thread per caller-order element.
@@ -161,6 +282,15 @@ __global__ void __launch_bounds__(256, DIM3 ? 2 : RVF_MC2D_MIN_BLOCKS) k_pairs_m
       const int32_t gx = a.exclude ? g_lo : 0, gy = a.exclude ? g_hi : 0;
       uint64_t st = init_rng(a.seed, (uint64_t)(o_lo * N + o_hi + 1));
       uint8_t* logp = (a.ray_log && valid) ? a.ray_log + ((uint64_t)o_lo * N + o_hi) * a.n_samples : nullptr;
+      // curves with occlusion: the pair's candidate segments (one walk per pair)
+      int cand_seg[(!DIM3 && OCC) ? kMcCand : 1], cand_leaf[(!DIM3 && OCC) ? kMcCand : 1];
+      int ncand = -1;
+      if (!DIM3 && OCC && valid) {
+        double c_lo[2], c_hi[2], r_lo, r_hi;
+        line_bounds(a.coords, en_lo, f_lo, c_lo, r_lo);
+        line_bounds(a.coords, en_hi, f_hi, c_hi, r_hi);
+        ncand = mc_candidates(a, c_lo, c_hi, fmax(r_lo, r_hi), gx, gy, cand_seg, cand_leaf, tc);
+      }
       double Ks = 0.0;
       for (int k = 0; k < a.n_samples; ++k) {
         double ci[2], cj[2];
@@ -195,8 +325,20 @@ __global__ void __launch_bounds__(256, DIM3 ? 2 : RVF_MC2D_MIN_BLOCKS) k_pairs_m
             n_rays += cast ? 1 : 0;
             const double rxlo = fmin(xi[0], xj[0]), rxhi = fmax(xi[0], xj[0]);
             const double rylo = fmin(xi[1], xj[1]), ryhi = fmax(xi[1], xj[1]);
-            const bool blocked = packet_any_hit(
-                cast, a.nodes, a.n_nodes,
+            bool blocked = false;
+            if (cast && ncand >= 0) {
+              for (int c = 0; c < ncand && !blocked; ++c) {
+                const NodeD nd = a.nodes[cand_leaf[c]];
+                ++tc.nodes;
+                if (nd.lo[0] > rxhi || nd.hi[0] < rxlo || nd.lo[1] > ryhi || nd.hi[1] < rylo) continue;
+                ++tc.prims;
+                blocked = seg_blocks(a.segs[cand_seg[c]], xi, xj);
+              }
+            }
+            const bool walk = cast && ncand < 0;
+            if (__any_sync(kFull, walk)) {
+              const bool bw = packet_any_hit(
+                walk, a.nodes, a.n_nodes,
                 [&](const NodeD& nd) {
                   return !(nd.lo[0] > rxhi || nd.hi[0] < rxlo || nd.lo[1] > ryhi || nd.hi[1] < rylo);
                 },
@@ -207,6 +349,8 @@ __global__ void __launch_bounds__(256, DIM3 ? 2 : RVF_MC2D_MIN_BLOCKS) k_pairs_m
                   return seg_blocks(sg, xi, xj);
                 },
                 tc);
+              if (walk) blocked = bw;
+            }
             if (cast) lg = blocked ? 2 : 1;
             if (blocked) K = 0.0;
           }

@@ -108,6 +108,14 @@ void fill_mc_args(Session* s, rvf_mesh* m, const rvf_options* o, uint8_t* ray_lo
   c.n_nodes = occ ? m->n_nodes : 0;
   c.tris = occ ? (o->geometric_soup ? m->tris_geo.as<TriD>() : m->tris_ref.as<TriD>()) : nullptr;
   c.segs = occ ? m->segs.as<SegD>() : nullptr;
+  {
+    // a computed hit of the reference's segment test (src/BVH.jl:265-322:
+    // |den| >= 1e-8, parameters strictly inside (1e-8, 1 - 1e-8)) lies within
+    // about 2e-7 S^3 of both segments (S bounds every length), so a segment
+    // farther than this from a ray cannot block it
+    const double S = 2.0 * m->extent;
+    c.cand_margin = 1e-5 * S * S * S + std::ldexp(S, -16);
+  }
   c.tile_counter = s->tile_counter.as<unsigned long long>();
   c.counters = s->counters.as<unsigned long long>();
   c.ray_log = ray_log;
