@@ -115,6 +115,7 @@ uint64_t footprint_of(const rvf_mesh_desc* d, const rvf_options* o) {
   b += (uint64_t)std::max<int64_t>(d->n_obs, 0) * 400;                    // BVH nodes and primitives, both precisions
   b += (uint64_t)std::min<uint64_t>(256, std::max<uint64_t>(1, (1u << 20) / std::max<uint64_t>(N, 1))) * G * N * 8;
   b += (G * N + G * G + G + N) * 8;                                        // row-group, group and row sums
+  b += tiles * (tiles + 1) / 2 * (1 + kTile * 4);                          // tile classes and masks
   return b + (1u << 20);
 }
 

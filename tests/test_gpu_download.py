@@ -16,6 +16,9 @@ def test_chunked_solve_downloads_every_column(rvf, session, pinned, precision):
     md = rvf.meshes.cube_enclosure(16, box_m=6)
     N = md.n_elems
     o = rvf.make_options(3, seed=0, precision=precision)
+    # every ray through the queues (no tile classification), so that a small
+    # budget forces many chunks
+    o.disable_tile_cull = 1
     ref = np.empty((N, N), order="F")
     dm = _abi.DeviceMesh(session, rvf.mesh_desc_arrays(md, [7]))
     st_ref = dm.solve(o, ref)
