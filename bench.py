@@ -438,7 +438,7 @@ def run_serve(rvf, sess, size: str, local: int):
     # the served results of these are compared with plain FP64 solves
     check = [k for k in sample if not reqs[k]["mc"]][:4]
     F64 = {}
-    t_mixed, t_fp64, dF = 0.0, 0.0, 0.0
+    t_mixed, t_fp64, dF, t_solve_only = 0.0, 0.0, 0.0, 0.0
     t_kind = {False: 0.0, True: 0.0}
     for k in sample:
         r = reqs[k]
@@ -446,10 +446,20 @@ def run_serve(rvf, sess, size: str, local: int):
         dm.solve(r["opts"])  # warm (tables, queues)
         t0 = time.perf_counter()
         dm.solve(r["opts"])
+        t_solve_only += time.perf_counter() - t0
+        dm.release()
+        # one request served alone: upload, solve (result on the device), release --
+        # the work the server does per request
+        t0 = time.perf_counter()
+        dm = _abi.DeviceMesh(sess, arrays[k])
+        dm.solve(r["opts"])
+        dm.release()
         dt = time.perf_counter() - t0
+        dm = _abi.DeviceMesh(sess, arrays[k])
         t_mixed += dt
         t_kind[r["mc"]] += dt
         o64 = rvf.make_options(r["nquad"], monte_carlo=r["mc"], n_samples=64, seed=r["opts"].seed, precision="fp64")
+        dm.solve(o64)  # warm
         t0 = time.perf_counter()
         dm.solve(o64)
         t_fp64 += time.perf_counter() - t0
@@ -528,8 +538,13 @@ def run_serve(rvf, sess, size: str, local: int):
         "metric": "serve latency and throughput", "requests": n_req, "failed": len(err),
         "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "mean_ms": st["mean_ms"],
         "throughput_pairs_per_s": total_pairs / wall, "wall_s": wall,
-        "one_at_a_time_mixed_pairs_per_s": sample_pairs / t_mixed,
+        "one_at_a_time_pairs_per_s": sample_pairs / t_mixed,
+        "one_at_a_time": "each sampled request alone through the public API: mesh upload, solve with the "
+                         "request's options (result left on the device), release -- the work the server "
+                         "does per request",
+        "one_at_a_time_solve_only_pairs_per_s": sample_pairs / t_solve_only,
         "one_at_a_time_fp64_pairs_per_s": sample_pairs / t_fp64,
+        "burst_pairs_per_s": sum(pairs[k] for k in burst) / t_burst,
         "lambda_per_s": lam, "offered_load": 0.8, "estimated_service_s": est_service,
         "burst_s": t_burst, "burst_requests": len(burst),
         "max_abs_dF_vs_fp64_solo": dF, "checked_requests": len(check),

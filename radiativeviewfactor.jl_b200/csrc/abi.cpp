@@ -82,6 +82,18 @@ int DevBuf::alloc(Session* s, size_t n) {
       return RVF_OK;  // already charged to the budget
     }
   }
+  // Large buffers come in size classes 2^(1/4) apart (at most 19% spare), so
+  // that a freed one serves the next request of about the same size -- mesh
+  // after mesh of different element counts, as a serving stream sends them --
+  // instead of a cudaMalloc / cudaFree of gigabytes each time.
+  if (n >= kSpareMin) {
+    size_t c = kSpareMin;
+    while (c < n) {
+      const size_t next = (size_t)((double)c * 1.189207115002721);  // 2^(1/4)
+      c = (next + 4095) & ~(size_t)4095;
+    }
+    if (s->used + c <= s->budget || s->used + n > s->budget) n = c;  // the class when it fits the budget
+  }
   if (s->used + n > s->budget) release_spares(s);
   if (s->used + n > s->budget)
     return set_err(RVF_EBUDGET, "HBM budget exceeded: need %zu more bytes, %zu of %zu in use", n, s->used,

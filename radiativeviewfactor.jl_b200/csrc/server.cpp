@@ -108,7 +108,7 @@ uint64_t footprint_of(const rvf_mesh_desc* d, const rvf_options* o) {
   const uint64_t tiles = (N + kTile - 1) / kTile;
   const uint64_t pm = (uint64_t)pmax_of(d, o->nquad);
   const uint64_t G = (uint64_t)std::max(d->n_groups, 1);
-  uint64_t b = 8 * std::max<uint64_t>(N * N, 1);                          // F
+  uint64_t b = (uint64_t)(8.0 * 1.19 * (double)std::max<uint64_t>(N * N, 1));  // F, in its size class
   b += tiles * kTile * kComp * pm * 8;                                     // FP64 table
   if (o->precision == RVF_PREC_MIXED) b += tiles * kTile * kComp * pm * 4;  // FP32 table
   b += N * 256 + 24 * (uint64_t)std::max<int64_t>(d->n_nodes, 0);          // per-element arrays, coordinates
@@ -157,7 +157,7 @@ namespace {
 // and the oldest requests finish at short intervals (quadrature point pairs
 // of the mixed pipeline; Monte Carlo sample pairs, each of which evaluates
 // both elements' geometry).
-constexpr double kChunkPointPairs = 4e8;
+constexpr double kChunkPointPairs = 2e9;
 constexpr double kChunkSamplePairs = 1e8;
 
 const int kCand[][2] = {{0, 0}, {2, 0}, {0, 2}, {2, 2}};
