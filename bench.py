@@ -563,7 +563,7 @@ class _DeviceMatrix:
     through the CUDA array interface (no copy)."""
 
     def __init__(self, ptr: int, n: int):
-        self.__cuda_array_interface__ = {"shape": (n, n), "typestr": "<f8", "data": (int(ptr), True),
+        self.__cuda_array_interface__ = {"shape": (n, n), "typestr": "<f8", "data": (int(ptr), False),
                                          "version": 3, "strides": (8, 8 * n)}
 
 

@@ -42,10 +42,16 @@ def test_culled_cube_fp64(rvf, orc, session, geometric):
     F, A, st = solve(rvf, session, md, 3, [7], geometric=geometric)
     F0, A0, st0 = solve(rvf, session, md, 3, [7], cull=False, geometric=geometric)
     assert st["n_tiles_culled"] > 0 and st0["n_tiles_culled"] == 0
-    assert st["n_rays_traced"] < st0["n_rays_traced"]
     assert st["n_rays"] == st0["n_rays"]  # every cast ray is counted, traced or not
     assert np.array_equal(A, A0)
     assert_rel(F, F0, rtol=1e-12)
+    if geometric:
+        # true triangles cover the box: every ray through its box can hit one,
+        # so the masks keep exactly the rays the root-box test keeps
+        assert st["n_rays_traced"] == st0["n_rays_traced"]
+    else:
+        # the reference's transposed read leaves most of them unblockable
+        assert st["n_rays_traced"] < st0["n_rays_traced"] // 2
     m = orc.Mesh(md, [7])
     raw, area, _, _ = orc.solve_plain(m, 3, geometric=geometric, row_stride=37)
     assert np.array_equal(A, area)
