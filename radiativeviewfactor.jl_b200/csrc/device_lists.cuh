@@ -47,6 +47,42 @@ __device__ __forceinline__ bool pair_misses_tri(const float* a, const float* b, 
                         f1[0] * f2[1] - f1[1] * f2[0], rm);
 }
 
+// The same test over more separating axes: the coordinate axes first (the
+// cheapest and, for the long thin triangles the reference's transposed read
+// produces, often enough), then the segment direction crossed with each
+// edge, the normal, and each coordinate axis crossed with each edge.  Each
+// axis is a valid separation on its own (the capsule projects onto w as its
+// centroid segment widened by rm |w|), so more axes only drop more.
+__device__ __forceinline__ bool pair_misses_tri_full(const float* a, const float* b, const float* d, float R,
+                                                     float em, const float4& p0, const float4& p1,
+                                                     const float4& p2) {
+  const float rm = R + p0.w + em;
+  {
+    const float ax[3] = {a[0], a[1], a[2]}, bx[3] = {b[0], b[1], b[2]};
+    const float q0[3] = {p0.x, p0.y, p0.z}, q1[3] = {p1.x, p1.y, p1.z}, q2[3] = {p2.x, p2.y, p2.z};
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const float tlo = fminf(q0[k], fminf(q1[k], q2[k])), thi = fmaxf(q0[k], fmaxf(q1[k], q2[k]));
+      const float slo = fminf(ax[k], bx[k]), shi = fmaxf(ax[k], bx[k]);
+      if (tlo - shi > rm || slo - thi > rm) return true;
+    }
+  }
+  if (pair_misses_tri(a, b, d, R, em, p0, p1, p2)) return true;
+  const float f[3][3] = {{p1.x - p0.x, p1.y - p0.y, p1.z - p0.z},
+                         {p2.x - p0.x, p2.y - p0.y, p2.z - p0.z},
+                         {p2.x - p1.x, p2.y - p1.y, p2.z - p1.z}};
+#pragma unroll
+  for (int m = 0; m < 3; ++m)
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      float w[3] = {0.f, 0.f, 0.f};  // e_k x f_m
+      w[(k + 1) % 3] = -f[m][(k + 2) % 3];
+      w[(k + 2) % 3] = f[m][(k + 1) % 3];
+      if (axis_separates(a, b, p0, p1, p2, w[0], w[1], w[2], rm)) return true;
+    }
+  return false;
+}
+
 // The pair's capsule for the list walk, in FP32: the centroid segment's
 // start A and direction reciprocals (from FP64, rounded once), and the radius
 // grown by em.  A box test in FP32 (capsule_misses_box) then only reports a

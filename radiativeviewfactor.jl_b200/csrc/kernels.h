@@ -186,6 +186,7 @@ struct MixedArgs {
   double near_factor;
   const double* rad;
   double cull_margin;
+  double tiny_gap;  // pairs closer than rad_i + rad_j + tiny_gap run in FP64 (as near-field pairs)
   const int32_t* group;
   const int32_t* orig;
   double* F;

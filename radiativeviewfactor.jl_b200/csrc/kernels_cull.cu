@@ -162,10 +162,12 @@ __global__ void __launch_bounds__(kCullWarps * 32) k_tile_class(const TileClassA
   __shared__ int s_front[kCullWarps][2 * kListFront];
   __shared__ int s_leaf[kCullWarps][kTileLeaves];
   __shared__ int s_list[kCullWarps][kTileTris];
+  __shared__ int s_row[kCullWarps][kTileTris];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   int* front = s_front[warp];
   int* leaves = s_leaf[warp];
   int* list = s_list[warp];
+  int* rowl = s_row[warp];
   const int64_t N = a.N;
   uint32_t n_culled = 0, n_masked = 0;
   for (int64_t t = (int64_t)blockIdx.x * kCullWarps + warp; t < a.n_tiles; t += (int64_t)gridDim.x * kCullWarps) {
@@ -208,6 +210,8 @@ __global__ void __launch_bounds__(kCullWarps * 32) k_tile_class(const TileClassA
     uint8_t cls = (__any_sync(kFull, near) ? kClsNear : 0) | (__any_sync(kFull, tiny) ? kClsTiny : 0);
     bool all_ones = false;  // occlusion the tile cannot classify: every pair keeps its rays
     int nl = 0;             // listed triangles
+    HullF H;                // the tile's hull (occlusion, 3-D)
+    float rmaxJ = 0.0f;     // largest point radius of the column block
     if (a.occ && !a.dim3) {
       all_ones = true;
     } else if (a.occ) {
@@ -235,7 +239,10 @@ __global__ void __launch_bounds__(kCullWarps * 32) k_tile_class(const TileClassA
       // one group per block: its triangles are skipped by every ray of the tile
       const int32_t gi0 = __shfl_sync(kFull, gi, 0), gj0 = __shfl_sync(kFull, gj, 0);
       const bool g_same = __all_sync(kFull, (!oki || gi == gi0) && (!okj || gj == gj0));
-      HullF H;
+      double rj_max = rj;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) rj_max = fmax(rj_max, __shfl_xor_sync(kFull, rj_max, o));
+      rmaxJ = __double2float_ru(rj_max);
 #pragma unroll
       for (int b = 0; b < 2; ++b)
 #pragma unroll
@@ -314,7 +321,10 @@ __global__ void __launch_bounds__(kCullWarps * 32) k_tile_class(const TileClassA
       a.mask[t * kTile + lane] = 0xffffffffu;
       n_masked += 32;
     } else if (nl > 0) {
-      // per pair: some listed triangle survives the pair-list tests
+      // per pair: some listed triangle survives the pair-list tests.  Row by
+      // row, the warp first keeps the listed triangles the row's own hull
+      // (its centroid and the column block's box, radius max(rad_i, rad_J))
+      // can reach, 32 at a time, then each lane tests its pair against those.
       cls |= kClsSlow;
       for (int li = 0; li < kTile; ++li) {
         const int64_t i = bi * kTile + li;
@@ -322,17 +332,49 @@ __global__ void __launch_bounds__(kCullWarps * 32) k_tile_class(const TileClassA
                      x2 = __shfl_sync(kFull, ci[2], li);
         const double rr = __shfl_sync(kFull, ri, li);
         const int32_t g_i = __shfl_sync(kFull, gi, li);
-        const bool valid = okj && i < N && i < ej;
+        if (i >= N) {
+          if (lane == 0) a.mask[t * kTile + li] = 0u;
+          continue;
+        }
+        HullF Hr;
+        const double xr[3] = {x0, x1, x2};
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          const float l = __double2float_rd(xr[c]), h = __double2float_ru(xr[c]);
+          Hr.c[0][c] = 0.5f * (l + h);
+          Hr.h[0][c] = 0.5f * (h - l);
+          Hr.c[1][c] = H.c[1][c];
+          Hr.h[1][c] = H.h[1][c];
+          Hr.d[c] = Hr.c[1][c] - Hr.c[0][c];
+        }
+        const float Rr = fmaxf(__double2float_ru(rr), rmaxJ) + __double2float_ru(a.cull_margin);
+        int nr = 0;
+        for (int b = 0; b < nl; b += 32) {
+          const int e = b + lane;
+          bool keep = false;
+          int u = 0;
+          if (e < nl) {
+            u = list[e];
+            const float4 p0 = a.sat[3 * u], p1 = a.sat[3 * u + 1], p2 = a.sat[3 * u + 2];
+            const int32_t g = __float_as_int(p1.w);
+            keep = g != g_i && !hull_misses_box(Hr, a.nodesf[a.leaf_of[u]], Rr + a.sat_em) &&
+                   !hull_misses_tri(Hr, p0, p1, p2, Rr + p0.w + a.sat_em);
+          }
+          const uint32_t m = __ballot_sync(kFull, keep);
+          if (keep) rowl[nr + __popc(m & lanemask_lt())] = u;  // in list order, so grouped by leaf
+          nr += __popc(m);
+        }
+        __syncwarp();
+        const bool valid = okj && i < ej;
         CapsuleF cap{};
         float bf[3] = {0.f, 0.f, 0.f}, df[3] = {0.f, 0.f, 0.f};
         float Rf = 0.0f;
-        if (valid) {
+        if (valid && nr > 0) {
           const double R = fmax(rr, rj) + a.cull_margin;
-          const double A3[3] = {x0, x1, x2};
 #pragma unroll
           for (int c = 0; c < 3; ++c) {
-            const double dd = cj[c] - A3[c];
-            cap.A[c] = (float)A3[c];
+            const double dd = cj[c] - xr[c];
+            cap.A[c] = (float)xr[c];
             bf[c] = (float)cj[c];
             cap.zero[c] = dd == 0.0;
             cap.inv[c] = cap.zero[c] ? 0.0f : (float)(1.0 / dd);
@@ -345,9 +387,9 @@ __global__ void __launch_bounds__(kCullWarps * 32) k_tile_class(const TileClassA
         bool bit = false, done = !valid;
         int last = -1;
         bool lpass = false;
-        for (int e = 0; e < nl; ++e) {
+        for (int e = 0; e < nr; ++e) {
           if (__all_sync(kFull, done)) break;
-          const int u = list[e];
+          const int u = rowl[e];
           const int lf = a.leaf_of[u];
           if (lf != last) {
             last = lf;
@@ -356,12 +398,13 @@ __global__ void __launch_bounds__(kCullWarps * 32) k_tile_class(const TileClassA
           if (!done && lpass) {
             const float4 p0 = a.sat[3 * u], p1 = a.sat[3 * u + 1], p2 = a.sat[3 * u + 2];
             const int32_t g = __float_as_int(p1.w);
-            if (g != g_i && g != gj && !pair_misses_tri(cap.A, bf, df, Rf, a.sat_em, p0, p1, p2)) {
+            if (g != gj && !pair_misses_tri_full(cap.A, bf, df, Rf, a.sat_em, p0, p1, p2)) {
               bit = true;
               done = true;
             }
           }
         }
+        __syncwarp();
         const uint32_t m = __ballot_sync(kFull, bit);
         if (lane == 0) {
           a.mask[t * kTile + li] = m;

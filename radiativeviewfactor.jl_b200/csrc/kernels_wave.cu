@@ -247,7 +247,7 @@ __device__ __forceinline__ int find_req(const int64_t* tile_base, int n_req, int
 // Out of line: their registers are allocated apart from the ray pipeline's.
 // ---------------------------------------------------------------------------
 template <bool DIM3, bool OCC, int QB>
-__device__ __noinline__ void gen_fast_fp64(const PairArgs& a, const double* iblk, int64_t bi, int64_t bj, int warp,
+__device__ __noinline__ void gen_fast_fp64(const PairArgs& a, const double* iblk, int64_t bi, int64_t bj, int li0,
                                            int lane, uint32_t& n_pp, uint32_t& n_rays) {
   const int64_t N = a.N;
   const int pm = a.pmax;
@@ -256,8 +256,10 @@ __device__ __noinline__ void gen_fast_fp64(const PairArgs& a, const double* iblk
   const int64_t oj = jok ? (a.orig ? (int64_t)a.orig[j] : j) : 0;
   const int npj0 = jok ? a.np[j] : 0;
   const double* jb = a.tab + bj * kComp * pm * kTile + lane;
-  for (int rr = 0; rr < kTile / 8; ++rr) {
-    const int li = warp + 8 * rr;
+  // li0 < 8: the warp's rows li0, li0 + 8, ...; li0 >= 8: the single row li0 - 8
+  const int r_last = li0 < 8 ? kTile / 8 : 1;
+  for (int rr = 0; rr < r_last; ++rr) {
+    const int li = li0 < 8 ? li0 + 8 * rr : li0 - 8;
     const int64_t i = bi * kTile + li;
     if (i >= N) break;  // warp-uniform; later rows are further out
     const bool valid = jok && i < j;
@@ -371,7 +373,7 @@ __device__ __noinline__ void gen_fast_fp64(const PairArgs& a, const double* iblk
 // here: no ray depends on the sign of their K, and their FP32 error is that
 // of any other far-field term.
 template <bool OCC, int QB>
-__device__ __noinline__ void gen_fast_mixed(const MixedArgs& a, const float* iblk, int64_t bi, int64_t bj, int warp,
+__device__ __noinline__ void gen_fast_mixed(const MixedArgs& a, const float* iblk, int64_t bi, int64_t bj, int li0,
                                             int lane, uint32_t& n_pp, uint32_t& n_rays) {
   const int64_t N = a.N;
   const int pm = a.pmax;
@@ -381,8 +383,10 @@ __device__ __noinline__ void gen_fast_mixed(const MixedArgs& a, const float* ibl
   const int npj0 = jok ? a.np[j] : 0;
   const float* jbf = a.tabf + bj * kComp * pm * kTile + lane;
   const double cj0 = jok ? a.cen[3 * j] : 0.0, cj1 = jok ? a.cen[3 * j + 1] : 0.0, cj2 = jok ? a.cen[3 * j + 2] : 0.0;
-  for (int rr = 0; rr < kTile / 8; ++rr) {
-    const int li = warp + 8 * rr;
+  // li0 < 8: the warp's rows li0, li0 + 8, ...; li0 >= 8: the single row li0 - 8
+  const int r_last = li0 < 8 ? kTile / 8 : 1;
+  for (int rr = 0; rr < r_last; ++rr) {
+    const int li = li0 < 8 ? li0 + 8 * rr : li0 - 8;
     const int64_t i = bi * kTile + li;
     if (i >= N) break;  // warp-uniform
     const bool valid = jok && i < j;
@@ -445,6 +449,23 @@ __device__ __noinline__ void gen_fast_mixed(const MixedArgs& a, const float* ibl
       a.F[oi + oi * N] = 0.0 / a.area[i];
     }
   }
+}
+
+// The fast loop with the point block for the rule's size (li0 as there).
+template <bool DIM3, bool OCC>
+__device__ __forceinline__ void fast_fp64(const PairArgs& a, const double* iblk, int64_t bi, int64_t bj, int li0,
+                                          int lane, uint32_t& n_pp, uint32_t& n_rays) {
+  if (a.pmax <= 3) gen_fast_fp64<DIM3, OCC, 3>(a, iblk, bi, bj, li0, lane, n_pp, n_rays);
+  else gen_fast_fp64<DIM3, OCC, 4>(a, iblk, bi, bj, li0, lane, n_pp, n_rays);
+}
+template <bool OCC>
+__device__ __forceinline__ void fast_mixed(const MixedArgs& a, const float* iblk, int64_t bi, int64_t bj, int li0,
+                                           int lane, uint32_t& n_pp, uint32_t& n_rays) {
+  const int pm = a.pmax;
+  if (pm == 7 || pm == 13 || pm == 49) gen_fast_mixed<OCC, 7>(a, iblk, bi, bj, li0, lane, n_pp, n_rays);
+  else if (pm == 5 || pm == 25) gen_fast_mixed<OCC, 5>(a, iblk, bi, bj, li0, lane, n_pp, n_rays);
+  else if (pm == 3 || pm == 9) gen_fast_mixed<OCC, 3>(a, iblk, bi, bj, li0, lane, n_pp, n_rays);
+  else gen_fast_mixed<OCC, 8>(a, iblk, bi, bj, li0, lane, n_pp, n_rays);
 }
 
 // Tile class of request-local tile t (kernels_cull.cu) and the mask words of
@@ -521,8 +542,7 @@ __global__ void __launch_bounds__(256, 2) k_gen_fp64(const GenBatch* __restrict_
     phase ^= 1u;
 
     if (a.tcls && !(cls & kClsSlow) && !a.ray_log) {  // block-uniform: no ray of the tile can be blocked
-      if (pm <= 3) gen_fast_fp64<DIM3, OCC, 3>(a, iblk, bi, bj, warp, lane, n_pp, n_rays);
-      else gen_fast_fp64<DIM3, OCC, 4>(a, iblk, bi, bj, warp, lane, n_pp, n_rays);
+      fast_fp64<DIM3, OCC>(a, iblk, bi, bj, warp, lane, n_pp, n_rays);
       __syncthreads();
       if (OCC && threadIdx.x == 0) resv_release(Q, need, need_s);
       continue;
@@ -535,6 +555,10 @@ __global__ void __launch_bounds__(256, 2) k_gen_fp64(const GenBatch* __restrict_
       const int li = warp + 8 * rr;
       const int64_t i = bi * kTile + li;
       if (i >= N) continue;  // warp-uniform
+      if (a.tcls && !a.ray_log && s_mask[li] == 0u) {  // no ray of this row can be blocked
+        fast_fp64<DIM3, OCC>(a, iblk, bi, bj, li + 8, lane, n_pp, n_rays);
+        continue;
+      }
       const bool valid = (j < N) && (i < j);
       const int64_t oi = a.orig ? (int64_t)a.orig[i] : i;
       const bool sw = valid && oi > oj;  // the reference casts from the lower caller index
@@ -763,10 +787,7 @@ __global__ void __launch_bounds__(256, 2) k_gen_mixed(const GenBatch* __restrict
     phase ^= 1u;
 
     if (a.tcls && !(cls & (kClsSlow | kClsNear | kClsTiny)) && !a.ray_log) {  // block-uniform
-      if (pm == 7 || pm == 13 || pm == 49) gen_fast_mixed<OCC, 7>(a, iblk, bi, bj, warp, lane, n_pp, n_rays);
-      else if (pm == 5 || pm == 25) gen_fast_mixed<OCC, 5>(a, iblk, bi, bj, warp, lane, n_pp, n_rays);
-      else if (pm == 3 || pm == 9) gen_fast_mixed<OCC, 3>(a, iblk, bi, bj, warp, lane, n_pp, n_rays);
-      else gen_fast_mixed<OCC, 8>(a, iblk, bi, bj, warp, lane, n_pp, n_rays);
+      fast_mixed<OCC>(a, iblk, bi, bj, warp, lane, n_pp, n_rays);
       __syncthreads();
       if (OCC && threadIdx.x == 0) resv_release(Q, need, need_s);
       continue;
@@ -797,6 +818,17 @@ __global__ void __launch_bounds__(256, 2) k_gen_mixed(const GenBatch* __restrict
         dc0 = a.cen[3 * j] - ci0; dc1 = a.cen[3 * j + 1] - ci1; dc2 = a.cen[3 * j + 2] - ci2;
         const double dm = fmax(a.diam[i], a.diam[j]) * a.near_factor;
         near = (dc0 * dc0 + dc1 * dc1 + dc2 * dc2) < dm * dm;
+      }
+      if (a.tcls && !a.ray_log && s_mask[li] == 0u) {
+        bool close = near;
+        if (valid && !close) {
+          const double sr = a.rad[i] + a.rad[j] + a.tiny_gap;
+          close = (dc0 * dc0 + dc1 * dc1 + dc2 * dc2) <= sr * sr;
+        }
+        if (!__any_sync(kFull, close)) {  // no ray can be blocked, every pair far field
+          fast_mixed<OCC>(a, iblk, bi, bj, li + 8, lane, n_pp, n_rays);
+          continue;
+        }
       }
       n_near += (near && npj > 0) ? 1 : 0;
       const float d0 = (float)dc0, d1 = (float)dc1, d2 = (float)dc2;
@@ -1023,7 +1055,7 @@ __device__ int build_pair_list(const TraceArgs& a, const PendSlot& ps, int* fron
         u = (ab >> 4) + u8;
         const float4 p0 = a.sat[3 * u], p1 = a.sat[3 * u + 1], p2 = a.sat[3 * u + 2];
         const int32_t g = __float_as_int(p1.w);
-        keep = g != gi && g != gj && !pair_misses_tri(cap.A, bf, df, Rf, a.sat_em, p0, p1, p2);
+        keep = g != gi && g != gj && !pair_misses_tri_full(cap.A, bf, df, Rf, a.sat_em, p0, p1, p2);
       }
     }
     const uint32_t m = __ballot_sync(kFull, keep);

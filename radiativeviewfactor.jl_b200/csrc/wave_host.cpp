@@ -125,7 +125,7 @@ int wave_prepare(Session* s, rvf_mesh* m, Tables* T, const rvf_options* o, uint8
     x.N = N; x.nT = a.nT; x.n_tiles = a.n_tiles; x.pmax = a.pmax;
     x.tab = a.tab; x.tabf = T->tabf.as<float>(); x.np = a.np; x.area = a.area; x.flat = a.flat; x.nrm = a.nrm;
     x.cen = T->cen.as<double>(); x.diam = T->diam.as<double>(); x.near_factor = o->near_field_factor;
-    x.rad = a.rad; x.cull_margin = a.cull_margin;
+    x.rad = a.rad; x.cull_margin = a.cull_margin; x.tiny_gap = std::ldexp(m->extent, -16);
     x.group = a.group; x.orig = a.orig; x.F = a.F;
     x.nodes = a.nodes; x.n_nodes = a.n_nodes;
     x.nodesf = occ ? m->nodesf.as<NodeF>() : nullptr;
