@@ -346,7 +346,8 @@ def phases(stats):
     keys = ("ms_cull", "ms_gen", "ms_trace", "ms_lists", "ms_trace_fp64", "ms_resolve", "ms_duffy", "ms_pairs",
             "ms_prep", "ms_reduce")
     d = {k: statistics.mean(s[k] for s in stats) for k in keys}
-    for k in ("n_chunks", "n_rays_traced", "n_list_pairs", "n_walk_pairs", "n_tiles_culled", "n_pairs_masked"):
+    for k in ("n_chunks", "n_rays_traced", "n_list_pairs", "n_walk_pairs", "n_tiles_culled", "n_pairs_masked",
+              "n_tiles_unclassified"):
         d[k] = int(stats[-1][k])
     return d
 

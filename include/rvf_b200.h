@@ -158,7 +158,8 @@ typedef struct {
   int64_t n_tiles_culled; /* 3-D occlusion: tiles none of whose shadow rays can be blocked (no ray work) */
   int64_t n_pairs_masked; /*   pairs whose rays may be blocked (the only ones through the ray pipeline) */
   double ms_cull;         /* tile classification before the pair pipeline */
-  int64_t reserved[2];
+  int64_t n_tiles_unclassified; /* tiles whose walk overflowed its frontier or lists (every pair keeps its rays) */
+  int64_t reserved[1];
 } rvf_stats;
 
 const char* rvf_version(void);

@@ -105,7 +105,8 @@ struct RvfStats
     n_tiles_culled::Int64
     n_pairs_masked::Int64
     ms_cull::Float64
-    reserved::NTuple{2,Int64}
+    n_tiles_unclassified::Int64
+    reserved::NTuple{1,Int64}
 end
 
 struct RvfServerOpts

@@ -64,7 +64,8 @@ class Stats(C.Structure):
                 ("n_chunks", C.c_int64), ("ms_gen", C.c_double), ("ms_trace", C.c_double),
                 ("ms_trace_fp64", C.c_double), ("ms_resolve", C.c_double), ("n_list_pairs", C.c_int64),
                 ("n_walk_pairs", C.c_int64), ("ms_lists", C.c_double), ("n_tiles_culled", C.c_int64),
-                ("n_pairs_masked", C.c_int64), ("ms_cull", C.c_double), ("reserved", C.c_int64 * 2)]
+                ("n_pairs_masked", C.c_int64), ("ms_cull", C.c_double),
+                ("n_tiles_unclassified", C.c_int64), ("reserved", C.c_int64 * 1)]
 
     def as_dict(self):
         d = {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}

@@ -52,7 +52,8 @@ enum : uint8_t {
   kClsNear = 2,  // some pair is near field (mixed precision integrates it in FP64)
   kClsTiny = 4,  // some pair's points may nearly coincide (mixed precision: FP64)
 };
-constexpr int kTileLeaves = 128;  // candidate leaves of a tile's walk
+constexpr int kTileLeaves = 256;  // candidate leaves of a tile's walk
+constexpr int kTileFront = 256;   // breadth-first frontier of a tile's walk
 constexpr int kTileTris = 1024;   // listed triangles of a tile (more: every pair keeps its rays)
 
 struct TileClassArgs {
@@ -74,7 +75,7 @@ struct TileClassArgs {
   float sat_em;
   uint8_t* cls;    // n_tiles
   uint32_t* mask;  // n_tiles x 32
-  unsigned long long* counters;  // [culled tiles, masked pairs]
+  unsigned long long* counters;  // [culled tiles, masked pairs, tiles left unclassified]
 };
 
 struct WaveQ {

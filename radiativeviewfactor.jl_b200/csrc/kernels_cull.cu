@@ -159,7 +159,7 @@ __device__ __forceinline__ bool hull_misses_tri(const HullF& H, const float4& p0
 
 // One warp per tile, grid-stride over the tiles of one request.
 __global__ void __launch_bounds__(kCullWarps * 32) k_tile_class(const TileClassArgs a) {
-  __shared__ int s_front[kCullWarps][2 * kListFront];
+  __shared__ int s_front[kCullWarps][2 * kTileFront];
   __shared__ int s_leaf[kCullWarps][kTileLeaves];
   __shared__ int s_list[kCullWarps][kTileTris];
   __shared__ int s_row[kCullWarps][kTileTris];
@@ -169,7 +169,7 @@ __global__ void __launch_bounds__(kCullWarps * 32) k_tile_class(const TileClassA
   int* list = s_list[warp];
   int* rowl = s_row[warp];
   const int64_t N = a.N;
-  uint32_t n_culled = 0, n_masked = 0;
+  uint32_t n_culled = 0, n_masked = 0, n_over = 0;
   for (int64_t t = (int64_t)blockIdx.x * kCullWarps + warp; t < a.n_tiles; t += (int64_t)gridDim.x * kCullWarps) {
     int64_t bi, bj;
     tile_coords(t, a.nT, bi, bj);
@@ -257,7 +257,7 @@ __global__ void __launch_bounds__(kCullWarps * 32) k_tile_class(const TileClassA
       const float mbox = Rt + a.sat_em;
       // breadth-first walk from the start frontier
       int* cur = front;
-      int* nxt = front + kListFront;
+      int* nxt = front + kTileFront;
       if (lane < a.n_frontier) cur[lane] = a.frontier[lane];
       __syncwarp();
       int ncur = a.n_frontier, nleaf = 0;
@@ -280,14 +280,14 @@ __global__ void __launch_bounds__(kCullWarps * 32) k_tile_class(const TileClassA
           if (pass && leaf && pl < kTileLeaves) leaves[pl] = k;
           nleaf += __popc(ml);
           const int pi = nnext + 2 * __popc(mi & lanemask_lt());
-          if (pass && !leaf && pi + 1 < kListFront) {
+          if (pass && !leaf && pi + 1 < kTileFront) {
             nxt[pi] = k + 1;
             nxt[pi + 1] = right;
           }
           nnext += 2 * __popc(mi);
         }
         __syncwarp();
-        if (nleaf > kTileLeaves || nnext > kListFront) over = true;
+        if (nleaf > kTileLeaves || nnext > kTileFront) over = true;
         int* tmp = cur;
         cur = nxt;
         nxt = tmp;
@@ -320,6 +320,7 @@ __global__ void __launch_bounds__(kCullWarps * 32) k_tile_class(const TileClassA
       cls |= kClsSlow;
       a.mask[t * kTile + lane] = 0xffffffffu;
       n_masked += 32;
+      n_over += lane == 0 ? 1 : 0;
     } else if (nl > 0) {
       // per pair: some listed triangle survives the pair-list tests.  Row by
       // row, the warp first keeps the listed triangles the row's own hull
@@ -417,10 +418,12 @@ __global__ void __launch_bounds__(kCullWarps * 32) k_tile_class(const TileClassA
     if (lane == 0) a.cls[t] = cls;
   }
   if (a.counters) {
-    const uint64_t s_c = warp_sum_u64(lane == 0 ? n_culled : 0), s_m = warp_sum_u64(n_masked);
+    const uint64_t s_c = warp_sum_u64(lane == 0 ? n_culled : 0), s_m = warp_sum_u64(n_masked),
+                   s_o = warp_sum_u64(n_over);
     if (lane == 0) {
       atomicAdd(a.counters + 0, s_c);
       atomicAdd(a.counters + 1, s_m);
+      atomicAdd(a.counters + 2, s_o);
     }
   }
 }

@@ -1055,7 +1055,7 @@ __device__ int build_pair_list(const TraceArgs& a, const PendSlot& ps, int* fron
         u = (ab >> 4) + u8;
         const float4 p0 = a.sat[3 * u], p1 = a.sat[3 * u + 1], p2 = a.sat[3 * u + 2];
         const int32_t g = __float_as_int(p1.w);
-        keep = g != gi && g != gj && !pair_misses_tri_full(cap.A, bf, df, Rf, a.sat_em, p0, p1, p2);
+        keep = g != gi && g != gj && !pair_misses_tri(cap.A, bf, df, Rf, a.sat_em, p0, p1, p2);
       }
     }
     const uint32_t m = __ballot_sync(kFull, keep);

@@ -632,6 +632,7 @@ int rvf_solve(rvf_session* s, rvf_mesh* m, const rvf_options* o, double* F_elem,
     S.n_walk_pairs = (int64_t)c[12];
     S.n_tiles_culled = (int64_t)c[13];
     S.n_pairs_masked = (int64_t)c[14];
+    S.n_tiles_unclassified = (int64_t)c[15];
     if (N > 0 && m->G > 0) {
       std::vector<double> rs(N);
       cudaMemcpy(rs.data(), m->rowsum.ptr, sizeof(double) * N, cudaMemcpyDeviceToHost);
