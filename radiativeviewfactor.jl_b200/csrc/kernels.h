@@ -75,6 +75,7 @@ struct TileClassArgs {
   float sat_em;
   uint8_t* cls;    // n_tiles
   uint32_t* mask;  // n_tiles x 32
+  unsigned long long* claim;  // zeroed tile counter (warps claim tiles one at a time)
   unsigned long long* counters;  // [culled tiles, masked pairs, tiles left unclassified]
 };
 
@@ -147,6 +148,7 @@ struct PairArgs {
   int64_t tile0;                 // batched generation: first tile of this request in the launch
   const uint8_t* tcls;           // tile classes and masks (kernels_cull.cu), or null
   const uint32_t* tmask;
+  bool fast_done;                // tiles without ray work were integrated by k_fast_fp64: skip them
 };
 
 struct RedArgs {
@@ -207,6 +209,7 @@ struct MixedArgs {
   int64_t tile0;
   const uint8_t* tcls;  // tile classes and masks (kernels_cull.cu), or null
   const uint32_t* tmask;
+  bool fast_done;       // tiles without ray work were integrated by k_fast_mixed: skip them
 };
 
 struct TraceArgs {
@@ -315,6 +318,10 @@ cudaError_t launch_resolve(const WaveShape& sh, const ResolveBatch* r, int sm_co
 cudaError_t launch_plist(const TraceBatch* t, int sm_count, cudaStream_t st);
 // Tile classes and masks of one request (before its first chunk).
 cudaError_t launch_tile_class(const TileClassArgs& a, int sm_count, cudaStream_t st);
+// Every tile of one request that needs no shadow-ray work (its class), one
+// warp per tile, before the request's chunks; task_ctr: a zeroed counter.
+cudaError_t launch_fast(bool mixed, bool dim3, bool occ, const PairArgs& a, const MixedArgs& m,
+                        unsigned long long* task_ctr, unsigned long long* counters, int sm_count, cudaStream_t st);
 
 // A Quad8 pair sharing corner nodes (src/DuffyKernel.jl:95-115), i < j in the
 // caller's order (the reference integrates with elem_i = the lower index).

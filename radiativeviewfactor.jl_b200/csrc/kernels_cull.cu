@@ -170,7 +170,12 @@ __global__ void __launch_bounds__(kCullWarps * 32) k_tile_class(const TileClassA
   int* rowl = s_row[warp];
   const int64_t N = a.N;
   uint32_t n_culled = 0, n_masked = 0, n_over = 0;
-  for (int64_t t = (int64_t)blockIdx.x * kCullWarps + warp; t < a.n_tiles; t += (int64_t)gridDim.x * kCullWarps) {
+  for (;;) {
+    // tiles claimed one at a time: their costs differ by orders of magnitude
+    unsigned long long tc = 0;
+    if (lane == 0) tc = atomicAdd(a.claim, 1ull);
+    const int64_t t = (int64_t)__shfl_sync(kFull, tc, 0);
+    if (t >= a.n_tiles) break;
     int64_t bi, bj;
     tile_coords(t, a.nT, bi, bj);
     const int64_t ei = bi * kTile + lane, ej = bj * kTile + lane;
@@ -436,6 +441,8 @@ cudaError_t launch_tile_class(const TileClassArgs& a, int sm_count, cudaStream_t
     per_sm = 1;
   const int64_t want = (a.n_tiles + kCullWarps - 1) / kCullWarps;
   const int grid = (int)std::min<int64_t>(want, (int64_t)sm_count * per_sm);
+  const cudaError_t e = cudaMemsetAsync(a.claim, 0, sizeof(unsigned long long), st);
+  if (e != cudaSuccess) return e;
   k_tile_class<<<(unsigned)grid, kCullWarps * 32, 0, st>>>(a);
   return cudaGetLastError();
 }

@@ -247,8 +247,8 @@ __device__ __forceinline__ int find_req(const int64_t* tile_base, int n_req, int
 // Out of line: their registers are allocated apart from the ray pipeline's.
 // ---------------------------------------------------------------------------
 template <bool DIM3, bool OCC, int QB>
-__device__ __noinline__ void gen_fast_fp64(const PairArgs& a, const double* iblk, int64_t bi, int64_t bj, int li0,
-                                           int lane, uint32_t& n_pp, uint32_t& n_rays) {
+__device__ __forceinline__ void gen_fast_fp64_body(const PairArgs& a, const double* iblk, int64_t bi, int64_t bj,
+                                                   int li0, int lane, uint32_t& n_pp, uint32_t& n_rays) {
   const int64_t N = a.N;
   const int pm = a.pmax;
   const int64_t j = bj * kTile + lane;
@@ -373,8 +373,8 @@ __device__ __noinline__ void gen_fast_fp64(const PairArgs& a, const double* iblk
 // here: no ray depends on the sign of their K, and their FP32 error is that
 // of any other far-field term.
 template <bool OCC, int QB>
-__device__ __noinline__ void gen_fast_mixed(const MixedArgs& a, const float* iblk, int64_t bi, int64_t bj, int li0,
-                                            int lane, uint32_t& n_pp, uint32_t& n_rays) {
+__device__ __forceinline__ void gen_fast_mixed_body(const MixedArgs& a, const float* iblk, int64_t bi, int64_t bj,
+                                                    int li0, int lane, uint32_t& n_pp, uint32_t& n_rays) {
   const int64_t N = a.N;
   const int pm = a.pmax;
   const int64_t j = bj * kTile + lane;
@@ -449,6 +449,19 @@ __device__ __noinline__ void gen_fast_mixed(const MixedArgs& a, const float* ibl
       a.F[oi + oi * N] = 0.0 / a.area[i];
     }
   }
+}
+
+// Out of line inside the chunked generation kernels, whose own registers are
+// allocated for the ray pipeline.
+template <bool DIM3, bool OCC, int QB>
+__device__ __noinline__ void gen_fast_fp64(const PairArgs& a, const double* iblk, int64_t bi, int64_t bj, int li0,
+                                           int lane, uint32_t& n_pp, uint32_t& n_rays) {
+  gen_fast_fp64_body<DIM3, OCC, QB>(a, iblk, bi, bj, li0, lane, n_pp, n_rays);
+}
+template <bool OCC, int QB>
+__device__ __noinline__ void gen_fast_mixed(const MixedArgs& a, const float* iblk, int64_t bi, int64_t bj, int li0,
+                                            int lane, uint32_t& n_pp, uint32_t& n_rays) {
+  gen_fast_mixed_body<OCC, QB>(a, iblk, bi, bj, li0, lane, n_pp, n_rays);
 }
 
 // The fast loop with the point block for the rule's size (li0 as there).
@@ -542,7 +555,7 @@ __global__ void __launch_bounds__(256, 2) k_gen_fp64(const GenBatch* __restrict_
     phase ^= 1u;
 
     if (a.tcls && !(cls & kClsSlow) && !a.ray_log) {  // block-uniform: no ray of the tile can be blocked
-      fast_fp64<DIM3, OCC>(a, iblk, bi, bj, warp, lane, n_pp, n_rays);
+      if (!a.fast_done) fast_fp64<DIM3, OCC>(a, iblk, bi, bj, warp, lane, n_pp, n_rays);
       __syncthreads();
       if (OCC && threadIdx.x == 0) resv_release(Q, need, need_s);
       continue;
@@ -787,7 +800,7 @@ __global__ void __launch_bounds__(256, 2) k_gen_mixed(const GenBatch* __restrict
     phase ^= 1u;
 
     if (a.tcls && !(cls & (kClsSlow | kClsNear | kClsTiny)) && !a.ray_log) {  // block-uniform
-      fast_mixed<OCC>(a, iblk, bi, bj, warp, lane, n_pp, n_rays);
+      if (!a.fast_done) fast_mixed<OCC>(a, iblk, bi, bj, warp, lane, n_pp, n_rays);
       __syncthreads();
       if (OCC && threadIdx.x == 0) resv_release(Q, need, need_s);
       continue;
@@ -1474,8 +1487,87 @@ __global__ void __launch_bounds__(256) k_resolve_mixed(const ResolveBatch* __res
 }
 
 // ---------------------------------------------------------------------------
+// 1c. Tiles without shadow-ray work, in a kernel of their own before the
+// chunks: each warp claims whole tiles, reads the source element's points
+// from the table in global memory (L1 / L2 resident; the warp's lanes read
+// the same address) and runs the quadrature-only loop over the tile's 32
+// rows -- no shared-memory staging, no block barriers, and the registers of
+// that loop alone (the chunked generation then skips these tiles).
+// ---------------------------------------------------------------------------
+template <bool DIM3, bool OCC>
+__global__ void __launch_bounds__(256, 2) k_fast_fp64(const PairArgs a, unsigned long long* task_ctr,
+                                                      unsigned long long* counters) {
+  const int lane = threadIdx.x & 31;
+  uint32_t n_pp = 0, n_rays = 0;
+  for (;;) {
+    unsigned long long t = 0;
+    if (lane == 0) t = atomicAdd(task_ctr, 1ull);
+    t = __shfl_sync(kFull, t, 0);
+    if (t >= (unsigned long long)a.n_tiles) break;
+    if (a.tcls[t] & kClsSlow) continue;
+    int64_t bi, bj;
+    tile_coords((int64_t)t, a.nT, bi, bj);
+    const double* ib = a.tab + bi * kComp * a.pmax * kTile;
+    if (a.pmax <= 3) {
+      for (int r = 0; r < 8; ++r) gen_fast_fp64_body<DIM3, OCC, 3>(a, ib, bi, bj, r, lane, n_pp, n_rays);
+    } else {
+      for (int r = 0; r < 8; ++r) gen_fast_fp64_body<DIM3, OCC, 4>(a, ib, bi, bj, r, lane, n_pp, n_rays);
+    }
+  }
+  const uint64_t s_pp = warp_sum_u64(n_pp), s_rays = warp_sum_u64(n_rays);
+  if (lane == 0 && counters) {
+    atomicAdd(counters + 0, s_pp);
+    atomicAdd(counters + 1, s_rays);
+  }
+}
+
+template <bool OCC>
+__global__ void __launch_bounds__(256, 2) k_fast_mixed(const MixedArgs a, unsigned long long* task_ctr,
+                                                       unsigned long long* counters) {
+  const int lane = threadIdx.x & 31;
+  uint32_t n_pp = 0, n_rays = 0;
+  for (;;) {
+    unsigned long long t = 0;
+    if (lane == 0) t = atomicAdd(task_ctr, 1ull);
+    t = __shfl_sync(kFull, t, 0);
+    if (t >= (unsigned long long)a.n_tiles) break;
+    if (a.tcls[t] & (kClsSlow | kClsNear | kClsTiny)) continue;
+    int64_t bi, bj;
+    tile_coords((int64_t)t, a.nT, bi, bj);
+    const float* ib = a.tabf + bi * kComp * a.pmax * kTile;
+    const int pm = a.pmax;
+    if (pm == 7 || pm == 13 || pm == 49) {
+      for (int r = 0; r < 8; ++r) gen_fast_mixed_body<OCC, 7>(a, ib, bi, bj, r, lane, n_pp, n_rays);
+    } else if (pm == 5 || pm == 25) {
+      for (int r = 0; r < 8; ++r) gen_fast_mixed_body<OCC, 5>(a, ib, bi, bj, r, lane, n_pp, n_rays);
+    } else if (pm == 3 || pm == 9) {
+      for (int r = 0; r < 8; ++r) gen_fast_mixed_body<OCC, 3>(a, ib, bi, bj, r, lane, n_pp, n_rays);
+    } else {
+      for (int r = 0; r < 8; ++r) gen_fast_mixed_body<OCC, 8>(a, ib, bi, bj, r, lane, n_pp, n_rays);
+    }
+  }
+  const uint64_t s_pp = warp_sum_u64(n_pp), s_rays = warp_sum_u64(n_rays);
+  if (lane == 0 && counters) {
+    atomicAdd(counters + 0, s_pp);
+    atomicAdd(counters + 1, s_rays);
+  }
+}
+
+// ---------------------------------------------------------------------------
 // host launchers
 // ---------------------------------------------------------------------------
+cudaError_t launch_fast(bool mixed, bool dim3, bool occ, const PairArgs& a, const MixedArgs& m,
+                        unsigned long long* task_ctr, unsigned long long* counters, int sm_count, cudaStream_t st) {
+  auto launch = [&](auto fn, const auto& args) -> cudaError_t {
+    int per_sm = 1;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 256, 0) != cudaSuccess || per_sm < 1) per_sm = 1;
+    fn<<<(unsigned)(sm_count * per_sm), 256, 0, st>>>(args, task_ctr, counters);
+    return cudaGetLastError();
+  };
+  if (mixed) return occ ? launch(k_fast_mixed<true>, m) : launch(k_fast_mixed<false>, m);
+  if (dim3) return occ ? launch(k_fast_fp64<true, true>, a) : launch(k_fast_fp64<true, false>, a);
+  return occ ? launch(k_fast_fp64<false, true>, a) : launch(k_fast_fp64<false, false>, a);
+}
 size_t gen_smem_bytes(bool mixed, int pmax, bool occ) {
   // tile block, then (occlusion) the per-warp FP64 staging (mixed) and the
   // per-lane runs, then the mbarrier

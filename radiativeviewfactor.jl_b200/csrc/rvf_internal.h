@@ -73,6 +73,7 @@ struct rvf_session {
   // wavefront pair pipeline (kernels_wave.cu, wave_host.cpp): queues,
   // device launch blocks, pinned counter readback, graphs per launch shape
   rvf::DevBuf wq_ctr, wq_rec64, wq_rec32, wq_slots, wq_vis, wq_plist, wq_pool;
+  rvf::DevBuf fast_ctr;  // tile counter of the kernel for tiles without ray work
   rvf::DevBuf wl_pair, wl_mixed, wl_trace, wl_resolve, wl_tilebase, wl_gen, wl_tb, wl_rb;
   unsigned long long* h_ctr = nullptr;
   std::map<uint64_t, cudaGraphExec_t> graphs;

@@ -223,6 +223,7 @@ int admit_one(rvf_server* sv, Req* r) {
   m->has_result = false;
   if (N == 1) cudaMemsetAsync(m->F.ptr, 0, sizeof(double), s->stream);
   if ((rc = wave_prepare(s, m, r->T, &r->opts, nullptr, r->w, nullptr))) return rc;
+  if ((rc = wave_fast(s, r->w, nullptr))) return rc;
   const cudaError_t e = cudaStreamSynchronize(s->stream);
   return e == cudaSuccess ? RVF_OK : cuda_err(e, "request set-up");
 }

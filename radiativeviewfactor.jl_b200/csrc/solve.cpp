@@ -319,6 +319,7 @@ int rvf_session_destroy(rvf_session* s) try {
     s->err.free_();
     s->tile_counter.free_();
     s->counters.free_();
+    s->fast_ctr.free_();
     s->wq_ctr.free_(); s->wq_rec64.free_(); s->wq_rec32.free_(); s->wq_slots.free_(); s->wq_vis.free_(); s->wq_plist.free_(); s->wq_pool.free_();
     for (rvf::DevBuf* b : {&s->wl_pair, &s->wl_mixed, &s->wl_trace, &s->wl_resolve, &s->wl_tilebase, &s->wl_gen,
                            &s->wl_tb, &s->wl_rb})
@@ -508,6 +509,11 @@ int rvf_solve(rvf_session* s, rvf_mesh* m, const rvf_options* o, double* F_elem,
       EvTimer tc(s->stream);
       if ((rc = wave_prepare(s, m, T, o, o->ray_log ? log.as<uint8_t>() : nullptr, w, &n_kernels))) return rc;
       S.ms_cull = tc.stop();
+    }
+    {
+      EvTimer tf(s->stream);
+      if ((rc = wave_fast(s, w, &n_kernels))) return rc;
+      S.ms_gen += tf.stop();
     }
     // Duffy and self pairs overwrite F after the pipeline: no early columns then
     if (F_elem && N > 1 && !(o->use_duffy && m->dim == 2) && !o->self_vf) {

@@ -166,6 +166,8 @@ int wave_prepare(Session* s, rvf_mesh* m, Tables* T, const rvf_options* o, uint8
     }
     c.cls = T->tcls.as<uint8_t>();
     c.mask = T->tmask.as<uint32_t>();
+    if (!s->fast_ctr.ptr && (rc = s->fast_ctr.alloc(s, 256))) return rc;
+    c.claim = s->fast_ctr.as<unsigned long long>() + 1;
     c.counters = s->counters.as<unsigned long long>() + 13;
     const cudaError_t e = launch_tile_class(c, s->sm_count, s->stream);
     if (e != cudaSuccess) return cuda_err(e, "tile classification launch");
@@ -193,6 +195,21 @@ int wave_prepare(Session* s, rvf_mesh* m, Tables* T, const rvf_options* o, uint8
   ra.F = a.F;
   w.nodes_d = a.nodes;
   w.nodes_f = w.ma.nodesf;
+  return 0;
+}
+
+int wave_fast(Session* s, WaveReq& w, int64_t* n_kernels) {
+  if (!w.pa.tcls || w.pa.ray_log || w.n_tiles == 0) return 0;
+  int rc = 0;
+  if (!s->fast_ctr.ptr && (rc = s->fast_ctr.alloc(s, 256))) return rc;
+  cudaError_t e = cudaMemsetAsync(s->fast_ctr.ptr, 0, sizeof(unsigned long long), s->stream);
+  if (e == cudaSuccess)
+    e = launch_fast(w.mixed, w.dim3, w.occ, w.pa, w.ma, s->fast_ctr.as<unsigned long long>(),
+                    s->counters.as<unsigned long long>(), s->sm_count, s->stream);
+  if (e != cudaSuccess) return cuda_err(e, "quadrature-only tiles launch");
+  if (n_kernels) *n_kernels += 1;
+  w.pa.fast_done = true;
+  w.ma.fast_done = true;
   return 0;
 }
 

@@ -38,6 +38,9 @@ int ensure_wave(Session* s, bool two_queues, bool occ, bool lists, int pmax, int
 int wave_prepare(Session* s, rvf_mesh* m, Tables* T, const rvf_options* o, uint8_t* ray_log, WaveReq& w,
                  int64_t* n_kernels);
 WaveShape wave_shape(Session* s, WaveReq* const* reqs, int n);
+// The request's tiles without shadow-ray work (by class), before its chunks;
+// the chunks then skip them.  No-op without tile classes or with a ray log.
+int wave_fast(Session* s, WaveReq& w, int64_t* n_kernels);
 // One chunk over n requests of one shape (mixed, dim3, occ equal): claims
 // tiles in request order while the queues have room, traces and resolves
 // them, and advances each request's progress.  use_graph replays a CUDA
