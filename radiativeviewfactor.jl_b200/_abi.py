@@ -12,7 +12,8 @@ from pathlib import Path
 
 import numpy as np
 
-LIB_PATH = Path(__file__).resolve().parent / "lib" / "librvf_b200.so"
+# the in-tree build; RVF_B200_LIB names another build of the same library
+LIB_PATH = Path(os.environ.get("RVF_B200_LIB") or Path(__file__).resolve().parent / "lib" / "librvf_b200.so")
 
 RVF_OK = 0
 STATUS_NAMES = {0: "RVF_OK", -1: "RVF_EINVAL", -2: "RVF_ENOMEM", -3: "RVF_EBUDGET", -4: "RVF_ECUDA",

@@ -51,6 +51,11 @@ namespace {
 
 constexpr int kCullWarps = 4;
 
+// Pair masks: the capsule test over all 16 axes (1) or the pair lists' 4 (0).
+#ifndef RVF_MASK_FULL_AXES
+#define RVF_MASK_FULL_AXES 1
+#endif
+
 // H = conv(B_1 u B_2) of two boxes (FP32 centres c and half extents h).
 struct HullF {
   float c[2][3], h[2][3];
@@ -404,7 +409,9 @@ __global__ void __launch_bounds__(kCullWarps * 32) k_tile_class(const TileClassA
           if (!done && lpass) {
             const float4 p0 = a.sat[3 * u], p1 = a.sat[3 * u + 1], p2 = a.sat[3 * u + 2];
             const int32_t g = __float_as_int(p1.w);
-            if (g != gj && !pair_misses_tri_full(cap.A, bf, df, Rf, a.sat_em, p0, p1, p2)) {
+            const bool miss = RVF_MASK_FULL_AXES ? pair_misses_tri_full(cap.A, bf, df, Rf, a.sat_em, p0, p1, p2)
+                                                 : pair_misses_tri(cap.A, bf, df, Rf, a.sat_em, p0, p1, p2);
+            if (g != gj && !miss) {
               bit = true;
               done = true;
             }
