@@ -149,6 +149,7 @@ struct PairArgs {
   const uint8_t* tcls;           // tile classes and masks (kernels_cull.cu), or null
   const uint32_t* tmask;
   bool fast_done;                // tiles without ray work were integrated by k_fast_fp64: skip them
+  const int32_t* work;           // the tiles of the chunked pipeline in order (null: every tile)
 };
 
 struct RedArgs {
@@ -210,6 +211,7 @@ struct MixedArgs {
   const uint8_t* tcls;  // tile classes and masks (kernels_cull.cu), or null
   const uint32_t* tmask;
   bool fast_done;       // tiles without ray work were integrated by k_fast_mixed: skip them
+  const int32_t* work;  // the tiles of the chunked pipeline in order (null: every tile)
 };
 
 struct TraceArgs {

@@ -202,7 +202,8 @@ __global__ void __launch_bounds__(kCullWarps * 32) k_tile_class(const TileClassA
     }
     // near-field and nearly coincident pairs (lane = j, loop over the row block)
     bool near = false, tiny = false;
-    for (int li = 0; li < kTile; ++li) {
+    const bool classify_near = a.near_factor >= 0.0 || a.tiny_gap >= 0.0;  // mixed precision only
+    for (int li = 0; li < (classify_near ? kTile : 0); ++li) {
       const double x0 = __shfl_sync(kFull, ci[0], li), x1 = __shfl_sync(kFull, ci[1], li),
                    x2 = __shfl_sync(kFull, ci[2], li);
       const double rr = __shfl_sync(kFull, ri, li), dd = __shfl_sync(kFull, di, li);
@@ -214,8 +215,10 @@ __global__ void __launch_bounds__(kCullWarps * 32) k_tile_class(const TileClassA
         const double dm = fmax(dd, dj) * a.near_factor;
         near = near || q < dm * dm;
       }
-      const double s = rr + rj + a.tiny_gap;
-      tiny = tiny || q <= s * s;
+      if (a.tiny_gap >= 0.0) {
+        const double s = rr + rj + a.tiny_gap;
+        tiny = tiny || q <= s * s;
+      }
     }
     uint8_t cls = (__any_sync(kFull, near) ? kClsNear : 0) | (__any_sync(kFull, tiny) ? kClsTiny : 0);
     bool all_ones = false;  // occlusion the tile cannot classify: every pair keeps its rays

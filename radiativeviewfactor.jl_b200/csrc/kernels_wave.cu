@@ -527,6 +527,7 @@ __global__ void __launch_bounds__(256, 2) k_gen_fp64(const GenBatch* __restrict_
         const PairArgs& a = L.reqs[r];
         s_req = r;
         s_tile = g - L.tile_base[r] + a.tile0;
+        if (a.work) s_tile = a.work[s_tile];
         if (OCC) s_root = a.nodes[0];
         int64_t bi, bj;
         tile_coords(s_tile, a.nT, bi, bj);
@@ -769,6 +770,7 @@ __global__ void __launch_bounds__(256, 2) k_gen_mixed(const GenBatch* __restrict
         const MixedArgs& a = L.mreqs[r];
         s_req = r;
         s_tile = g - L.tile_base[r] + a.tile0;
+        if (a.work) s_tile = a.work[s_tile];
         if (OCC) {
           s_rootf = a.nodesf[0];
           s_root = a.nodes[0];

@@ -54,6 +54,7 @@ struct Tables {
   DevBuf area_orig;                                   // areas in the caller's element order
   DevBuf tabf;  // FP32 table, built on the first mixed-precision solve
   DevBuf tcls, tmask;  // tile classes and masks of the last solve (kernels_cull.cu)
+  DevBuf twork;        // the tiles the chunked pipeline integrates (tile indices, row-major)
 };
 
 }  // namespace rvf

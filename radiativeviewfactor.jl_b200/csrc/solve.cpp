@@ -398,9 +398,13 @@ struct ColumnDownload {
   int64_t N = 0, nT = 0, rows_done = 0;
   bool issued = false;
   std::vector<int32_t> cols;
+  const std::vector<int64_t>* listed = nullptr;  // the pipeline's tile list: listed tiles through each row
 
-  // one past the last tile of row bi
-  int64_t row_end(int64_t bi) const { return (bi + 1) * nT - bi * (bi + 1) / 2; }
+  // one past the last tile of row bi (in the pipeline's claim order)
+  int64_t row_end(int64_t bi) const {
+    if (listed && !listed->empty()) return (*listed)[(size_t)bi];
+    return (bi + 1) * nT - bi * (bi + 1) / 2;
+  }
 
   cudaError_t advance(int64_t claimed_tiles) {
     cols.clear();
@@ -522,6 +526,7 @@ int rvf_solve(rvf_session* s, rvf_mesh* m, const rvf_options* o, double* F_elem,
       dl.host = F_elem;
       dl.N = N;
       dl.nT = (N + kTile - 1) / kTile;
+      dl.listed = &w.row_end;
     }
     EvTimer t(s->stream);
     WaveReq* one = &w;

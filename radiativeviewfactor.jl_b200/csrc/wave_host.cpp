@@ -151,7 +151,7 @@ int wave_prepare(Session* s, rvf_mesh* m, Tables* T, const rvf_options* o, uint8
     c.diam = T->diam.as<double>();
     c.group = a.group;
     c.near_factor = w.mixed ? o->near_field_factor : -1.0;
-    c.tiny_gap = std::ldexp(m->extent, -16);
+    c.tiny_gap = w.mixed ? std::ldexp(m->extent, -16) : -1.0;
     c.cull_margin = a.cull_margin;
     c.occ = occ;
     c.dim3 = w.dim3;
@@ -176,6 +176,36 @@ int wave_prepare(Session* s, rvf_mesh* m, Tables* T, const rvf_options* o, uint8
     a.tmask = c.mask;
     w.ma.tcls = c.cls;
     w.ma.tmask = c.mask;
+    if (!ray_log) {
+      // The chunked pipeline's tiles: those with ray work (or near-field /
+      // nearly coincident pairs in mixed precision), in row-major order; the
+      // others go to the quadrature-only kernel (wave_fast).
+      std::vector<uint8_t> cls(nt);
+      cudaError_t e2 = cudaMemcpyAsync(cls.data(), c.cls, nt, cudaMemcpyDeviceToHost, s->stream);
+      if (e2 == cudaSuccess) e2 = cudaStreamSynchronize(s->stream);
+      if (e2 != cudaSuccess) return cuda_err(e2, "tile classes");
+      const uint8_t need = w.mixed ? (uint8_t)(kClsSlow | kClsNear | kClsTiny) : (uint8_t)kClsSlow;
+      std::vector<int32_t> work;
+      w.row_end.assign((size_t)a.nT, 0);
+      int64_t t = 0;
+      for (int64_t bi = 0; bi < a.nT; ++bi) {
+        for (int64_t bj = bi; bj < a.nT; ++bj, ++t)
+          if (cls[(size_t)t] & need) work.push_back((int32_t)t);
+        w.row_end[(size_t)bi] = (int64_t)work.size();
+      }
+      if (!work.empty()) {
+        if (T->twork.bytes < sizeof(int32_t) * work.size() &&
+            (rc = T->twork.alloc(s, sizeof(int32_t) * work.size())))
+          return rc;
+        e2 = cudaMemcpyAsync(T->twork.ptr, work.data(), sizeof(int32_t) * work.size(), cudaMemcpyHostToDevice,
+                             s->stream);
+        if (e2 == cudaSuccess) e2 = cudaStreamSynchronize(s->stream);  // the host vector goes out of scope
+        if (e2 != cudaSuccess) return cuda_err(e2, "tile list upload");
+      }
+      a.work = T->twork.as<int32_t>();
+      w.ma.work = a.work;
+      w.n_tiles = (int64_t)work.size();
+    }
   }
   TraceArgs& ta = w.ta;
   ta.N = N; ta.pmax = a.pmax; ta.dim3 = a.dim3; ta.tab = a.tab; ta.tabf = w.ma.tabf; ta.cen = a.cen;

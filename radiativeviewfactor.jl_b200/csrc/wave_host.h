@@ -1,6 +1,8 @@
 // wave_host.h -- host side of the wavefront pair pipeline (wave_host.cpp).
 #pragma once
 
+#include <vector>
+
 #include <functional>
 
 #include "kernels.h"
@@ -16,7 +18,8 @@ struct WaveReq {
   ResolveArgs ra{};
   bool mixed = false, occ = false, dim3 = true;
   int pmax = 0;
-  int64_t n_tiles = 0;  // upper-triangle tiles of the mesh
+  int64_t n_tiles = 0;  // tiles of the chunked pipeline (every upper-triangle tile, or the listed ones)
+  std::vector<int64_t> row_end;  // with a tile list: listed tiles in tile rows 0..r (for the F download)
   int64_t claimed = 0;  // tiles integrated so far
   int claim_retries = 4096;  // compare-and-swap attempts of a tile claim (0: every claim gives up)
   const NodeD* nodes_d = nullptr;
