@@ -167,11 +167,15 @@ __global__ void __launch_bounds__(kCullWarps * 32) k_tile_class(const TileClassA
   __shared__ int s_front[kCullWarps][2 * kTileFront];
   __shared__ int s_leaf[kCullWarps][kTileLeaves];
   __shared__ int s_list[kCullWarps][kTileTris];
-  __shared__ int s_row[kCullWarps][kTileTris];
+  __shared__ int s_rleaf[kCullWarps][kTileLeaves];  // runs of the list: leaf node
+  __shared__ int s_rspan[kCullWarps][kTileLeaves];  //   first list entry * 16 + count
+  __shared__ int s_row[kCullWarps][kTileLeaves];    // a row's runs
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   int* front = s_front[warp];
   int* leaves = s_leaf[warp];
   int* list = s_list[warp];
+  int* rleaf = s_rleaf[warp];
+  int* rspan = s_rspan[warp];
   int* rowl = s_row[warp];
   const int64_t N = a.N;
   uint32_t n_culled = 0, n_masked = 0, n_over = 0;
@@ -223,6 +227,7 @@ __global__ void __launch_bounds__(kCullWarps * 32) k_tile_class(const TileClassA
     uint8_t cls = (__any_sync(kFull, near) ? kClsNear : 0) | (__any_sync(kFull, tiny) ? kClsTiny : 0);
     bool all_ones = false;  // occlusion the tile cannot classify: every pair keeps its rays
     int nl = 0;             // listed triangles
+    int nrun = 0;           // leaves with listed triangles (runs of the list)
     HullF H;                // the tile's hull (occlusion, 3-D)
     float rmaxJ = 0.0f;     // largest point radius of the column block
     if (a.occ && !a.dim3) {
@@ -323,8 +328,24 @@ __global__ void __launch_bounds__(kCullWarps * 32) k_tile_class(const TileClassA
         const uint32_t m = __ballot_sync(kFull, keep);
         const int pos = nl + __popc(m & lanemask_lt());
         if (keep && pos < kTileTris) list[pos] = u;
+        // one run per leaf of this round that kept triangles
+        if (lane < 4 && b + lane < nleaf) {
+          const uint32_t lm = (m >> (8 * lane)) & 0xffu;
+          if (lm) {
+            int before = 0;
+            for (int k = 0; k < lane; ++k) before += ((m >> (8 * k)) & 0xffu) ? 1 : 0;
+            const int r = nrun + before;
+            rleaf[r] = leaves[b + lane];
+            rspan[r] = (nl + __popc(m & ((1u << (8 * lane)) - 1u))) * 16 + __popc(lm);
+          }
+        }
+        int nnew = 0;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) nnew += ((m >> (8 * k)) & 0xffu) ? 1 : 0;
+        nrun += nnew;
         nl += __popc(m);
         if (nl > kTileTris) over = true;
+        __syncwarp();
       }
       __syncwarp();
       all_ones = over;
@@ -336,9 +357,10 @@ __global__ void __launch_bounds__(kCullWarps * 32) k_tile_class(const TileClassA
       n_over += lane == 0 ? 1 : 0;
     } else if (nl > 0) {
       // per pair: some listed triangle survives the pair-list tests.  Row by
-      // row, the warp first keeps the listed triangles the row's own hull
-      // (its centroid and the column block's box, radius max(rad_i, rad_J))
-      // can reach, 32 at a time, then each lane tests its pair against those.
+      // row, the warp first keeps the runs (leaves with listed triangles)
+      // whose box the row's own hull (its centroid and the column block's box,
+      // radius max(rad_i, rad_J)) can reach, 32 at a time; each lane then
+      // tests its pair against those leaves and their triangles.
       cls |= kClsSlow;
       for (int li = 0; li < kTile; ++li) {
         const int64_t i = bi * kTile + li;
@@ -361,21 +383,13 @@ __global__ void __launch_bounds__(kCullWarps * 32) k_tile_class(const TileClassA
           Hr.h[1][c] = H.h[1][c];
           Hr.d[c] = Hr.c[1][c] - Hr.c[0][c];
         }
-        const float Rr = fmaxf(__double2float_ru(rr), rmaxJ) + __double2float_ru(a.cull_margin);
+        const float Rr = fmaxf(__double2float_ru(rr), rmaxJ) + __double2float_ru(a.cull_margin) + a.sat_em;
         int nr = 0;
-        for (int b = 0; b < nl; b += 32) {
-          const int e = b + lane;
-          bool keep = false;
-          int u = 0;
-          if (e < nl) {
-            u = list[e];
-            const float4 p0 = a.sat[3 * u], p1 = a.sat[3 * u + 1], p2 = a.sat[3 * u + 2];
-            const int32_t g = __float_as_int(p1.w);
-            keep = g != g_i && !hull_misses_box(Hr, a.nodesf[a.leaf_of[u]], Rr + a.sat_em) &&
-                   !hull_misses_tri(Hr, p0, p1, p2, Rr + p0.w + a.sat_em);
-          }
+        for (int b = 0; b < nrun; b += 32) {
+          const int r = b + lane;
+          const bool keep = r < nrun && !hull_misses_box(Hr, a.nodesf[rleaf[r]], Rr);
           const uint32_t m = __ballot_sync(kFull, keep);
-          if (keep) rowl[nr + __popc(m & lanemask_lt())] = u;  // in list order, so grouped by leaf
+          if (keep) rowl[nr + __popc(m & lanemask_lt())] = r;
           nr += __popc(m);
         }
         __syncwarp();
@@ -399,26 +413,21 @@ __global__ void __launch_bounds__(kCullWarps * 32) k_tile_class(const TileClassA
           Rf = (float)R;
         }
         bool bit = false, done = !valid;
-        int last = -1;
-        bool lpass = false;
         for (int e = 0; e < nr; ++e) {
           if (__all_sync(kFull, done)) break;
-          const int u = rowl[e];
-          const int lf = a.leaf_of[u];
-          if (lf != last) {
-            last = lf;
-            lpass = !done && !capsule_misses_box(cap, a.nodesf[lf]);
-          }
-          if (!done && lpass) {
+          const int r = rowl[e];
+          const int span = rspan[r];
+          if (done || capsule_misses_box(cap, a.nodesf[rleaf[r]])) continue;
+          for (int k = span >> 4; k < (span >> 4) + (span & 15) && !bit; ++k) {
+            const int u = list[k];
             const float4 p0 = a.sat[3 * u], p1 = a.sat[3 * u + 1], p2 = a.sat[3 * u + 2];
             const int32_t g = __float_as_int(p1.w);
+            if (g == g_i || g == gj) continue;
             const bool miss = RVF_MASK_FULL_AXES ? pair_misses_tri_full(cap.A, bf, df, Rf, a.sat_em, p0, p1, p2)
                                                  : pair_misses_tri(cap.A, bf, df, Rf, a.sat_em, p0, p1, p2);
-            if (g != gj && !miss) {
-              bit = true;
-              done = true;
-            }
+            bit = !miss;
           }
+          done = done || bit;
         }
         __syncwarp();
         const uint32_t m = __ballot_sync(kFull, bit);

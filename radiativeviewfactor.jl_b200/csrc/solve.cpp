@@ -527,6 +527,11 @@ int rvf_solve(rvf_session* s, rvf_mesh* m, const rvf_options* o, double* F_elem,
       dl.N = N;
       dl.nT = (N + kTile - 1) / kTile;
       dl.listed = &w.row_end;
+      // rows without listed tiles are final once the quadrature-only kernel
+      // ends: their columns may go out before any chunk, on the copy stream
+      if ((e = cudaEventRecord(s->ev[7], s->stream)) != cudaSuccess ||
+          (e = cudaStreamWaitEvent(s->copy_stream, s->ev[7], 0)) != cudaSuccess)
+        return cuda_err(e, "download ordering");
     }
     EvTimer t(s->stream);
     WaveReq* one = &w;

@@ -229,7 +229,7 @@ int wave_prepare(Session* s, rvf_mesh* m, Tables* T, const rvf_options* o, uint8
 }
 
 int wave_fast(Session* s, WaveReq& w, int64_t* n_kernels) {
-  if (!w.pa.tcls || w.pa.ray_log || w.n_tiles == 0) return 0;
+  if (!w.pa.tcls || w.pa.ray_log || w.pa.n_tiles == 0) return 0;
   int rc = 0;
   if (!s->fast_ctr.ptr && (rc = s->fast_ctr.alloc(s, 256))) return rc;
   cudaError_t e = cudaMemsetAsync(s->fast_ctr.ptr, 0, sizeof(unsigned long long), s->stream);
