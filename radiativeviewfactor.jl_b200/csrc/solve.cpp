@@ -398,11 +398,12 @@ struct ColumnDownload {
   int64_t N = 0, nT = 0, rows_done = 0;
   bool issued = false;
   std::vector<int32_t> cols;
-  const std::vector<int64_t>* listed = nullptr;  // the pipeline's tile list: listed tiles through each row
+  std::vector<int64_t> listed;  // the pipeline's tile list: listed tiles through each row (a copy: the
+                                // pipeline's request ends before the last download)
 
   // one past the last tile of row bi (in the pipeline's claim order)
   int64_t row_end(int64_t bi) const {
-    if (listed && !listed->empty()) return (*listed)[(size_t)bi];
+    if (!listed.empty()) return listed[(size_t)bi];
     return (bi + 1) * nT - bi * (bi + 1) / 2;
   }
 
@@ -526,7 +527,7 @@ int rvf_solve(rvf_session* s, rvf_mesh* m, const rvf_options* o, double* F_elem,
       dl.host = F_elem;
       dl.N = N;
       dl.nT = (N + kTile - 1) / kTile;
-      dl.listed = &w.row_end;
+      dl.listed = w.row_end;
       // rows without listed tiles are final once the quadrature-only kernel
       // ends: their columns may go out before any chunk, on the copy stream
       if ((e = cudaEventRecord(s->ev[7], s->stream)) != cudaSuccess ||
