@@ -293,6 +293,7 @@ __device__ __forceinline__ void gen_fast_fp64_body(const PairArgs& a, const doub
       // the chunk again below with k_fast's own arithmetic
       bool graze = false;
       uint32_t cast = 0;
+      const int ulim = npj - q0;
       for (int p = 0; p < npi; ++p) {
         double xi[3], ni[3];
 #pragma unroll
@@ -301,22 +302,23 @@ __device__ __forceinline__ void gen_fast_fp64_body(const PairArgs& a, const doub
           ni[c] = ib[((3 + c) * pm + p) * kTile];
         }
         const double wi = ib[(6 * pm + p) * kTile];
+        // straight-line over the block: a point q0 + u >= npj has zero
+        // normal and weight, so its dj is -0 and its K zero (it only must not
+        // ask for the grazing redo)
 #pragma unroll
         for (int u = 0; u < QB; ++u) {
-          if (q0 + u < npj) {
-            const double rx = xq[u][0] - xi[0], ry = xq[u][1] - xi[1], rz = xq[u][2] - xi[2];
-            const double r2 = (rx * rx + ry * ry) + rz * rz;
-            const double di = fma(ni[0], rx, fma(ni[1], ry, ni[2] * rz));
-            const double dj = -fma(nq[u][0], rx, fma(nq[u][1], ry, nq[u][2] * rz));
-            const double thr = 1e-10 * r2;
-            const bool big = !(r2 < 1e-30);
-            graze = graze || (big && (di * di <= thr || dj * dj <= thr));
-            double K = 0.0;
-            if (big && di > 0.0 && dj > 0.0)
-              K = DIM3 ? (di * dj) * rcp_nr(kPiD * (r2 * r2)) : (di * dj) * rcp_nr(2.0 * (r2 * sqrt(r2)));
-            cast += K > 0.0 ? 1 : 0;
-            inner[u] = fma(wi, K, inner[u]);
-          }
+          const double rx = xq[u][0] - xi[0], ry = xq[u][1] - xi[1], rz = xq[u][2] - xi[2];
+          const double r2 = (rx * rx + ry * ry) + rz * rz;
+          const double di = fma(ni[0], rx, fma(ni[1], ry, ni[2] * rz));
+          const double dj = -fma(nq[u][0], rx, fma(nq[u][1], ry, nq[u][2] * rz));
+          const double thr = 1e-10 * r2;
+          const bool big = !(r2 < 1e-30);
+          graze = graze || (u < ulim && big && (di * di <= thr || dj * dj <= thr));
+          double K = 0.0;
+          if (big && di > 0.0 && dj > 0.0)
+            K = DIM3 ? (di * dj) * rcp_nr(kPiD * (r2 * r2)) : (di * dj) * rcp_nr(2.0 * (r2 * sqrt(r2)));
+          cast += K > 0.0 ? 1 : 0;
+          inner[u] = fma(wi, K, inner[u]);
         }
       }
       if (__any_sync(kFull, graze) && graze) {  // rare: the chunk again, exactly as the ray pipeline forms it
@@ -422,17 +424,17 @@ __device__ __forceinline__ void gen_fast_mixed_body(const MixedArgs& a, const fl
         const float op0 = ibf[(0 * pm + p) * kTile], op1 = ibf[(1 * pm + p) * kTile], op2 = ibf[(2 * pm + p) * kTile];
         const float np0 = ibf[(3 * pm + p) * kTile], np1 = ibf[(4 * pm + p) * kTile], np2 = ibf[(5 * pm + p) * kTile];
         const float wp = ibf[(6 * pm + p) * kTile];
+        // straight-line over the block: a point q0 + u >= npj has zero
+        // normal, so its dj is -0 and its K zero
 #pragma unroll
         for (int u = 0; u < QB; ++u) {
-          if (q0 + u < npj) {
-            const float rx = d0 + (oq[u][0] - op0), ry = d1 + (oq[u][1] - op1), rz = d2 + (oq[u][2] - op2);
-            const float r2 = fmaf(rx, rx, fmaf(ry, ry, rz * rz));
-            const float di = fmaf(np0, rx, fmaf(np1, ry, np2 * rz));
-            const float dj = -fmaf(nq[u][0], rx, fmaf(nq[u][1], ry, nq[u][2] * rz));
-            const float K32 = (di > 0.0f && dj > 0.0f) ? (di * dj) * rcp_approx(3.14159265f * (r2 * r2)) : 0.0f;
-            cast += K32 > 0.0f ? 1 : 0;
-            inner[u] = fmaf(wp, K32, inner[u]);
-          }
+          const float rx = d0 + (oq[u][0] - op0), ry = d1 + (oq[u][1] - op1), rz = d2 + (oq[u][2] - op2);
+          const float r2 = fmaf(rx, rx, fmaf(ry, ry, rz * rz));
+          const float di = fmaf(np0, rx, fmaf(np1, ry, np2 * rz));
+          const float dj = -fmaf(nq[u][0], rx, fmaf(nq[u][1], ry, nq[u][2] * rz));
+          const float K32 = (di > 0.0f && dj > 0.0f) ? (di * dj) * rcp_approx(3.14159265f * (r2 * r2)) : 0.0f;
+          cast += K32 > 0.0f ? 1 : 0;
+          inner[u] = fmaf(wp, K32, inner[u]);
         }
       }
 #pragma unroll
@@ -1496,8 +1498,13 @@ __global__ void __launch_bounds__(256) k_resolve_mixed(const ResolveBatch* __res
 // rows -- no shared-memory staging, no block barriers, and the registers of
 // that loop alone (the chunked generation then skips these tiles).
 // ---------------------------------------------------------------------------
+// resident blocks of 256 per SM the quadrature-only kernels are compiled for
+#ifndef RVF_FAST_MIN_BLOCKS
+#define RVF_FAST_MIN_BLOCKS 2
+#endif
+
 template <bool DIM3, bool OCC>
-__global__ void __launch_bounds__(256, 2) k_fast_fp64(const PairArgs a, unsigned long long* task_ctr,
+__global__ void __launch_bounds__(256, RVF_FAST_MIN_BLOCKS) k_fast_fp64(const PairArgs a, unsigned long long* task_ctr,
                                                       unsigned long long* counters) {
   const int lane = threadIdx.x & 31;
   uint32_t n_pp = 0, n_rays = 0;
@@ -1524,7 +1531,7 @@ __global__ void __launch_bounds__(256, 2) k_fast_fp64(const PairArgs a, unsigned
 }
 
 template <bool OCC>
-__global__ void __launch_bounds__(256, 2) k_fast_mixed(const MixedArgs a, unsigned long long* task_ctr,
+__global__ void __launch_bounds__(256, RVF_FAST_MIN_BLOCKS) k_fast_mixed(const MixedArgs a, unsigned long long* task_ctr,
                                                        unsigned long long* counters) {
   const int lane = threadIdx.x & 31;
   uint32_t n_pp = 0, n_rays = 0;
