@@ -427,8 +427,11 @@ def serve_work(r) -> int:
 
 def run_serve(rvf, sess, size: str, local: int):
     """p50/p99 latency and throughput of a Poisson request stream through the
-    serving loop, offered at 80% of the estimated one-at-a-time service time;
-    a sample of the results is compared with plain FP64 one-at-a-time solves."""
+    serving loop, offered at 80% of the server's measured capacity; the
+    capacity (a burst of the stream's first 32 requests) is set beside the
+    same 32 requests solved one at a time, and a fixed sample of the served
+    results is compared with plain FP64 one-at-a-time solves."""
+    import math
     import queue
     import threading
     import numpy as np
@@ -437,59 +440,27 @@ def run_serve(rvf, sess, size: str, local: int):
     reqs = serve_requests(rvf, n_req, n_lo, n_hi)
     arrays = [rvf.mesh_desc_arrays(r["md"], r["obs"]) for r in reqs]
     pairs = [r["N"] * (r["N"] - 1) // 2 for r in reqs]
-    # one-at-a-time solves (the request's own options, then plain FP64) on a
-    # sample of both kinds: six quadrature requests and two Monte Carlo ones,
-    # evenly spread over the stream
-    quad = [k for k in range(n_req) if not reqs[k]["mc"]]
-    mc = [k for k in range(n_req) if reqs[k]["mc"]]
-    sample = quad[::max(1, len(quad) // 6)][:6] + mc[::max(1, len(mc) // 2)][:2]
-    # the served results of these are compared with plain FP64 solves
-    check = [k for k in sample if not reqs[k]["mc"]][:4]
-    F64 = {}
-    t_mixed, t_fp64, dF, t_solve_only = 0.0, 0.0, 0.0, 0.0
-    t_kind = {False: 0.0, True: 0.0}
-    for k in sample:
+    burst = list(range(min(n_req, 32)))
+    # the burst's requests one at a time through the public API: mesh upload,
+    # solve with the request's options (result left on the device), release --
+    # the work the server does per request; each after one warm-up solve of
+    # its own mesh (session buffers and launch graphs warm, as in a service)
+    t_alone, t_solve_only = [], []
+    for k in burst:
         r = reqs[k]
         dm = _abi.DeviceMesh(sess, arrays[k])
-        dm.solve(r["opts"])  # warm (tables, queues)
+        dm.solve(r["opts"])
         t0 = time.perf_counter()
         dm.solve(r["opts"])
-        t_solve_only += time.perf_counter() - t0
+        t_solve_only.append(time.perf_counter() - t0)
         dm.release()
-        # one request served alone: upload, solve (result on the device), release --
-        # the work the server does per request
         t0 = time.perf_counter()
         dm = _abi.DeviceMesh(sess, arrays[k])
         dm.solve(r["opts"])
         dm.release()
-        dt = time.perf_counter() - t0
-        dm = _abi.DeviceMesh(sess, arrays[k])
-        t_mixed += dt
-        t_kind[r["mc"]] += dt
-        o64 = rvf.make_options(r["nquad"], monte_carlo=r["mc"], n_samples=64, seed=r["opts"].seed, precision="fp64")
-        dm.solve(o64)  # warm
-        t0 = time.perf_counter()
-        dm.solve(o64)
-        t_fp64 += time.perf_counter() - t0
-        if k in check:
-            F64[k] = np.empty((r["N"], r["N"]), order="F")
-            dm.solve(rvf.make_options(r["nquad"], seed=0, precision="fp64"), F64[k])
-        dm.release()
-    # Offered load.  Each request's cost is its work (quadrature point pairs,
-    # or Monte Carlo sample pairs) weighted by the one-at-a-time time per unit
-    # of its kind on the sample.  The server's capacity in that cost is
-    # measured on a burst: the stream's first 32 requests submitted at once
-    # to a server of their own, each released when done.  The arrival rate
-    # puts the stream at 80% of that capacity.
-    work = [serve_work(r) for r in reqs]
-    sec_per_unit = {}
-    for kind in (False, True):
-        units = sum(work[k] for k in sample if reqs[k]["mc"] == kind)
-        sec_per_unit[kind] = t_kind[kind] / units if units else 0.0
-    if not sec_per_unit[True]:
-        sec_per_unit[True] = sec_per_unit[False]
-    cost = [work[k] * sec_per_unit[reqs[k]["mc"]] for k in range(n_req)]
-    burst = list(range(min(n_req, 32)))
+        t_alone.append(time.perf_counter() - t0)
+    # the burst: the same requests submitted at once to a server of their own,
+    # each released when done
     sv = _abi.Server(sess, admit_bytes=admit)
     t0 = time.perf_counter()
     rids = [sv.submit(arrays[k], reqs[k]["opts"]) for k in burst]
@@ -497,16 +468,44 @@ def run_serve(rvf, sess, size: str, local: int):
         sv.wait(rid, 3_600_000)
         sv.release(rid)
     t_burst = time.perf_counter() - t0
+    st_burst = sv.stats()
     sv.close()
+    # Offered load: each request's cost is its work (quadrature point pairs or
+    # Monte Carlo sample pairs) at the burst's measured rate for its kind;
+    # the arrival rate puts the stream at 80% of that capacity.
+    work = [serve_work(r) for r in reqs]
+    t_kind = {kind: sum(t_alone[n] for n, k in enumerate(burst) if reqs[k]["mc"] == kind) for kind in (False, True)}
+    sec_per_unit = {}
+    for kind in (False, True):
+        units = sum(work[k] for k in burst if reqs[k]["mc"] == kind)
+        sec_per_unit[kind] = t_kind[kind] / units if units else 0.0
+    if not sec_per_unit[True]:
+        sec_per_unit[True] = sec_per_unit[False]
+    cost = [work[k] * sec_per_unit[reqs[k]["mc"]] for k in range(n_req)]
     est_service = sum(cost) * t_burst / sum(cost[k] for k in burst)
     mean_service = est_service / n_req
-    sample_pairs = sum(pairs[k] for k in sample)
     lam = 0.8 / mean_service
     rng = np.random.default_rng(7)
     arrivals = np.cumsum(rng.exponential(1.0 / lam, size=n_req))
+    # a fixed sample of the quadrature requests (10% of the stream, at least
+    # 50 on the full one), evenly spread: 64 rows and columns of each served
+    # F against a plain FP64 one-at-a-time solve of the same mesh
+    quad = [k for k in range(n_req) if not reqs[k]["mc"]]
+    n_check = min(len(quad), max(math.ceil(0.1 * n_req), 50 if size == "full" else 4))
+    check = sorted({quad[int(c * len(quad) / n_check)] for c in range(n_check)})
+    ref_rows = {}
+    for k in check:
+        r = reqs[k]
+        N = r["N"]
+        dm = _abi.DeviceMesh(sess, arrays[k])
+        dm.solve(rvf.make_options(r["nquad"], seed=0, precision="fp64"))
+        idx = np.unique(np.linspace(0, N - 1, min(N, 64)).astype(np.int64))
+        ref_rows[k] = (idx,) + device_rows_cols(dm.result_device(), N, idx, local)
+        dm.release()
     sv = _abi.Server(sess, admit_bytes=admit)
     submitted = queue.Queue()
     err = []
+    dF, n_checked = 0.0, 0
 
     def submitter():
         t0 = time.perf_counter()
@@ -519,18 +518,18 @@ def run_serve(rvf, sess, size: str, local: int):
     th = threading.Thread(target=submitter)
     t_start = time.perf_counter()
     th.start()
-    # The client reads each result (the checked ones) and releases it as soon
-    # as it is done: a finished request keeps its device memory and its
-    # admission charge until rvf_release, so releasing only at the end would
-    # stall the stream once finished results fill the admission budget.
+    # The client reads each checked result on the device and releases every
+    # request as soon as it is done: a finished request keeps its device
+    # memory and its admission charge until rvf_release.
     for _ in range(n_req):
         k, rid = submitted.get()
         try:
             sv.wait(rid, 3_600_000)
-            if k in F64:
-                F = sv.result(rid)[0]
-                dF = max(dF, float(np.nanmax(np.abs(F - F64.pop(k)))))
-                del F
+            if k in ref_rows:
+                idx, rr, cc = ref_rows.pop(k)
+                rows, cols = device_rows_cols(sv.result_device(rid), reqs[k]["N"], idx, local)
+                dF = max(dF, float(np.nanmax(np.abs(rows - rr))), float(np.nanmax(np.abs(cols - cc))))
+                n_checked += 1
         except _abi.RVFError as e:
             err.append(str(e))
         try:
@@ -542,22 +541,25 @@ def run_serve(rvf, sess, size: str, local: int):
     st = sv.stats()
     sv.close()
     total_pairs = sum(pairs)
+    burst_pairs = sum(pairs[k] for k in burst)
     return {
         "metric": "serve latency and throughput", "requests": n_req, "failed": len(err),
         "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "mean_ms": st["mean_ms"],
         "throughput_pairs_per_s": total_pairs / wall, "wall_s": wall,
-        "one_at_a_time_pairs_per_s": sample_pairs / t_mixed,
-        "one_at_a_time": "each sampled request alone through the public API: mesh upload, solve with the "
-                         "request's options (result left on the device), release -- the work the server "
-                         "does per request",
-        "one_at_a_time_solve_only_pairs_per_s": sample_pairs / t_solve_only,
-        "one_at_a_time_fp64_pairs_per_s": sample_pairs / t_fp64,
-        "burst_pairs_per_s": sum(pairs[k] for k in burst) / t_burst,
+        "burst_pairs_per_s": burst_pairs / t_burst, "burst_s": t_burst, "burst_requests": len(burst),
+        "one_at_a_time_pairs_per_s": burst_pairs / sum(t_alone),
+        "one_at_a_time_s": sum(t_alone),
+        "one_at_a_time": "the burst's requests, each alone through the public API after a warm-up solve of its "
+                         "mesh: mesh upload, solve with the request's options (result left on the device), "
+                         "release -- the work the server does per request",
+        "one_at_a_time_solve_only_pairs_per_s": burst_pairs / sum(t_solve_only),
+        "burst_over_one_at_a_time": sum(t_alone) / t_burst,
         "lambda_per_s": lam, "offered_load": 0.8, "estimated_service_s": est_service,
-        "burst_s": t_burst, "burst_requests": len(burst),
-        "max_abs_dF_vs_fp64_solo": dF, "checked_requests": len(check),
+        "max_abs_dF_vs_fp64_solo": dF, "checked_requests": n_checked,
+        "check": "64 rows and columns of each checked served F against a plain FP64 one-at-a-time solve",
         "chunks": st["chunks"], "batched_requests": st["batched_requests"], "graph_replays": st["graph_replays"],
         "admit_bytes": admit, "admitted_bytes_peak": st["admitted_bytes_peak"],
+        "tuned_shapes": st["tuned"], "tuned_shapes_burst": st_burst["tuned"],
         "config": {"stream": f"{n_req} seeded requests (seed 5), Poisson arrivals, N log-uniform {n_lo}-{n_hi}, "
                              "plates / cube / cylinder, Tri3 / Quad4 / Quad8, nquad 2-5, 30% obstruction box, "
                              "20% Monte Carlo (64 samples), quadrature in mixed precision",

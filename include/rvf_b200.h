@@ -115,7 +115,10 @@ typedef struct {
   int32_t disable_tile_cull;  /* 1: no tile classification -- every shadow ray goes through the ray pipeline
                                  and every tile through its generation loop (same view factors; for testing) */
   int32_t fault_inject;       /* test hooks, 0 in production: RVF_FAULT_* bits */
-  int32_t reserved[4];
+  int32_t fast_points;        /* quadrature-only tiles: destination points per lane block -- 0 = by the
+                                 rule's size; FP64 2..4, mixed 2, 3, 4, 5, 7 or 8 (same view factors) */
+  int32_t fast_row_groups;    /* quadrature-only tiles: warp tasks per tile, 0/1 (whole tile), 2 or 4 */
+  int32_t reserved[2];
 } rvf_options;
 
 /* fault_inject bits (failure-path tests; each injects one host-visible failure
@@ -238,7 +241,9 @@ typedef struct {
   uint64_t admit_bytes;  /* admission budget for the admitted requests' footprints (0 = 70% of the session budget) */
   int32_t max_batch;     /* requests per batched launch, 1..64 (0 = 64) */
   int32_t use_graphs;    /* 0 or 1: replay a CUDA graph per launch shape; -1: eager launches */
-  int32_t autotune;      /* 0 = default grids; 1 = sweep grid sizes on the first chunks of each launch class */
+  int32_t autotune;      /* >= 0: sweep launch shapes -- the chunk grids on the first chunks of each launch
+                            class, the quadrature-only kernel's shape on the first admissions of each launch
+                            class and size class -- and keep the fastest; -1: default shapes */
   int32_t reserved[8];
 } rvf_server_opts;
 
@@ -254,6 +259,19 @@ typedef struct {
   int32_t reserved[8];
 } rvf_request_info;
 
+/* A launch shape the server's autotuner chose for one launch class (precision,
+ * occlusion, surface or curve mesh) and size class of requests. */
+typedef struct {
+  int32_t mixed, occlusion, dim3;
+  int32_t size_class;              /* requests with 4^k <= quadrature-only tiles < 4^(k+1) */
+  int32_t gen_blocks_per_sm;       /* chunked generation grid (0: occupancy default; chunk sweep) */
+  int32_t trace_blocks_per_sm;     /* traversal grid (0: occupancy default; chunk sweep) */
+  int32_t fast_points;             /* quadrature-only kernel: destination points per lane block */
+  int32_t fast_row_groups;         /*   and warp tasks per tile */
+  double fast_ms_per_gpp;          /* its measured time per 1e9 point pairs */
+  double fast_ms_per_gpp_default;  /*   and the default shape's (points by the rule, 1 task per tile) */
+} rvf_tuned_shape;
+
 typedef struct {
   int64_t submitted, completed, failed, canceled, in_flight;
   double p50_ms, p99_ms, mean_ms;  /* latency submit -> done of the completed requests */
@@ -263,7 +281,9 @@ typedef struct {
   int64_t graph_replays;
   int64_t batched_requests;        /* sum over chunks of the requests in the chunk */
   uint64_t admitted_bytes_peak;
-  int32_t reserved[8];
+  int32_t n_tuned;                 /* entries of tuned[] in use */
+  int32_t reserved[7];
+  rvf_tuned_shape tuned[8];        /* the autotuner's choices (the first 8 classes it finished) */
 } rvf_server_stats;
 
 int rvf_server_create(rvf_session* s, const rvf_server_opts* o, rvf_server** out);
@@ -281,6 +301,9 @@ int rvf_cancel(rvf_server* sv, int64_t id);
 /* Host copies of a done request's result (any pointer may be NULL). */
 int rvf_request_result(rvf_server* sv, int64_t id, double* F_elem, double* A_elem, double* F_group,
                        double* A_group, double* row_sums);
+/* Device addresses of a done request's F (n_elems^2, column-major) and A,
+ * valid until rvf_release: for callers that read the result on the GPU. */
+int rvf_request_result_device(rvf_server* sv, int64_t id, const double** F_dev, const double** A_dev);
 /* Frees a finished request's device memory and its admission charge. */
 int rvf_release(rvf_server* sv, int64_t id);
 int rvf_server_stats_get(rvf_server* sv, rvf_server_stats* st);

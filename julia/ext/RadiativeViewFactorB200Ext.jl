@@ -67,7 +67,9 @@ struct RvfOptions
     self_vf::Int32
     disable_tile_cull::Int32
     fault_inject::Int32
-    reserved::NTuple{4,Int32}
+    fast_points::Int32
+    fast_row_groups::Int32
+    reserved::NTuple{2,Int32}
 end
 
 struct RvfStats
@@ -127,6 +129,39 @@ struct RvfRequestInfo
     t_done_ms::Float64
     n_chunks::Int64
     reserved::NTuple{8,Int32}
+end
+
+struct RvfTunedShape
+    mixed::Int32
+    occlusion::Int32
+    dim3::Int32
+    size_class::Int32
+    gen_blocks_per_sm::Int32
+    trace_blocks_per_sm::Int32
+    fast_points::Int32
+    fast_row_groups::Int32
+    fast_ms_per_gpp::Float64
+    fast_ms_per_gpp_default::Float64
+end
+
+struct RvfServerStats
+    submitted::Int64
+    completed::Int64
+    failed::Int64
+    canceled::Int64
+    in_flight::Int64
+    p50_ms::Float64
+    p99_ms::Float64
+    mean_ms::Float64
+    wall_ms::Float64
+    pairs_done::Int64
+    chunks::Int64
+    graph_replays::Int64
+    batched_requests::Int64
+    admitted_bytes_peak::UInt64
+    n_tuned::Int32
+    reserved::NTuple{7,Int32}
+    tuned::NTuple{8,RvfTunedShape}
 end
 
 const RVF_PREC_FP64 = Int32(0)
@@ -256,6 +291,13 @@ function collect!(sv, id, N, G)
                 sv, id, F, A, Fg, Ag, C_NULL))
     check(ccall((:rvf_release, LIB), Cint, (Ptr{Cvoid}, Int64), sv, id))
     F, A, Fg, Ag
+end
+
+# counts, latency percentiles and the autotuner's chosen launch shapes
+function stats(sv)
+    st = Ref{RvfServerStats}()
+    check(ccall((:rvf_server_stats_get, LIB), Cint, (Ptr{Cvoid}, Ref{RvfServerStats}), sv, st))
+    st[]
 end
 
 end # module

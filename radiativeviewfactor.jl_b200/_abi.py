@@ -50,7 +50,7 @@ class Options(C.Structure):
                 ("geometric_soup", C.c_int32), ("mc_exclude_groups", C.c_int32), ("near_field_factor", C.c_double),
                 ("ray_log", _pu8), ("ray_log_pm", C.c_int32), ("disable_pair_lists", C.c_int32),
                 ("self_vf", C.c_int32), ("disable_tile_cull", C.c_int32), ("fault_inject", C.c_int32),
-                ("reserved", C.c_int32 * 4)]
+                ("fast_points", C.c_int32), ("fast_row_groups", C.c_int32), ("reserved", C.c_int32 * 2)]
 
 
 class Stats(C.Structure):
@@ -93,15 +93,28 @@ class RequestInfo(C.Structure):
                 ("t_done_ms", C.c_double), ("n_chunks", C.c_int64), ("reserved", C.c_int32 * 8)]
 
 
+class TunedShape(C.Structure):
+    _fields_ = [("mixed", C.c_int32), ("occlusion", C.c_int32), ("dim3", C.c_int32), ("size_class", C.c_int32),
+                ("gen_blocks_per_sm", C.c_int32), ("trace_blocks_per_sm", C.c_int32), ("fast_points", C.c_int32),
+                ("fast_row_groups", C.c_int32), ("fast_ms_per_gpp", C.c_double),
+                ("fast_ms_per_gpp_default", C.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 class ServerStats(C.Structure):
     _fields_ = [("submitted", C.c_int64), ("completed", C.c_int64), ("failed", C.c_int64),
                 ("canceled", C.c_int64), ("in_flight", C.c_int64), ("p50_ms", C.c_double),
                 ("p99_ms", C.c_double), ("mean_ms", C.c_double), ("wall_ms", C.c_double),
                 ("pairs_done", C.c_int64), ("chunks", C.c_int64), ("graph_replays", C.c_int64),
-                ("batched_requests", C.c_int64), ("admitted_bytes_peak", C.c_uint64), ("reserved", C.c_int32 * 8)]
+                ("batched_requests", C.c_int64), ("admitted_bytes_peak", C.c_uint64), ("n_tuned", C.c_int32),
+                ("reserved", C.c_int32 * 7), ("tuned", TunedShape * 8)]
 
     def as_dict(self):
-        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+        d = {k: getattr(self, k) for k, _ in self._fields_ if k not in ("reserved", "tuned")}
+        d["tuned"] = [self.tuned[k].as_dict() for k in range(min(self.n_tuned, 8))]
+        return d
 
 
 REQ_STATES = {0: "queued", 1: "running", 2: "done", 3: "failed", 4: "canceled"}
@@ -136,6 +149,7 @@ SIGNATURES = {
     "rvf_wait": (C.c_int, [_p, C.c_int64, C.c_int64, C.POINTER(RequestInfo)]),
     "rvf_cancel": (C.c_int, [_p, C.c_int64]),
     "rvf_request_result": (C.c_int, [_p, C.c_int64, _pd, _pd, _pd, _pd, _pd]),
+    "rvf_request_result_device": (C.c_int, [_p, C.c_int64, C.POINTER(_pd), C.POINTER(_pd)]),
     "rvf_release": (C.c_int, [_p, C.c_int64]),
     "rvf_server_stats_get": (C.c_int, [_p, C.POINTER(ServerStats)]),
 }
@@ -407,6 +421,12 @@ class Server:
                                           ptr(Fg, C.c_double), ptr(Ag, C.c_double), ptr(row_sums, C.c_double)),
               self.lib)
         return F, A, Fg, Ag
+
+    def result_device(self, rid: int):
+        """Device address of a done request's F (column-major N x N), valid until release."""
+        F = _pd()
+        check(self.lib.rvf_request_result_device(self.handle, rid, C.byref(F), None), self.lib)
+        return F
 
     def release(self, rid: int):
         check(self.lib.rvf_release(self.handle, rid), self.lib)

@@ -149,6 +149,7 @@ struct PairArgs {
   const uint8_t* tcls;           // tile classes and masks (kernels_cull.cu), or null
   const uint32_t* tmask;
   bool fast_done;                // tiles without ray work were integrated by k_fast_fp64: skip them
+  int fast_groups;               // k_fast_fp64 tasks per tile (1, 2 or 4 row groups)
   const int32_t* work;           // the tiles of the chunked pipeline in order (null: every tile)
 };
 
@@ -211,6 +212,7 @@ struct MixedArgs {
   const uint8_t* tcls;  // tile classes and masks (kernels_cull.cu), or null
   const uint32_t* tmask;
   bool fast_done;       // tiles without ray work were integrated by k_fast_mixed: skip them
+  int fast_groups;      // k_fast_mixed tasks per tile (1, 2 or 4 row groups)
   const int32_t* work;  // the tiles of the chunked pipeline in order (null: every tile)
 };
 
@@ -321,8 +323,13 @@ cudaError_t launch_plist(const TraceBatch* t, int sm_count, cudaStream_t st);
 // Tile classes and masks of one request (before its first chunk).
 cudaError_t launch_tile_class(const TileClassArgs& a, int sm_count, cudaStream_t st);
 // Every tile of one request that needs no shadow-ray work (its class), one
-// warp per tile, before the request's chunks; task_ctr: a zeroed counter.
-cudaError_t launch_fast(bool mixed, bool dim3, bool occ, const PairArgs& a, const MixedArgs& m,
+// warp per task (a.fast_groups tasks per tile), before the request's chunks;
+// qb points of the destination element per lane block (fast_qb_default: by
+// the rule's size; fast_qb_supported: the compiled blocks); task_ctr: a
+// zeroed counter.
+int fast_qb_default(bool mixed, int pmax);
+bool fast_qb_supported(bool mixed, int qb);
+cudaError_t launch_fast(bool mixed, bool dim3, bool occ, int qb, const PairArgs& a, const MixedArgs& m,
                         unsigned long long* task_ctr, unsigned long long* counters, int sm_count, cudaStream_t st);
 
 // A Quad8 pair sharing corner nodes (src/DuffyKernel.jl:95-115), i < j in the

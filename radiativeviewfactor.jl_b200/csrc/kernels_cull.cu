@@ -53,7 +53,7 @@ constexpr int kCullWarps = 4;
 
 // Pair masks: the capsule test over all 16 axes (1) or the pair lists' 4 (0).
 #ifndef RVF_MASK_FULL_AXES
-#define RVF_MASK_FULL_AXES 1
+#define RVF_MASK_FULL_AXES 0
 #endif
 
 // H = conv(B_1 u B_2) of two boxes (FP32 centres c and half extents h).

@@ -1503,25 +1503,40 @@ __global__ void __launch_bounds__(256) k_resolve_mixed(const ResolveBatch* __res
 #define RVF_FAST_MIN_BLOCKS 2
 #endif
 
-template <bool DIM3, bool OCC>
+// A task is one row group of a tile: groups = 1 (the whole tile: row
+// classes li0 = 0..7, each the rows li0, li0 + 8, ...), 2 or 4 (half or a
+// quarter of the row classes), so small meshes spread over more warps.  The
+// shape changes no sum: every pair is formed by the same loop.
+__device__ __forceinline__ bool fast_task(unsigned long long* task_ctr, int64_t n_tiles, int groups,
+                                          const uint8_t* tcls, uint8_t skip, int lane, int64_t& t, int& r0,
+                                          int& r1) {
+  for (;;) {
+    unsigned long long k = 0;
+    if (lane == 0) k = atomicAdd(task_ctr, 1ull);
+    k = __shfl_sync(kFull, k, 0);
+    const unsigned long long tile = k / (unsigned)groups;
+    if (tile >= (unsigned long long)n_tiles) return false;
+    if (tcls[tile] & skip) continue;
+    const int g = (int)(k - tile * (unsigned)groups), per = 8 / groups;
+    t = (int64_t)tile;
+    r0 = g * per;
+    r1 = r0 + per;
+    return true;
+  }
+}
+
+template <bool DIM3, bool OCC, int QB>
 __global__ void __launch_bounds__(256, RVF_FAST_MIN_BLOCKS) k_fast_fp64(const PairArgs a, unsigned long long* task_ctr,
-                                                      unsigned long long* counters) {
+                                                                       unsigned long long* counters) {
   const int lane = threadIdx.x & 31;
   uint32_t n_pp = 0, n_rays = 0;
-  for (;;) {
-    unsigned long long t = 0;
-    if (lane == 0) t = atomicAdd(task_ctr, 1ull);
-    t = __shfl_sync(kFull, t, 0);
-    if (t >= (unsigned long long)a.n_tiles) break;
-    if (a.tcls[t] & kClsSlow) continue;
+  int64_t t;
+  int r0, r1;
+  while (fast_task(task_ctr, a.n_tiles, a.fast_groups, a.tcls, kClsSlow, lane, t, r0, r1)) {
     int64_t bi, bj;
-    tile_coords((int64_t)t, a.nT, bi, bj);
+    tile_coords(t, a.nT, bi, bj);
     const double* ib = a.tab + bi * kComp * a.pmax * kTile;
-    if (a.pmax <= 3) {
-      for (int r = 0; r < 8; ++r) gen_fast_fp64_body<DIM3, OCC, 3>(a, ib, bi, bj, r, lane, n_pp, n_rays);
-    } else {
-      for (int r = 0; r < 8; ++r) gen_fast_fp64_body<DIM3, OCC, 4>(a, ib, bi, bj, r, lane, n_pp, n_rays);
-    }
+    for (int r = r0; r < r1; ++r) gen_fast_fp64_body<DIM3, OCC, QB>(a, ib, bi, bj, r, lane, n_pp, n_rays);
   }
   const uint64_t s_pp = warp_sum_u64(n_pp), s_rays = warp_sum_u64(n_rays);
   if (lane == 0 && counters) {
@@ -1530,30 +1545,18 @@ __global__ void __launch_bounds__(256, RVF_FAST_MIN_BLOCKS) k_fast_fp64(const Pa
   }
 }
 
-template <bool OCC>
+template <bool OCC, int QB>
 __global__ void __launch_bounds__(256, RVF_FAST_MIN_BLOCKS) k_fast_mixed(const MixedArgs a, unsigned long long* task_ctr,
-                                                       unsigned long long* counters) {
+                                                                        unsigned long long* counters) {
   const int lane = threadIdx.x & 31;
   uint32_t n_pp = 0, n_rays = 0;
-  for (;;) {
-    unsigned long long t = 0;
-    if (lane == 0) t = atomicAdd(task_ctr, 1ull);
-    t = __shfl_sync(kFull, t, 0);
-    if (t >= (unsigned long long)a.n_tiles) break;
-    if (a.tcls[t] & (kClsSlow | kClsNear | kClsTiny)) continue;
+  int64_t t;
+  int r0, r1;
+  while (fast_task(task_ctr, a.n_tiles, a.fast_groups, a.tcls, kClsSlow | kClsNear | kClsTiny, lane, t, r0, r1)) {
     int64_t bi, bj;
-    tile_coords((int64_t)t, a.nT, bi, bj);
+    tile_coords(t, a.nT, bi, bj);
     const float* ib = a.tabf + bi * kComp * a.pmax * kTile;
-    const int pm = a.pmax;
-    if (pm == 7 || pm == 13 || pm == 49) {
-      for (int r = 0; r < 8; ++r) gen_fast_mixed_body<OCC, 7>(a, ib, bi, bj, r, lane, n_pp, n_rays);
-    } else if (pm == 5 || pm == 25) {
-      for (int r = 0; r < 8; ++r) gen_fast_mixed_body<OCC, 5>(a, ib, bi, bj, r, lane, n_pp, n_rays);
-    } else if (pm == 3 || pm == 9) {
-      for (int r = 0; r < 8; ++r) gen_fast_mixed_body<OCC, 3>(a, ib, bi, bj, r, lane, n_pp, n_rays);
-    } else {
-      for (int r = 0; r < 8; ++r) gen_fast_mixed_body<OCC, 8>(a, ib, bi, bj, r, lane, n_pp, n_rays);
-    }
+    for (int r = r0; r < r1; ++r) gen_fast_mixed_body<OCC, QB>(a, ib, bi, bj, r, lane, n_pp, n_rays);
   }
   const uint64_t s_pp = warp_sum_u64(n_pp), s_rays = warp_sum_u64(n_rays);
   if (lane == 0 && counters) {
@@ -1565,7 +1568,18 @@ __global__ void __launch_bounds__(256, RVF_FAST_MIN_BLOCKS) k_fast_mixed(const M
 // ---------------------------------------------------------------------------
 // host launchers
 // ---------------------------------------------------------------------------
-cudaError_t launch_fast(bool mixed, bool dim3, bool occ, const PairArgs& a, const MixedArgs& m,
+int fast_qb_default(bool mixed, int pmax) {
+  if (!mixed) return pmax <= 3 ? 3 : 4;
+  if (pmax == 7 || pmax == 13 || pmax == 49) return 7;
+  if (pmax == 5 || pmax == 25) return 5;
+  if (pmax == 3 || pmax == 9) return 3;
+  return 8;
+}
+bool fast_qb_supported(bool mixed, int qb) {
+  return mixed ? (qb == 2 || qb == 3 || qb == 4 || qb == 5 || qb == 7 || qb == 8) : (qb >= 2 && qb <= 4);
+}
+
+cudaError_t launch_fast(bool mixed, bool dim3, bool occ, int qb, const PairArgs& a, const MixedArgs& m,
                         unsigned long long* task_ctr, unsigned long long* counters, int sm_count, cudaStream_t st) {
   auto launch = [&](auto fn, const auto& args) -> cudaError_t {
     int per_sm = 1;
@@ -1573,9 +1587,28 @@ cudaError_t launch_fast(bool mixed, bool dim3, bool occ, const PairArgs& a, cons
     fn<<<(unsigned)(sm_count * per_sm), 256, 0, st>>>(args, task_ctr, counters);
     return cudaGetLastError();
   };
-  if (mixed) return occ ? launch(k_fast_mixed<true>, m) : launch(k_fast_mixed<false>, m);
-  if (dim3) return occ ? launch(k_fast_fp64<true, true>, a) : launch(k_fast_fp64<true, false>, a);
-  return occ ? launch(k_fast_fp64<false, true>, a) : launch(k_fast_fp64<false, false>, a);
+  if (mixed) {
+    switch (qb) {
+      case 2: return occ ? launch(k_fast_mixed<true, 2>, m) : launch(k_fast_mixed<false, 2>, m);
+      case 3: return occ ? launch(k_fast_mixed<true, 3>, m) : launch(k_fast_mixed<false, 3>, m);
+      case 4: return occ ? launch(k_fast_mixed<true, 4>, m) : launch(k_fast_mixed<false, 4>, m);
+      case 5: return occ ? launch(k_fast_mixed<true, 5>, m) : launch(k_fast_mixed<false, 5>, m);
+      case 7: return occ ? launch(k_fast_mixed<true, 7>, m) : launch(k_fast_mixed<false, 7>, m);
+      case 8: return occ ? launch(k_fast_mixed<true, 8>, m) : launch(k_fast_mixed<false, 8>, m);
+      default: return cudaErrorInvalidValue;
+    }
+  }
+  switch (qb) {
+#define RVF_FAST64(Q)                                                                          \
+  case Q:                                                                                      \
+    if (dim3) return occ ? launch(k_fast_fp64<true, true, Q>, a) : launch(k_fast_fp64<true, false, Q>, a); \
+    return occ ? launch(k_fast_fp64<false, true, Q>, a) : launch(k_fast_fp64<false, false, Q>, a);
+    RVF_FAST64(2)
+    RVF_FAST64(3)
+    RVF_FAST64(4)
+#undef RVF_FAST64
+    default: return cudaErrorInvalidValue;
+  }
 }
 size_t gen_smem_bytes(bool mixed, int pmax, bool occ) {
   // tile block, then (occlusion) the per-warp FP64 staging (mixed) and the

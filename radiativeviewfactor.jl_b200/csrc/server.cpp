@@ -147,6 +147,16 @@ struct rvf_server {
     bool done = false;
   };
   std::map<uint64_t, Tune> tune;
+  // shape sweep of the quadrature-only kernel per launch class and size
+  // class, one candidate per admission: ms per 1e9 point pairs
+  struct FastTune {
+    size_t next = 0;
+    double score[4] = {0, 0, 0, 0};
+    int qb = 0, groups = 1;
+    bool done = false;
+  };
+  std::map<uint64_t, FastTune> ftune;
+  std::vector<uint64_t> ftune_done;  // keys in the order their sweeps ended
 
   double now_ms() const { return std::chrono::duration<double, std::milli>(Clock::now() - t0).count(); }
 };
@@ -162,6 +172,32 @@ constexpr double kChunkSamplePairs = 1e8;
 
 const int kCand[][2] = {{0, 0}, {2, 0}, {0, 2}, {2, 2}};
 constexpr int kNCand = 4;
+
+// Candidate shapes of the quadrature-only kernel: the default (points by the
+// rule, whole tiles), about half the points per lane block (fewer registers,
+// more resident warps), and 2 or 4 warp tasks per tile (more tasks than
+// warps for small meshes).
+constexpr int kNFastCand = 4;
+void fast_cand(bool mixed, int pmax, size_t c, int& qb, int& groups) {
+  const int d = fast_qb_default(mixed, pmax);
+  qb = d;
+  groups = 1;
+  if (c == 1) qb = std::max(2, (d + 1) / 2);
+  if (c == 2) groups = 2;
+  if (c == 3) groups = 4;
+}
+
+// launch class: precision, surface or curve mesh, occlusion
+uint64_t class_key(const Req* r) {
+  return (uint64_t)r->w.mixed | ((uint64_t)r->w.dim3 << 1) | ((uint64_t)r->w.occ << 2);
+}
+
+// launch class and size class (4^k <= quadrature-only tiles < 4^(k+1))
+uint64_t fast_key(uint64_t class_key, int64_t n_fast_tiles) {
+  int k = 0;
+  while (k < 15 && ((int64_t)1 << (2 * (k + 1))) <= n_fast_tiles) ++k;
+  return class_key | ((uint64_t)k << 8);
+}
 
 void finish(rvf_server* sv, Req* r, int state, int status) {  // sv->mu held
   r->state = state;
@@ -223,9 +259,46 @@ int admit_one(rvf_server* sv, Req* r) {
   m->has_result = false;
   if (N == 1) cudaMemsetAsync(m->F.ptr, 0, sizeof(double), s->stream);
   if ((rc = wave_prepare(s, m, r->T, &r->opts, nullptr, r->w, nullptr))) return rc;
+  // the quadrature-only kernel's shape: the caller's, the tuned one, or the
+  // next candidate of this launch class and size class
+  const bool own = r->opts.fast_points != 0 || r->opts.fast_row_groups != 0;
+  const uint64_t fkey = fast_key(class_key(r), r->w.n_fast_tiles);
+  int cand = -1;
+  if (!own && r->w.n_fast_tiles > 0) {
+    std::lock_guard<std::mutex> lk2(sv->mu);
+    rvf_server::FastTune& t = sv->ftune[fkey];
+    if (t.done) {
+      r->w.fast_qb = t.qb;
+      r->w.fast_groups = t.groups;
+    } else if (sv->o.autotune >= 0) {
+      cand = (int)t.next;
+      fast_cand(r->w.mixed, r->w.pmax, t.next, r->w.fast_qb, r->w.fast_groups);
+    }
+  }
+  cudaEventRecord(s->ev[0], s->stream);
   if ((rc = wave_fast(s, r->w, nullptr))) return rc;
+  cudaEventRecord(s->ev[1], s->stream);
   const cudaError_t e = cudaStreamSynchronize(s->stream);
-  return e == cudaSuccess ? RVF_OK : cuda_err(e, "request set-up");
+  if (e != cudaSuccess) return cuda_err(e, "request set-up");
+  if (cand >= 0) {
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, s->ev[0], s->ev[1]);
+    const double gpp = (double)r->w.n_fast_tiles * kTile * kTile * r->w.pmax * r->w.pmax * 1e-9;
+    std::lock_guard<std::mutex> lk2(sv->mu);
+    rvf_server::FastTune& t = sv->ftune[fkey];
+    if (!t.done && t.next == (size_t)cand) {
+      t.score[cand] = (double)ms / gpp;
+      if (++t.next >= (size_t)kNFastCand) {
+        size_t b = 0;
+        for (size_t c = 1; c < (size_t)kNFastCand; ++c)
+          if (t.score[c] < t.score[b]) b = c;
+        fast_cand(r->w.mixed, r->w.pmax, b, t.qb, t.groups);
+        t.done = true;
+        sv->ftune_done.push_back(fkey);
+      }
+    }
+  }
+  return RVF_OK;
 }
 
 // Self pairs, Duffy pairs, the one-element case and the reductions of a
@@ -267,9 +340,6 @@ int finish_quad(Session* s, Req* r) {
   return RVF_OK;
 }
 
-uint64_t class_key(const Req* r) {
-  return (uint64_t)r->w.mixed | ((uint64_t)r->w.dim3 << 1) | ((uint64_t)r->w.occ << 2);
-}
 
 // One batched chunk over reqs (same class); finishes the requests it completes.
 void run_chunk(rvf_server* sv, std::vector<Req*>& batch) {
@@ -663,6 +733,19 @@ int rvf_cancel(rvf_server* sv, int64_t id) try {
   return exception_status();
 }
 
+int rvf_request_result_device(rvf_server* sv, int64_t id, const double** F_dev, const double** A_dev) try {
+  if (!sv) return set_err(RVF_EINVAL, "null server");
+  std::lock_guard<std::mutex> lk(sv->mu);
+  Req* r = find(sv, id);
+  if (!r) return set_err(RVF_EINVAL, "unknown request %lld", (long long)id);
+  if (r->state != RVF_REQ_DONE || !r->m) return set_err(RVF_EBUSY, "request %lld has no result", (long long)id);
+  if (F_dev) *F_dev = r->m->F.as<double>();
+  if (A_dev) *A_dev = r->m->result_area;
+  return RVF_OK;
+} catch (...) {
+  return exception_status();
+}
+
 int rvf_request_result(rvf_server* sv, int64_t id, double* F_elem, double* A_elem, double* F_group,
                        double* A_group, double* row_sums) try {
   if (!sv) return set_err(RVF_EINVAL, "null server");
@@ -737,6 +820,26 @@ int rvf_server_stats_get(rvf_server* sv, rvf_server_stats* st) try {
   st->graph_replays = sv->graph_replays;
   st->batched_requests = sv->batched;
   st->admitted_bytes_peak = sv->admitted_peak;
+  for (uint64_t key : sv->ftune_done) {
+    if (st->n_tuned >= 8) break;
+    const rvf_server::FastTune& f = sv->ftune[key];
+    rvf_tuned_shape& o = st->tuned[st->n_tuned++];
+    o.mixed = (int32_t)(key & 1);
+    o.dim3 = (int32_t)((key >> 1) & 1);
+    o.occlusion = (int32_t)((key >> 2) & 1);
+    o.size_class = (int32_t)((key >> 8) & 15);
+    const auto g = sv->tune.find(key & 0xff);
+    if (g != sv->tune.end() && g->second.done) {
+      o.gen_blocks_per_sm = g->second.gen;
+      o.trace_blocks_per_sm = g->second.trace;
+    }
+    o.fast_points = f.qb;
+    o.fast_row_groups = f.groups;
+    double best = f.score[0];
+    for (int c = 1; c < kNFastCand; ++c) best = std::min(best, f.score[c]);
+    o.fast_ms_per_gpp = best;
+    o.fast_ms_per_gpp_default = f.score[0];
+  }
   return RVF_OK;
 } catch (...) {
   return exception_status();

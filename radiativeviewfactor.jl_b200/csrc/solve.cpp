@@ -75,9 +75,14 @@ int validate_options(const rvf_mesh* m, const rvf_options* o) {
   if (o->fault_inject & ~(RVF_FAULT_CLAIM | RVF_FAULT_ALLOC))
     return set_err(RVF_EINVAL, "unknown fault_inject bits 0x%x", o->fault_inject);
   if (o->self_vf != 0 && o->self_vf != 1) return set_err(RVF_EINVAL, "self_vf must be 0 or 1, got %d", o->self_vf);
+  if (o->fast_points &&
+      !fast_qb_supported(o->precision == RVF_PREC_MIXED && m->dim == 2 && o->method == RVF_METHOD_QUADRATURE,
+                         o->fast_points))
+    return set_err(RVF_EINVAL, "fast_points %d is not a compiled block for this precision", o->fast_points);
+  if (o->fast_row_groups != 0 && o->fast_row_groups != 1 && o->fast_row_groups != 2 && o->fast_row_groups != 4)
+    return set_err(RVF_EINVAL, "fast_row_groups must be 0, 1, 2 or 4, got %d", o->fast_row_groups);
   if (o->self_vf && o->method == RVF_METHOD_MONTE_CARLO)
     return set_err(RVF_EINVAL, "self_vf is supported with quadrature only");
-  (void)m;
   return RVF_OK;
 }
 

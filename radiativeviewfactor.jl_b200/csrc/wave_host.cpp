@@ -87,6 +87,8 @@ int wave_prepare(Session* s, rvf_mesh* m, Tables* T, const rvf_options* o, uint8
   w.dim3 = (m->dim == 2);
   w.pmax = T->pmax;
   if (o->fault_inject & RVF_FAULT_CLAIM) w.claim_retries = 0;
+  w.fast_qb = o->fast_points;
+  w.fast_groups = o->fast_row_groups > 0 ? o->fast_row_groups : 1;
   PairArgs& a = w.pa;
   a.N = N;
   a.nT = (N + kTile - 1) / kTile;
@@ -205,6 +207,7 @@ int wave_prepare(Session* s, rvf_mesh* m, Tables* T, const rvf_options* o, uint8
       a.work = T->twork.as<int32_t>();
       w.ma.work = a.work;
       w.n_tiles = (int64_t)work.size();
+      w.n_fast_tiles = a.n_tiles - w.n_tiles;
     }
   }
   TraceArgs& ta = w.ta;
@@ -232,9 +235,11 @@ int wave_fast(Session* s, WaveReq& w, int64_t* n_kernels) {
   if (!w.pa.tcls || w.pa.ray_log || w.pa.n_tiles == 0) return 0;
   int rc = 0;
   if (!s->fast_ctr.ptr && (rc = s->fast_ctr.alloc(s, 256))) return rc;
+  w.pa.fast_groups = w.ma.fast_groups = w.fast_groups;
+  const int qb = w.fast_qb > 0 ? w.fast_qb : fast_qb_default(w.mixed, w.pmax);
   cudaError_t e = cudaMemsetAsync(s->fast_ctr.ptr, 0, sizeof(unsigned long long), s->stream);
   if (e == cudaSuccess)
-    e = launch_fast(w.mixed, w.dim3, w.occ, w.pa, w.ma, s->fast_ctr.as<unsigned long long>(),
+    e = launch_fast(w.mixed, w.dim3, w.occ, qb, w.pa, w.ma, s->fast_ctr.as<unsigned long long>(),
                     s->counters.as<unsigned long long>(), s->sm_count, s->stream);
   if (e != cudaSuccess) return cuda_err(e, "quadrature-only tiles launch");
   if (n_kernels) *n_kernels += 1;

@@ -22,6 +22,9 @@ struct WaveReq {
   std::vector<int64_t> row_end;  // with a tile list: listed tiles in tile rows 0..r (for the F download)
   int64_t claimed = 0;  // tiles integrated so far
   int claim_retries = 4096;  // compare-and-swap attempts of a tile claim (0: every claim gives up)
+  int fast_qb = 0;           // quadrature-only kernel shape: points per lane block (0: by the rule)
+  int fast_groups = 1;       //   and warp tasks per tile
+  int64_t n_fast_tiles = 0;  // tiles of the quadrature-only kernel
   const NodeD* nodes_d = nullptr;
   const NodeF* nodes_f = nullptr;
   bool done() const { return claimed >= n_tiles; }

@@ -63,7 +63,7 @@ def test_struct_layouts_match_compiled_header(tmp_path, rvf):
         pytest.skip("gcc not available")
     structs = {"rvf_session_opts": _abi.SessionOpts, "rvf_mesh_desc": _abi.MeshDesc, "rvf_options": _abi.Options,
                "rvf_stats": _abi.Stats, "rvf_server_opts": _abi.ServerOpts, "rvf_request_info": _abi.RequestInfo,
-               "rvf_server_stats": _abi.ServerStats}
+               "rvf_server_stats": _abi.ServerStats, "rvf_tuned_shape": _abi.TunedShape}
     lines = ['#include <stdio.h>', '#include <stddef.h>', f'#include "{HEADER}"', 'int main(void) {']
     for cname, ct in structs.items():
         lines.append(f'  printf("{cname} size %zu\\n", sizeof({cname}));')

@@ -131,3 +131,37 @@ def test_cancel_timeout_release(rvf, session):
         assert st["completed"] == 1 and st["canceled"] == 1 and st["in_flight"] == 0
     finally:
         sv.close()
+
+
+def test_autotuned_shapes_reported_and_identical(rvf, session):
+    """The first admissions of a launch class and size class each run one
+    candidate shape of the quadrature-only kernel; the sweep's choice is
+    reported in rvf_server_stats, and every result stays bit-identical to
+    rvf_solve whatever shape computed it."""
+    from rvf_b200 import _abi
+    m = rvf.meshes
+    mk = rvf.make_options
+    mix = []
+    for prec in ("fp64", "mixed"):
+        md = m.cube_enclosure(10, family="tri3", box_m=3)
+        mix += [(md, [7], mk(3, seed=0, precision=prec))] * 6
+    expect = {prec: solo(rvf, session, mix[k][0], [7], mix[k][2]) for k, prec in ((0, "fp64"), (6, "mixed"))}
+    sv = _abi.Server(session, max_batch=1)
+    try:
+        ids = [sv.submit(rvf.mesh_desc_arrays(md, obs), o) for md, obs, o in mix]
+        for k, rid in enumerate(ids):
+            sv.wait(rid, 120000)
+            F, A, Fg, Ag = sv.result(rid)
+            eF, eA, eFg, eAg = expect["fp64" if k < 6 else "mixed"]
+            assert same(F, eF) and same(A, eA) and same(Fg, eFg), f"request {k}"
+            sv.release(rid)
+        st = sv.stats()
+        assert st["completed"] == len(mix)
+        tuned = st["tuned"]
+        assert sorted(t["mixed"] for t in tuned) == [0, 1], tuned
+        for t in tuned:
+            assert t["occlusion"] == 1 and t["dim3"] == 1
+            assert t["fast_points"] >= 2 and t["fast_row_groups"] in (1, 2, 4)
+            assert 0 < t["fast_ms_per_gpp"] <= t["fast_ms_per_gpp_default"]
+    finally:
+        sv.close()

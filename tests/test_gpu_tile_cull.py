@@ -116,3 +116,35 @@ def test_near_tiles_keep_fp64_in_mixed(rvf, orc, session):
         F, A, st = solve(rvf, session, md, 4, [], precision="mixed", near=near)
         assert np.max(np.abs(F - Fo)) <= 1e-6
         assert (st["n_pairs_fp64"] > 0) == (near > 0)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_fast_kernel_shapes_bit_identical(rvf, session, precision):
+    """Every compiled shape of the quadrature-only kernel (points per lane
+    block, warp tasks per tile) forms each pair by the same loop: F is
+    identical bit for bit, with and without occlusion."""
+    from rvf_b200 import _abi
+    cases = [(rvf.meshes.cube_enclosure(9, family="tri3", box_m=3), [7], 3),
+             (rvf.meshes.parallel_plates(10, "quad"), [], 3)]
+    points = (2, 3, 4) if precision == "fp64" else (2, 3, 4, 5, 7, 8)
+    for md, obs, nquad in cases:
+        dm = _abi.DeviceMesh(session, rvf.mesh_desc_arrays(md, obs))
+        try:
+            N = md.n_elems
+            ref = None
+            for qb in (0,) + points:
+                for groups in (1, 2, 4):
+                    o = rvf.make_options(nquad, precision=precision, seed=0)
+                    o.fast_points, o.fast_row_groups = qb, groups
+                    F = np.empty((N, N), order="F")
+                    dm.solve(o, F)
+                    if ref is None:
+                        ref = F
+                    assert np.array_equal(F, ref, equal_nan=True), (qb, groups)
+            o = rvf.make_options(nquad, precision=precision, seed=0)
+            o.fast_points = 6
+            with pytest.raises(_abi.RVFError) as ei:
+                dm.solve(o, np.empty((N, N), order="F"))
+            assert ei.value.status == _abi.RVF_EINVAL
+        finally:
+            dm.release()

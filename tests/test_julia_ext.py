@@ -20,7 +20,8 @@ HEADER = ROOT / "include" / "rvf_b200.h"
 SCALARS = {"Int8": 1, "UInt8": 1, "Int32": 4, "UInt32": 4, "Int64": 8, "UInt64": 8, "Float64": 8, "Float32": 4,
            "Cint": 4, "Csize_t": 8}
 STRUCTS = {"RvfMeshDesc": "rvf_mesh_desc", "RvfOptions": "rvf_options", "RvfStats": "rvf_stats",
-           "RvfServerOpts": "rvf_server_opts", "RvfRequestInfo": "rvf_request_info"}
+           "RvfServerOpts": "rvf_server_opts", "RvfRequestInfo": "rvf_request_info",
+           "RvfTunedShape": "rvf_tuned_shape", "RvfServerStats": "rvf_server_stats"}
 
 
 def julia_structs():
@@ -41,6 +42,10 @@ def size_align(t):
     """(size, alignment) of a Julia field type in C layout."""
     if t in SCALARS:
         return SCALARS[t], SCALARS[t]
+    js = julia_structs()
+    if t in js:  # a nested struct of the extension
+        offs, size = julia_layout(js[t])
+        return size, max(size_align(ft)[1] for _, ft in js[t])
     if t.startswith("Ptr{"):
         return 8, 8
     m = re.fullmatch(r"NTuple\{(\d+),\s*(.+)\}", t)
@@ -100,7 +105,10 @@ def test_extension_covers_every_c_field():
         end = re.search(r"\}\s*" + cname + ";", hdr).start()
         body = hdr[hdr.rindex("typedef struct {", 0, end) + len("typedef struct {"):end]
         body = re.sub(r"/\*.*?\*/", "", body, flags=re.S)
-        names = re.findall(r"(\w+)(?:\[\d+\])?\s*;", body)
+        names = []
+        for decl in body.split(";"):  # "const type* a, b, c[4]" -> a, b, c
+            if decl.strip():
+                names += [re.search(r"(\w+)\s*(?:\[\w+\])?\s*$", v).group(1) for v in decl.split(",")]
         assert names == [f for f, _ in js[jname]], (jname, names)
 
 
