@@ -155,6 +155,10 @@ struct rvf_server {
     int qb = 0, groups = 1;
     bool done = false;
   };
+  // ftune and ftune_done have a lock of their own, taken last: admission
+  // holds the session lock, and rvf_release takes the session lock inside
+  // the server lock
+  std::mutex tune_mu;
   std::map<uint64_t, FastTune> ftune;
   std::vector<uint64_t> ftune_done;  // keys in the order their sweeps ended
 
@@ -265,7 +269,7 @@ int admit_one(rvf_server* sv, Req* r) {
   const uint64_t fkey = fast_key(class_key(r), r->w.n_fast_tiles);
   int cand = -1;
   if (!own && r->w.n_fast_tiles > 0) {
-    std::lock_guard<std::mutex> lk2(sv->mu);
+    std::lock_guard<std::mutex> lk2(sv->tune_mu);
     rvf_server::FastTune& t = sv->ftune[fkey];
     if (t.done) {
       r->w.fast_qb = t.qb;
@@ -284,7 +288,7 @@ int admit_one(rvf_server* sv, Req* r) {
     float ms = 0.f;
     cudaEventElapsedTime(&ms, s->ev[0], s->ev[1]);
     const double gpp = (double)r->w.n_fast_tiles * kTile * kTile * r->w.pmax * r->w.pmax * 1e-9;
-    std::lock_guard<std::mutex> lk2(sv->mu);
+    std::lock_guard<std::mutex> lk2(sv->tune_mu);
     rvf_server::FastTune& t = sv->ftune[fkey];
     if (!t.done && t.next == (size_t)cand) {
       t.score[cand] = (double)ms / gpp;
@@ -820,6 +824,7 @@ int rvf_server_stats_get(rvf_server* sv, rvf_server_stats* st) try {
   st->graph_replays = sv->graph_replays;
   st->batched_requests = sv->batched;
   st->admitted_bytes_peak = sv->admitted_peak;
+  std::lock_guard<std::mutex> lk2(sv->tune_mu);
   for (uint64_t key : sv->ftune_done) {
     if (st->n_tuned >= 8) break;
     const rvf_server::FastTune& f = sv->ftune[key];
