@@ -460,16 +460,19 @@ def run_serve(rvf, sess, size: str, local: int):
         dm.release()
         t_alone.append(time.perf_counter() - t0)
     # the burst: the same requests submitted at once to a server of their own,
-    # each released when done
-    sv = _abi.Server(sess, admit_bytes=admit)
-    t0 = time.perf_counter()
-    rids = [sv.submit(arrays[k], reqs[k]["opts"]) for k in burst]
-    for rid in rids:
-        sv.wait(rid, 3_600_000)
-        sv.release(rid)
-    t_burst = time.perf_counter() - t0
-    st_burst = sv.stats()
-    sv.close()
+    # each released when done; timed on its second pass, when the session's
+    # buffer cache holds F buffers for the burst's concurrent requests (as the
+    # one-at-a-time solves above reuse theirs: a service in steady state)
+    for rep in range(2):
+        sv = _abi.Server(sess, admit_bytes=admit)
+        t0 = time.perf_counter()
+        rids = [sv.submit(arrays[k], reqs[k]["opts"]) for k in burst]
+        for rid in rids:
+            sv.wait(rid, 3_600_000)
+            sv.release(rid)
+        t_burst = time.perf_counter() - t0
+        st_burst = sv.stats()
+        sv.close()
     # Offered load: each request's cost is its work (quadrature point pairs or
     # Monte Carlo sample pairs) at the burst's measured rate for its kind;
     # the arrival rate puts the stream at 80% of that capacity.

@@ -260,7 +260,9 @@ typedef struct {
 } rvf_request_info;
 
 /* A launch shape the server's autotuner chose for one launch class (precision,
- * occlusion, surface or curve mesh) and size class of requests. */
+ * occlusion, surface or curve mesh, points per element) and size class of
+ * requests.  The quadrature-only kernel's candidates all run on the class's
+ * first request (each forms the same F), and the fastest is kept. */
 typedef struct {
   int32_t mixed, occlusion, dim3;
   int32_t size_class;              /* requests with 4^k <= quadrature-only tiles < 4^(k+1) */
@@ -268,6 +270,8 @@ typedef struct {
   int32_t trace_blocks_per_sm;     /* traversal grid (0: occupancy default; chunk sweep) */
   int32_t fast_points;             /* quadrature-only kernel: destination points per lane block */
   int32_t fast_row_groups;         /*   and warp tasks per tile */
+  int32_t rule_points;             /* quadrature points per element of the class's rule */
+  int32_t reserved;
   double fast_ms_per_gpp;          /* its measured time per 1e9 point pairs */
   double fast_ms_per_gpp_default;  /*   and the default shape's (points by the rule, 1 task per tile) */
 } rvf_tuned_shape;

@@ -140,6 +140,8 @@ struct RvfTunedShape
     trace_blocks_per_sm::Int32
     fast_points::Int32
     fast_row_groups::Int32
+    rule_points::Int32
+    reserved::Int32
     fast_ms_per_gpp::Float64
     fast_ms_per_gpp_default::Float64
 end

@@ -96,11 +96,12 @@ class RequestInfo(C.Structure):
 class TunedShape(C.Structure):
     _fields_ = [("mixed", C.c_int32), ("occlusion", C.c_int32), ("dim3", C.c_int32), ("size_class", C.c_int32),
                 ("gen_blocks_per_sm", C.c_int32), ("trace_blocks_per_sm", C.c_int32), ("fast_points", C.c_int32),
-                ("fast_row_groups", C.c_int32), ("fast_ms_per_gpp", C.c_double),
+                ("fast_row_groups", C.c_int32), ("rule_points", C.c_int32), ("reserved", C.c_int32),
+                ("fast_ms_per_gpp", C.c_double),
                 ("fast_ms_per_gpp_default", C.c_double)]
 
     def as_dict(self):
-        return {k: getattr(self, k) for k, _ in self._fields_}
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
 
 
 class ServerStats(C.Structure):

@@ -328,6 +328,7 @@ cudaError_t launch_tile_class(const TileClassArgs& a, int sm_count, cudaStream_t
 // the rule's size; fast_qb_supported: the compiled blocks); task_ctr: a
 // zeroed counter.
 int fast_qb_default(bool mixed, int pmax);
+cudaError_t preload_fast();  // loads every compiled shape (before timing them)
 bool fast_qb_supported(bool mixed, int qb);
 cudaError_t launch_fast(bool mixed, bool dim3, bool occ, int qb, const PairArgs& a, const MixedArgs& m,
                         unsigned long long* task_ctr, unsigned long long* counters, int sm_count, cudaStream_t st);

@@ -1579,6 +1579,29 @@ bool fast_qb_supported(bool mixed, int qb) {
   return mixed ? (qb == 2 || qb == 3 || qb == 4 || qb == 5 || qb == 7 || qb == 8) : (qb >= 2 && qb <= 4);
 }
 
+// Loads every compiled quadrature-only kernel (module loading is lazy: a
+// kernel's first launch would otherwise also pay for it).
+cudaError_t preload_fast() {
+  cudaFuncAttributes fa;
+  cudaError_t e = cudaSuccess;
+  auto touch = [&](const void* fn) {
+    if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, fn);
+  };
+#define RVF_TOUCH_MIXED(Q)                        \
+  touch((const void*)k_fast_mixed<true, Q>);      \
+  touch((const void*)k_fast_mixed<false, Q>);
+#define RVF_TOUCH_FP64(Q)                             \
+  touch((const void*)k_fast_fp64<true, true, Q>);     \
+  touch((const void*)k_fast_fp64<true, false, Q>);    \
+  touch((const void*)k_fast_fp64<false, true, Q>);    \
+  touch((const void*)k_fast_fp64<false, false, Q>);
+  RVF_TOUCH_MIXED(2) RVF_TOUCH_MIXED(3) RVF_TOUCH_MIXED(4) RVF_TOUCH_MIXED(5) RVF_TOUCH_MIXED(7) RVF_TOUCH_MIXED(8)
+  RVF_TOUCH_FP64(2) RVF_TOUCH_FP64(3) RVF_TOUCH_FP64(4)
+#undef RVF_TOUCH_MIXED
+#undef RVF_TOUCH_FP64
+  return e;
+}
+
 cudaError_t launch_fast(bool mixed, bool dim3, bool occ, int qb, const PairArgs& a, const MixedArgs& m,
                         unsigned long long* task_ctr, unsigned long long* counters, int sm_count, cudaStream_t st) {
   auto launch = [&](auto fn, const auto& args) -> cudaError_t {

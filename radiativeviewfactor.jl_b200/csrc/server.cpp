@@ -147,10 +147,9 @@ struct rvf_server {
     bool done = false;
   };
   std::map<uint64_t, Tune> tune;
-  // shape sweep of the quadrature-only kernel per launch class and size
-  // class, one candidate per admission: ms per 1e9 point pairs
+  // shape sweep of the quadrature-only kernel per launch class, rule size
+  // and size class: ms per 1e9 point pairs of each candidate
   struct FastTune {
-    size_t next = 0;
     double score[4] = {0, 0, 0, 0};
     int qb = 0, groups = 1;
     bool done = false;
@@ -171,7 +170,7 @@ namespace {
 // and the oldest requests finish at short intervals (quadrature point pairs
 // of the mixed pipeline; Monte Carlo sample pairs, each of which evaluates
 // both elements' geometry).
-constexpr double kChunkPointPairs = 2e9;
+constexpr double kChunkPointPairs = 6e9;
 constexpr double kChunkSamplePairs = 1e8;
 
 const int kCand[][2] = {{0, 0}, {2, 0}, {0, 2}, {2, 2}};
@@ -263,44 +262,50 @@ int admit_one(rvf_server* sv, Req* r) {
   m->has_result = false;
   if (N == 1) cudaMemsetAsync(m->F.ptr, 0, sizeof(double), s->stream);
   if ((rc = wave_prepare(s, m, r->T, &r->opts, nullptr, r->w, nullptr))) return rc;
-  // the quadrature-only kernel's shape: the caller's, the tuned one, or the
-  // next candidate of this launch class and size class
+  // the quadrature-only kernel's shape: the caller's, the tuned one, or --
+  // on the first request of its launch class and size class -- the fastest
+  // candidate, every candidate run on this request (each forms the same F)
   const bool own = r->opts.fast_points != 0 || r->opts.fast_row_groups != 0;
-  const uint64_t fkey = fast_key(class_key(r), r->w.n_fast_tiles);
-  int cand = -1;
+  const uint64_t fkey = fast_key(class_key(r), r->w.n_fast_tiles) | ((uint64_t)r->w.pmax << 16);
+  bool sweep = false;
   if (!own && r->w.n_fast_tiles > 0) {
     std::lock_guard<std::mutex> lk2(sv->tune_mu);
-    rvf_server::FastTune& t = sv->ftune[fkey];
-    if (t.done) {
-      r->w.fast_qb = t.qb;
-      r->w.fast_groups = t.groups;
-    } else if (sv->o.autotune >= 0) {
-      cand = (int)t.next;
-      fast_cand(r->w.mixed, r->w.pmax, t.next, r->w.fast_qb, r->w.fast_groups);
+    const auto it = sv->ftune.find(fkey);
+    if (it != sv->ftune.end() && it->second.done) {
+      r->w.fast_qb = it->second.qb;
+      r->w.fast_groups = it->second.groups;
+    } else {
+      sweep = sv->o.autotune >= 0;
     }
   }
-  cudaEventRecord(s->ev[0], s->stream);
-  if ((rc = wave_fast(s, r->w, nullptr))) return rc;
-  cudaEventRecord(s->ev[1], s->stream);
-  const cudaError_t e = cudaStreamSynchronize(s->stream);
-  if (e != cudaSuccess) return cuda_err(e, "request set-up");
-  if (cand >= 0) {
+  if (!sweep) {
+    if ((rc = wave_fast(s, r->w, nullptr))) return rc;
+    const cudaError_t e = cudaStreamSynchronize(s->stream);
+    return e == cudaSuccess ? RVF_OK : cuda_err(e, "request set-up");
+  }
+  cudaError_t e = preload_fast();
+  if (e != cudaSuccess) return cuda_err(e, "kernel load");
+  rvf_server::FastTune t;
+  const double gpp = (double)r->w.n_fast_tiles * kTile * kTile * r->w.pmax * r->w.pmax * 1e-9;
+  for (int c = 0; c < kNFastCand; ++c) {
+    fast_cand(r->w.mixed, r->w.pmax, (size_t)c, r->w.fast_qb, r->w.fast_groups);
+    cudaEventRecord(s->ev[0], s->stream);
+    if ((rc = wave_fast(s, r->w, nullptr))) return rc;
+    cudaEventRecord(s->ev[1], s->stream);
+    if ((e = cudaStreamSynchronize(s->stream)) != cudaSuccess) return cuda_err(e, "request set-up");
     float ms = 0.f;
     cudaEventElapsedTime(&ms, s->ev[0], s->ev[1]);
-    const double gpp = (double)r->w.n_fast_tiles * kTile * kTile * r->w.pmax * r->w.pmax * 1e-9;
-    std::lock_guard<std::mutex> lk2(sv->tune_mu);
-    rvf_server::FastTune& t = sv->ftune[fkey];
-    if (!t.done && t.next == (size_t)cand) {
-      t.score[cand] = (double)ms / gpp;
-      if (++t.next >= (size_t)kNFastCand) {
-        size_t b = 0;
-        for (size_t c = 1; c < (size_t)kNFastCand; ++c)
-          if (t.score[c] < t.score[b]) b = c;
-        fast_cand(r->w.mixed, r->w.pmax, b, t.qb, t.groups);
-        t.done = true;
-        sv->ftune_done.push_back(fkey);
-      }
-    }
+    t.score[c] = (double)ms / gpp;
+  }
+  size_t b = 0;
+  for (size_t c = 1; c < (size_t)kNFastCand; ++c)
+    if (t.score[c] < t.score[b]) b = c;
+  fast_cand(r->w.mixed, r->w.pmax, b, t.qb, t.groups);
+  t.done = true;
+  std::lock_guard<std::mutex> lk2(sv->tune_mu);
+  if (!sv->ftune[fkey].done) {
+    sv->ftune[fkey] = t;
+    sv->ftune_done.push_back(fkey);
   }
   return RVF_OK;
 }
@@ -833,6 +838,7 @@ int rvf_server_stats_get(rvf_server* sv, rvf_server_stats* st) try {
     o.dim3 = (int32_t)((key >> 1) & 1);
     o.occlusion = (int32_t)((key >> 2) & 1);
     o.size_class = (int32_t)((key >> 8) & 15);
+    o.rule_points = (int32_t)(key >> 16);
     const auto g = sv->tune.find(key & 0xff);
     if (g != sv->tune.end() && g->second.done) {
       o.gen_blocks_per_sm = g->second.gen;
