@@ -562,6 +562,11 @@ def run_serve(rvf, sess, size: str, local: int):
         "check": "64 rows and columns of each checked served F against a plain FP64 one-at-a-time solve",
         "chunks": st["chunks"], "batched_requests": st["batched_requests"], "graph_replays": st["graph_replays"],
         "admit_bytes": admit, "admitted_bytes_peak": st["admitted_bytes_peak"],
+        "burst_worker_ms": {"admit": st_burst["ms_admit"], "quad_chunks": st_burst["ms_quad_chunks"],
+                            "mc_chunks": st_burst["ms_mc_chunks"]},
+        "one_at_a_time_ms": {"quad": 1e3 * sum(t for n, t in enumerate(t_alone) if not reqs[burst[n]]["mc"]),
+                             "mc": 1e3 * sum(t for n, t in enumerate(t_alone) if reqs[burst[n]]["mc"]),
+                             "solve_only": 1e3 * sum(t_solve_only)},
         "tuned_shapes": st["tuned"], "tuned_shapes_burst": st_burst["tuned"],
         "config": {"stream": f"{n_req} seeded requests (seed 5), Poisson arrivals, N log-uniform {n_lo}-{n_hi}, "
                              "plates / cube / cylinder, Tri3 / Quad4 / Quad8, nquad 2-5, 30% obstruction box, "

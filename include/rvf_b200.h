@@ -286,7 +286,10 @@ typedef struct {
   int64_t batched_requests;        /* sum over chunks of the requests in the chunk */
   uint64_t admitted_bytes_peak;
   int32_t n_tuned;                 /* entries of tuned[] in use */
-  int32_t reserved[7];
+  int32_t reserved;
+  double ms_admit;                 /* worker time: admissions (upload, tables, classes, quadrature-only tiles) */
+  double ms_quad_chunks;           /*   batched quadrature chunks (with the tail of the requests they finish) */
+  double ms_mc_chunks;             /*   Monte Carlo chunks */
   rvf_tuned_shape tuned[8];        /* the autotuner's choices (the first 8 classes it finished) */
 } rvf_server_stats;
 

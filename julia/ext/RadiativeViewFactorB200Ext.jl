@@ -162,7 +162,10 @@ struct RvfServerStats
     batched_requests::Int64
     admitted_bytes_peak::UInt64
     n_tuned::Int32
-    reserved::NTuple{7,Int32}
+    reserved::Int32
+    ms_admit::Float64
+    ms_quad_chunks::Float64
+    ms_mc_chunks::Float64
     tuned::NTuple{8,RvfTunedShape}
 end
 

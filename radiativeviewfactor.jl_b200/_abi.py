@@ -110,7 +110,8 @@ class ServerStats(C.Structure):
                 ("p99_ms", C.c_double), ("mean_ms", C.c_double), ("wall_ms", C.c_double),
                 ("pairs_done", C.c_int64), ("chunks", C.c_int64), ("graph_replays", C.c_int64),
                 ("batched_requests", C.c_int64), ("admitted_bytes_peak", C.c_uint64), ("n_tuned", C.c_int32),
-                ("reserved", C.c_int32 * 7), ("tuned", TunedShape * 8)]
+                ("reserved", C.c_int32), ("ms_admit", C.c_double), ("ms_quad_chunks", C.c_double),
+                ("ms_mc_chunks", C.c_double), ("tuned", TunedShape * 8)]
 
     def as_dict(self):
         d = {k: getattr(self, k) for k, _ in self._fields_ if k not in ("reserved", "tuned")}

@@ -394,6 +394,8 @@ struct McArgs {
   uint8_t* ray_log;  // [(i*N + j) * n_samples + k] for caller indices i < j
 };
 
+// Blocks of the Monte Carlo kernel resident at once (its persistent grid).
+int mc_resident_blocks(const McArgs& a, int sm_count);
 cudaError_t launch_mc(const McArgs& a, int sm_count, cudaStream_t st);
 cudaError_t launch_prep(const PrepArgs& a, cudaStream_t st);
 cudaError_t launch_prep_f32(const PrepF32Args& a, cudaStream_t st);

@@ -390,6 +390,15 @@ static cudaError_t launch_mc_t(const McArgs& a, int sm_count, cudaStream_t st) {
   return cudaGetLastError();
 }
 
+int mc_resident_blocks(const McArgs& a, int sm_count) {
+  const bool occ = a.n_nodes > 0;
+  int per_sm = 1;
+  const void* fn = a.dim3 ? (occ ? (const void*)k_pairs_mc<true, true> : (const void*)k_pairs_mc<true, false>)
+                          : (occ ? (const void*)k_pairs_mc<false, true> : (const void*)k_pairs_mc<false, false>);
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 256, 0) != cudaSuccess || per_sm < 1) per_sm = 1;
+  return sm_count * per_sm;
+}
+
 cudaError_t launch_mc(const McArgs& a, int sm_count, cudaStream_t st) {
   if (a.N == 0) return cudaSuccess;
   if (a.area_pass) {

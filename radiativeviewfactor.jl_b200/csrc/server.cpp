@@ -137,6 +137,7 @@ struct rvf_server {
   // statistics
   int64_t submitted = 0, completed = 0, failed = 0, canceled = 0;
   int64_t chunks = 0, graph_replays = 0, batched = 0, pairs_done = 0;
+  double ms_admit = 0, ms_quad = 0, ms_mc = 0;  // worker time by activity
   std::vector<double> latencies;
   double first_submit = -1, last_done = 0;
   // grid-size sweep per launch class: candidate (gen, trace) blocks per SM
@@ -171,7 +172,7 @@ namespace {
 // of the mixed pipeline; Monte Carlo sample pairs, each of which evaluates
 // both elements' geometry).
 constexpr double kChunkPointPairs = 6e9;
-constexpr double kChunkSamplePairs = 1e8;
+constexpr double kChunkSamplePairs = 3e8;
 
 const int kCand[][2] = {{0, 0}, {2, 0}, {0, 2}, {2, 2}};
 constexpr int kNCand = 4;
@@ -463,8 +464,10 @@ void run_mc_chunk(rvf_server* sv, Req* r) {
     cudaSetDevice(s->device);
     McArgs c{};
     fill_mc_args(s, r->m, &r->opts, nullptr, c);
+    // a whole number of waves of the persistent grid: no partial last wave
     const double per = (double)kTile * kTile * std::max(1, r->opts.n_samples);
-    const int64_t budget = std::max<int64_t>(1, (int64_t)(kChunkSamplePairs / per));
+    const int64_t grid = mc_resident_blocks(c, s->sm_count);
+    const int64_t budget = grid * std::max<int64_t>(1, (int64_t)(kChunkSamplePairs / per) / grid);
     c.tile0 = r->mc_claimed;
     c.tile_count = std::min<int64_t>(r->mc_tiles - r->mc_claimed, budget);
     c.area_pass = !r->mc_area_done;
@@ -565,8 +568,10 @@ void worker_loop(rvf_server* sv) {
       }
     }
     for (Req* r : admit) {
+      const auto a0 = Clock::now();
       const int rc = admit_one(sv, r);
       std::lock_guard<std::mutex> lk(sv->mu);
+      sv->ms_admit += std::chrono::duration<double, std::milli>(Clock::now() - a0).count();
       if (rc) {
         finish(sv, r, RVF_REQ_FAILED, rc);
         drop_device(sv, r);
@@ -605,8 +610,12 @@ void worker_loop(rvf_server* sv) {
             batch.push_back(r);
       }
     }
+    const auto c0 = Clock::now();
     if (mc) run_mc_chunk(sv, mc);
     else if (!batch.empty()) run_chunk(sv, batch);
+    const double ms = std::chrono::duration<double, std::milli>(Clock::now() - c0).count();
+    std::lock_guard<std::mutex> lk(sv->mu);
+    (mc ? sv->ms_mc : sv->ms_quad) += ms;
   }
 }
 
@@ -829,6 +838,9 @@ int rvf_server_stats_get(rvf_server* sv, rvf_server_stats* st) try {
   st->graph_replays = sv->graph_replays;
   st->batched_requests = sv->batched;
   st->admitted_bytes_peak = sv->admitted_peak;
+  st->ms_admit = sv->ms_admit;
+  st->ms_quad_chunks = sv->ms_quad;
+  st->ms_mc_chunks = sv->ms_mc;
   std::lock_guard<std::mutex> lk2(sv->tune_mu);
   for (uint64_t key : sv->ftune_done) {
     if (st->n_tuned >= 8) break;
