@@ -290,7 +290,8 @@ typedef struct {
   double ms_admit;                 /* worker time: admissions (upload, tables, classes, quadrature-only tiles) */
   double ms_quad_chunks;           /*   batched quadrature chunks (with the tail of the requests they finish) */
   double ms_mc_chunks;             /*   Monte Carlo chunks */
-  rvf_tuned_shape tuned[8];        /* the autotuner's choices (the first 8 classes it finished) */
+  rvf_tuned_shape tuned[8];        /* the autotuner's choices, kept by the session for all its servers (the
+                                      last 8 classes it finished) */
 } rvf_server_stats;
 
 int rvf_server_create(rvf_session* s, const rvf_server_opts* o, rvf_server** out);

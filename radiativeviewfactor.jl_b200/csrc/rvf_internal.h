@@ -57,6 +57,24 @@ struct Tables {
   DevBuf twork;        // the tiles the chunked pipeline integrates (tile indices, row-major)
 };
 
+// Autotuner choices of the request server (server.cpp), kept by the session
+// so that every server on it reuses them.  Chunk grids per launch class:
+// candidate (generation, traversal) blocks per SM, ms per million point
+// pairs of the claimed tiles.
+struct GridTune {
+  size_t next = 0;
+  std::vector<double> score;
+  int gen = 0, trace = 0;
+  bool done = false;
+};
+// The quadrature-only kernel's shape per launch class, rule size and size
+// class: ms per 1e9 point pairs of each candidate.
+struct FastTune {
+  double score[4] = {0, 0, 0, 0};
+  int qb = 0, groups = 1;
+  bool done = false;
+};
+
 }  // namespace rvf
 
 struct rvf_session {
@@ -68,6 +86,12 @@ struct rvf_session {
   int sm_count = 0;
   size_t smem_optin = 0;
   std::mutex mu;
+  // autotuner state: a lock of its own, always taken last (admission holds
+  // mu while it reads it, rvf_server_stats_get holds the server's lock)
+  std::mutex tune_mu;
+  std::map<uint64_t, rvf::GridTune> grid_tune;
+  std::map<uint64_t, rvf::FastTune> ftune;
+  std::vector<uint64_t> ftune_done;  // keys in the order their sweeps ended
   rvf::DevBuf err;           // int
   rvf::DevBuf tile_counter;  // u64
   rvf::DevBuf counters;      // u64 x 8

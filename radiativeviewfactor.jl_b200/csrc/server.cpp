@@ -140,28 +140,6 @@ struct rvf_server {
   double ms_admit = 0, ms_quad = 0, ms_mc = 0;  // worker time by activity
   std::vector<double> latencies;
   double first_submit = -1, last_done = 0;
-  // grid-size sweep per launch class: candidate (gen, trace) blocks per SM
-  struct Tune {
-    size_t next = 0;
-    std::vector<double> score;  // ms per million point pairs of claimed tiles
-    int gen = 0, trace = 0;
-    bool done = false;
-  };
-  std::map<uint64_t, Tune> tune;
-  // shape sweep of the quadrature-only kernel per launch class, rule size
-  // and size class: ms per 1e9 point pairs of each candidate
-  struct FastTune {
-    double score[4] = {0, 0, 0, 0};
-    int qb = 0, groups = 1;
-    bool done = false;
-  };
-  // ftune and ftune_done have a lock of their own, taken last: admission
-  // holds the session lock, and rvf_release takes the session lock inside
-  // the server lock
-  std::mutex tune_mu;
-  std::map<uint64_t, FastTune> ftune;
-  std::vector<uint64_t> ftune_done;  // keys in the order their sweeps ended
-
   double now_ms() const { return std::chrono::duration<double, std::milli>(Clock::now() - t0).count(); }
 };
 
@@ -172,7 +150,7 @@ namespace {
 // of the mixed pipeline; Monte Carlo sample pairs, each of which evaluates
 // both elements' geometry).
 constexpr double kChunkPointPairs = 6e9;
-constexpr double kChunkSamplePairs = 3e8;
+constexpr double kChunkSamplePairs = 2e9;
 
 const int kCand[][2] = {{0, 0}, {2, 0}, {0, 2}, {2, 2}};
 constexpr int kNCand = 4;
@@ -270,9 +248,9 @@ int admit_one(rvf_server* sv, Req* r) {
   const uint64_t fkey = fast_key(class_key(r), r->w.n_fast_tiles) | ((uint64_t)r->w.pmax << 16);
   bool sweep = false;
   if (!own && r->w.n_fast_tiles > 0) {
-    std::lock_guard<std::mutex> lk2(sv->tune_mu);
-    const auto it = sv->ftune.find(fkey);
-    if (it != sv->ftune.end() && it->second.done) {
+    std::lock_guard<std::mutex> lk2(s->tune_mu);
+    const auto it = s->ftune.find(fkey);
+    if (it != s->ftune.end() && it->second.done) {
       r->w.fast_qb = it->second.qb;
       r->w.fast_groups = it->second.groups;
     } else {
@@ -286,7 +264,7 @@ int admit_one(rvf_server* sv, Req* r) {
   }
   cudaError_t e = preload_fast();
   if (e != cudaSuccess) return cuda_err(e, "kernel load");
-  rvf_server::FastTune t;
+  FastTune t;
   const double gpp = (double)r->w.n_fast_tiles * kTile * kTile * r->w.pmax * r->w.pmax * 1e-9;
   for (int c = 0; c < kNFastCand; ++c) {
     fast_cand(r->w.mixed, r->w.pmax, (size_t)c, r->w.fast_qb, r->w.fast_groups);
@@ -303,10 +281,10 @@ int admit_one(rvf_server* sv, Req* r) {
     if (t.score[c] < t.score[b]) b = c;
   fast_cand(r->w.mixed, r->w.pmax, b, t.qb, t.groups);
   t.done = true;
-  std::lock_guard<std::mutex> lk2(sv->tune_mu);
-  if (!sv->ftune[fkey].done) {
-    sv->ftune[fkey] = t;
-    sv->ftune_done.push_back(fkey);
+  std::lock_guard<std::mutex> lk2(s->tune_mu);
+  if (!s->ftune[fkey].done) {
+    s->ftune[fkey] = t;
+    s->ftune_done.push_back(fkey);
   }
   return RVF_OK;
 }
@@ -359,8 +337,8 @@ void run_chunk(rvf_server* sv, std::vector<Req*>& batch) {
   size_t cand = 0;
   bool tuning = false;
   {
-    std::lock_guard<std::mutex> lk(sv->mu);
-    rvf_server::Tune& t = sv->tune[key];
+    std::lock_guard<std::mutex> lk(s->tune_mu);
+    GridTune& t = s->grid_tune[key];
     if (sv->o.autotune >= 0 && !t.done && batch[0]->w.occ) {
       tuning = true;
       cand = t.next;
@@ -422,7 +400,8 @@ void run_chunk(rvf_server* sv, std::vector<Req*>& batch) {
                        sv->active.end());
     }
     if (tuning && !rc && pp > 0) {
-      rvf_server::Tune& t = sv->tune[key];
+      std::lock_guard<std::mutex> lk2(s->tune_mu);
+      GridTune& t = s->grid_tune[key];
       t.score.resize(kNCand, 0.0);
       t.score[cand] = ms / ((double)pp * kTile * kTile * pm * pm * 1e-6);
       if (++t.next >= (size_t)kNCand) {
@@ -841,18 +820,20 @@ int rvf_server_stats_get(rvf_server* sv, rvf_server_stats* st) try {
   st->ms_admit = sv->ms_admit;
   st->ms_quad_chunks = sv->ms_quad;
   st->ms_mc_chunks = sv->ms_mc;
-  std::lock_guard<std::mutex> lk2(sv->tune_mu);
-  for (uint64_t key : sv->ftune_done) {
-    if (st->n_tuned >= 8) break;
-    const rvf_server::FastTune& f = sv->ftune[key];
+  Session* s = sv->s;
+  std::lock_guard<std::mutex> lk2(s->tune_mu);
+  const size_t first = s->ftune_done.size() > 8 ? s->ftune_done.size() - 8 : 0;
+  for (size_t n = first; n < s->ftune_done.size(); ++n) {
+    const uint64_t key = s->ftune_done[n];
+    const FastTune& f = s->ftune[key];
     rvf_tuned_shape& o = st->tuned[st->n_tuned++];
     o.mixed = (int32_t)(key & 1);
     o.dim3 = (int32_t)((key >> 1) & 1);
     o.occlusion = (int32_t)((key >> 2) & 1);
     o.size_class = (int32_t)((key >> 8) & 15);
     o.rule_points = (int32_t)(key >> 16);
-    const auto g = sv->tune.find(key & 0xff);
-    if (g != sv->tune.end() && g->second.done) {
+    const auto g = s->grid_tune.find(key & 0xff);
+    if (g != s->grid_tune.end() && g->second.done) {
       o.gen_blocks_per_sm = g->second.gen;
       o.trace_blocks_per_sm = g->second.trace;
     }

@@ -146,7 +146,8 @@ def test_autotuned_shapes_reported_and_identical(rvf, session):
         md = m.cube_enclosure(10, family="tri3", box_m=3)
         mix += [(md, [7], mk(3, seed=0, precision=prec))] * 6
     expect = {prec: solo(rvf, session, mix[k][0], [7], mix[k][2]) for k, prec in ((0, "fp64"), (6, "mixed"))}
-    sv = _abi.Server(session, max_batch=1)
+    own = rvf.Session(0)  # a session of its own: no choices of earlier tests
+    sv = _abi.Server(own, max_batch=1)
     try:
         ids = [sv.submit(rvf.mesh_desc_arrays(md, obs), o) for md, obs, o in mix]
         for k, rid in enumerate(ids):
@@ -157,11 +158,14 @@ def test_autotuned_shapes_reported_and_identical(rvf, session):
             sv.release(rid)
         st = sv.stats()
         assert st["completed"] == len(mix)
+        # this class in both precisions
         tuned = st["tuned"]
-        assert sorted(t["mixed"] for t in tuned) == [0, 1], tuned
+        assert sorted(t["mixed"] for t in tuned) == [0, 1], st["tuned"]
         for t in tuned:
-            assert t["occlusion"] == 1 and t["dim3"] == 1
+            assert t["occlusion"] == 1 and t["dim3"] == 1 and t["rule_points"] == 7
             assert t["fast_points"] >= 2 and t["fast_row_groups"] in (1, 2, 4)
             assert 0 < t["fast_ms_per_gpp"] <= t["fast_ms_per_gpp_default"]
+        assert len(st["tuned"]) == 2
     finally:
         sv.close()
+        own.close()
