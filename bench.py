@@ -53,8 +53,8 @@ REF_COUNTS = {
 # (dram__bytes_read.sum + dram__bytes_write.sum of k_trace32 / k_trace64 and
 # k_plist in one ncu capture of the medium workload divided by the rays it
 # traced; the capture is summarized under profiles/).
-TRAFFIC_PER_TRACED_RAY = {"mixed": (1.550799e9 + 0.032135e9 + 0.077273e9 + 0.239007e9) / 137006664,
-                          "fp64": (1.552282e9 + 0.029719e9 + 0.077296e9 + 0.238736e9) / 137012826}
+TRAFFIC_PER_TRACED_RAY = {"mixed": (0.987216e9 + 0.019866e9 + 0.039880e9 + 0.225654e9) / 75262173,
+                          "fp64": (0.990203e9 + 0.017742e9 + 0.039880e9 + 0.225654e9) / 75267549}
 
 
 def load_pkg():
@@ -466,10 +466,14 @@ def run_serve(rvf, sess, size: str, local: int):
     for rep in range(2):
         sv = _abi.Server(sess, admit_bytes=admit)
         t0 = time.perf_counter()
-        rids = [sv.submit(arrays[k], reqs[k]["opts"]) for k in burst]
-        for rid in rids:
-            sv.wait(rid, 3_600_000)
-            sv.release(rid)
+        rids = {sv.submit(arrays[k], reqs[k]["opts"]) for k in burst}
+        while rids:  # release in completion order
+            done = [rid for rid in rids if sv.poll(rid)[0] not in ("queued", "running")]
+            for rid in done:
+                sv.release(rid)
+                rids.discard(rid)
+            if not done:
+                time.sleep(0.0005)
         t_burst = time.perf_counter() - t0
         st_burst = sv.stats()
         sv.close()
@@ -522,23 +526,43 @@ def run_serve(rvf, sess, size: str, local: int):
     t_start = time.perf_counter()
     th.start()
     # The client reads each checked result on the device and releases every
-    # request as soon as it is done: a finished request keeps its device
-    # memory and its admission charge until rvf_release.
-    for _ in range(n_req):
-        k, rid = submitted.get()
-        try:
-            sv.wait(rid, 3_600_000)
-            if k in ref_rows:
-                idx, rr, cc = ref_rows.pop(k)
-                rows, cols = device_rows_cols(sv.result_device(rid), reqs[k]["N"], idx, local)
-                dF = max(dF, float(np.nanmax(np.abs(rows - rr))), float(np.nanmax(np.abs(cols - cc))))
-                n_checked += 1
-        except _abi.RVFError as e:
-            err.append(str(e))
-        try:
-            sv.release(rid)
-        except _abi.RVFError:
-            pass
+    # request as soon as it is done, in the order they complete: a finished
+    # request keeps its device memory and its admission charge until
+    # rvf_release, so releasing in submission order would hold finished
+    # results behind a long request and stall admission.
+    pending = {}
+    finished = 0
+    while finished < n_req:
+        while True:
+            try:
+                k, rid = submitted.get_nowait()
+                pending[rid] = k
+            except queue.Empty:
+                break
+        progressed = False
+        for rid in list(pending):
+            state, status, _ = sv.poll(rid)
+            if state in ("queued", "running"):
+                continue
+            k = pending.pop(rid)
+            finished += 1
+            progressed = True
+            try:
+                if status != 0:
+                    raise _abi.RVFError(status, f"request {k}: {state}")
+                if k in ref_rows:
+                    idx, rr, cc = ref_rows.pop(k)
+                    rows, cols = device_rows_cols(sv.result_device(rid), reqs[k]["N"], idx, local)
+                    dF = max(dF, float(np.nanmax(np.abs(rows - rr))), float(np.nanmax(np.abs(cols - cc))))
+                    n_checked += 1
+            except _abi.RVFError as e:
+                err.append(str(e))
+            try:
+                sv.release(rid)
+            except _abi.RVFError:
+                pass
+        if not progressed:
+            time.sleep(0.0005)
     wall = time.perf_counter() - t_start
     th.join()
     st = sv.stats()
@@ -737,17 +761,28 @@ def run_ours(args):
             for k in range(args.e2e_warmup + args.e2e_steps):
                 barrier(ws)
                 t0 = time.perf_counter()
-                d = _abi.DeviceMesh(sess, rvf.mesh_desc_arrays(md, W.obs))
-                d.solve(opts, F, A, Fg, Ag)
+                desc = rvf.mesh_desc_arrays(md, W.obs)
+                ta = time.perf_counter()
+                d = _abi.DeviceMesh(sess, desc)
+                tb = time.perf_counter()
+                st = d.solve(opts, F, A, Fg, Ag).as_dict()
+                tc = time.perf_counter()
                 d.release()
                 t1 = time.perf_counter()
                 if k >= args.e2e_warmup:
                     times.append(t1 - t0)
+                    # where the last step's time went (host clock, and the
+                    # solve's own event-timed phases)
+                    brk = {"flatten_ms": 1e3 * (ta - t0), "upload_ms": 1e3 * (tb - ta),
+                           "solve_ms": 1e3 * (tc - tb), "release_ms": 1e3 * (t1 - tc),
+                           "solve_phases_ms": {key: round(st[key], 2) for key in
+                                               ("ms_prep", "ms_cull", "ms_pairs", "ms_reduce", "ms_download",
+                                                "ms_total")}}
             t = allreduce_max(sum(times), ws)
             e2e_all[prec] = {"value": job_rate(pairs * len(times), t, ws), "unit": UNIT,
                              "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                              "host_buffer": "pinned" if pinned else "pageable", "steps": len(times),
-                             "s_per_step": t / len(times), "precision": prec}
+                             "s_per_step": t / len(times), "precision": prec, "last_step": brk}
         if pinned:
             Fh.free()
     e2e = e2e_all.get(head)

@@ -396,6 +396,11 @@ namespace {
 // copy stream while the next chunk computes (contiguous caller columns in
 // one copy).  A pageable destination makes the copies synchronous: still
 // correct, without the overlap.
+#ifndef RVF_DL_CHUNKS
+#define RVF_DL_CHUNKS 8
+#endif
+constexpr int kDownloadChunks = RVF_DL_CHUNKS;
+
 struct ColumnDownload {
   Session* s = nullptr;
   const rvf_mesh* m = nullptr;
@@ -548,11 +553,18 @@ int rvf_solve(rvf_session* s, rvf_mesh* m, const rvf_options* o, double* F_elem,
     const std::function<void()> queue_columns = [&]() {
       if (dl.host && dl_err == cudaSuccess) dl_err = dl.advance(dl_upto);
     };
+    // With a host F the pipeline runs in at least kDownloadChunks chunks, so
+    // that the columns of finished tile rows go down while later chunks
+    // compute (the last chunk's rows hold about 1/sqrt(chunks) of the
+    // columns); without, one chunk as far as the ray queues allow.
+    double pp_budget = 0.0;
+    if (dl.host && w.n_tiles > 0)
+      pp_budget = std::max(1e9, (double)w.n_tiles * kTile * kTile * w.pmax * w.pmax / kDownloadChunks);
     while (!w.done()) {  // chunks: each claims tiles while the ray queues have room
       ChunkInfo ci;
       const int64_t before = w.claimed;
       dl_upto = before;
-      if ((rc = wave_chunk(s, &one, 1, false, &ci, 0, 0, 0.0, &queue_columns))) return rc;
+      if ((rc = wave_chunk(s, &one, 1, false, &ci, 0, 0, pp_budget, &queue_columns))) return rc;
       if (dl_err != cudaSuccess) return cuda_err(dl_err, "F column download");
       if ((rc = read_err(s))) return rc;
       n_kernels += ci.kernels;
