@@ -761,9 +761,9 @@ def run_ours(args):
             for k in range(args.e2e_warmup + args.e2e_steps):
                 barrier(ws)
                 t0 = time.perf_counter()
-                desc = rvf.mesh_desc_arrays(md, W.obs)
+                mesh_arrays = rvf.mesh_desc_arrays(md, W.obs)
                 ta = time.perf_counter()
-                d = _abi.DeviceMesh(sess, desc)
+                d = _abi.DeviceMesh(sess, mesh_arrays)
                 tb = time.perf_counter()
                 st = d.solve(opts, F, A, Fg, Ag).as_dict()
                 tc = time.perf_counter()

@@ -138,6 +138,7 @@ struct rvf_server {
   int64_t submitted = 0, completed = 0, failed = 0, canceled = 0;
   int64_t chunks = 0, graph_replays = 0, batched = 0, pairs_done = 0;
   double ms_admit = 0, ms_quad = 0, ms_mc = 0;  // worker time by activity
+  double share_mc = 0, share_quad = 0;           // the same while both kinds wait (time sharing)
   std::vector<double> latencies;
   double first_submit = -1, last_done = 0;
   double now_ms() const { return std::chrono::duration<double, std::milli>(Clock::now() - t0).count(); }
@@ -567,19 +568,27 @@ void worker_loop(rvf_server* sv) {
         sv->active.push_back(r);
       }
     }
-    // next piece of work: a chunk of the oldest admitted request -- Monte
-    // Carlo alone, quadrature together with every request of its class
+    // next piece of work: a chunk of the oldest admitted Monte Carlo
+    // request (alone), or of the oldest quadrature request together with
+    // every request of its class.  While both kinds wait, each gets half of
+    // the worker's time, so short quadrature requests do not queue behind a
+    // long Monte Carlo one (a 40,000-element request takes ~20 s).
     Req* mc = nullptr;
     std::vector<Req*> batch;
     {
       std::lock_guard<std::mutex> lk(sv->mu);
       const int maxb = (sv->o.max_batch >= 1 && sv->o.max_batch <= kMaxBatch) ? sv->o.max_batch : kMaxBatch;
+      Req* head_q = nullptr;
+      Req* head_mc = nullptr;
+      for (Req* r : sv->active) {
+        if (r->cancel) continue;
+        if (r->quad && !r->w.done() && !head_q) head_q = r;
+        if (!r->quad && !head_mc) head_mc = r;
+      }
+      if (!head_q || !head_mc) sv->share_mc = sv->share_quad = 0.0;  // no contention: no debt either way
       const Req* head = nullptr;
-      for (Req* r : sv->active)
-        if (!r->cancel && (!r->quad || !r->w.done())) {
-          head = r;
-          break;
-        }
+      if (head_mc && (!head_q || sv->share_mc <= sv->share_quad)) head = head_mc;
+      else head = head_q;
       if (head && !head->quad) {
         mc = const_cast<Req*>(head);
       } else if (head) {
@@ -595,6 +604,7 @@ void worker_loop(rvf_server* sv) {
     const double ms = std::chrono::duration<double, std::milli>(Clock::now() - c0).count();
     std::lock_guard<std::mutex> lk(sv->mu);
     (mc ? sv->ms_mc : sv->ms_quad) += ms;
+    (mc ? sv->share_mc : sv->share_quad) += ms;
   }
 }
 
