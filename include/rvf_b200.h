@@ -117,7 +117,8 @@ typedef struct {
   int32_t fault_inject;       /* test hooks, 0 in production: RVF_FAULT_* bits */
   int32_t fast_points;        /* quadrature-only tiles: destination points per lane block -- 0 = by the
                                  rule's size; FP64 2..4, mixed 2, 3, 4, 5, 7 or 8 (same view factors) */
-  int32_t fast_row_groups;    /* quadrature-only tiles: warp tasks per tile, 0/1 (whole tile), 2 or 4 */
+  int32_t fast_row_groups;    /* quadrature-only tiles: warp tasks per tile, 1 (whole tile), 2, 4, 8 or 32
+                                 (one row each); 0 = enough tasks for four per resident warp */
   int32_t reserved[2];
 } rvf_options;
 

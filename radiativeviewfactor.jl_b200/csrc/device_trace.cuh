@@ -47,13 +47,8 @@ struct RayBankT {
   };
   int32_t gi[32], gj[32];
   const void* prims[32];         // each ray's primitive array (rays of one warp may come from different meshes)
-  union {
-    struct {
-      int32_t first[L][32];      // collected leaves: first primitive
-      uint16_t item[32 * L * 8];  // leaf phase: (lane, leaf slot, offset) per test
-    } walk;
-    int4 stage[(L * 32 * 4 + 32 * L * 8 * 2) / 16];  // the same bytes: pair-list staging (trace_list_staged)
-  };
+  int32_t first[L][32];          // collected leaves: first primitive
+  uint16_t item[32 * L * 8];     // leaf phase: (lane, leaf slot, offset) per test
   uint8_t hit[32];
   uint8_t unsure[32];
 };
@@ -197,7 +192,7 @@ __device__ __forceinline__ int trace_batch(bool have, const Src& nodes, int n_no
         ++cnt.unsure_slab;
         done = true;
       } else if (s == kHit && count > 0) {
-        ws.walk.first[nl][lane] = first;
+        ws.first[nl][lane] = first;
         counts |= (uint32_t)count << (4 * nl);
         total_own += count;
         ++nl;
@@ -223,15 +218,15 @@ __device__ __forceinline__ int trace_batch(bool have, const Src& nodes, int n_no
     int pos = incl - total_own;
     for (int sl = 0; sl < nl; ++sl) {
       const int c = (int)((counts >> (4 * sl)) & 15u);
-      for (int u = 0; u < c; ++u) ws.walk.item[pos++] = (uint16_t)((lane << 6) | (sl << 3) | u);
+      for (int u = 0; u < c; ++u) ws.item[pos++] = (uint16_t)((lane << 6) | (sl << 3) | u);
     }
     __syncwarp();
     for (int base = 0; base < total; base += 32) {
       const int t = base + lane;
       if (t < total) {
-        const int it = ws.walk.item[t];
+        const int it = ws.item[t];
         const int o = it >> 6;
-        const int r = pol.prim(ws, o, ws.walk.first[(it >> 3) & 7][o] + (it & 7), cnt);
+        const int r = pol.prim(ws, o, ws.first[(it >> 3) & 7][o] + (it & 7), cnt);
         if (r == kHit) ws.hit[o] = 1;
         else if (r == kUnsure) ws.unsure[o] = 1;
       }

@@ -1165,72 +1165,6 @@ __device__ __forceinline__ int trace_list(const int32_t* e, int n, const Src& no
   return unsure ? kUnsure : kMiss;
 }
 
-// trace_list for a whole warp (warp-uniform call): lanes whose rays share a
-// list (one pending pair: the rays of a run) gather B of its entries at a
-// time into the warp's shared-memory stage -- entry k's triangle and leaf
-// box by lane k, all loads in flight together -- and then run trace_list's
-// exact test sequence over the staged entries, so a list costs one round of
-// dependent loads per B entries instead of one per entry.  The staged box
-// carries its leaf's index in its miss field (trace_list's leaf-change test).
-// lst: the lane has a list (ln >= 0) of ln entries at e, for pending slot
-// `slot`; other lanes return kMiss.
-template <int B, typename Node, typename Src, typename Pol, typename Tri>
-__device__ __forceinline__ int trace_list_staged(bool lst, int64_t slot, const int32_t* e, int ln, const Src& nodes,
-                                                 const Tri* tris, const int32_t* leaf_of, const Pol& pol,
-                                                 int4* stage, int lane, TravCount& cnt) {
-  static_assert(B <= 32, "one entry per lane");
-  Tri* s_tri = reinterpret_cast<Tri*>(stage);
-  Node* s_node = reinterpret_cast<Node*>(s_tri + B);
-  int last = -1, s = kMiss;
-  bool unsure = false, hit = false;
-  const bool any = lst && ln > 0;
-  uint32_t todo = __ballot_sync(kFull, any);
-  while (todo) {
-    const int leader = __ffs(todo) - 1;
-    const long long ls = __shfl_sync(kFull, (long long)slot, leader);
-    const int n = __shfl_sync(kFull, ln, leader);
-    const int32_t* le = reinterpret_cast<const int32_t*>(
-        __shfl_sync(kFull, (unsigned long long)reinterpret_cast<uintptr_t>(e), leader));
-    const bool mine = any && (long long)slot == ls;
-    todo &= ~__ballot_sync(kFull, mine);
-    for (int b = 0; b < n; b += B) {
-      if (lane < B && b + lane < n) {
-        const int u = le[b + lane];
-        const int lf = leaf_of[u];
-        Node nd = nodes(lf);
-        nd.miss = lf;
-        s_node[lane] = nd;
-        s_tri[lane] = tris[u];
-      }
-      __syncwarp();
-      if (mine && !hit) {
-        const int m = min(B, n - b);
-        for (int q = 0; q < m; ++q) {
-          const Node nd = s_node[q];
-          if (nd.miss != last) {
-            last = nd.miss;
-            s = pol.node(nd);
-            ++cnt.nodes;
-            if (s == kUnsure) ++cnt.unsure_slab;
-          }
-          if (s != kMiss) {
-            ++cnt.prims;
-            const int mm = pol.prim_direct(s_tri[q]);
-            if (mm == kUnsure) ++cnt.unsure_prim;
-            if (mm == kHit && s == kHit) {
-              hit = true;
-              break;
-            }
-            if (mm != kMiss) unsure = true;
-          }
-        }
-      }
-      __syncwarp();
-    }
-  }
-  return hit ? kHit : (any && unsure) ? kUnsure : kMiss;
-}
-
 // Sets the (p, q) visibility bits of the warp's visible rays.  The rays of one
 // pair sit in consecutive lanes, so the bits of each run of lanes with the
 // same (slot, word) are OR-combined by a segmented scan and the last lane of
@@ -1323,12 +1257,11 @@ __global__ void __launch_bounds__(256, 3) k_trace64(const TraceBatch* __restrict
         if (pol.R.zdir || !(isfinite(pol.R.inv[0]) && isfinite(pol.R.inv[1]) && isfinite(pol.R.inv[2]))) ln = -1;
       }
       const bool walk = have && ln < 0;
-      static_assert(sizeof(ws.stage) >= 16 * (sizeof(TriD) + sizeof(NodeD)), "list stage");
-      res = in_smem ? trace_list_staged<16, NodeD>(have && ln >= 0, x.slot, le, ln,
-                                                   SwizNodes<NodeD>{reinterpret_cast<const int4*>(snodes)}, a.tris,
-                                                   a.leaf_of, pol, ws.stage, lane, tc)
-                    : trace_list_staged<16, NodeD>(have && ln >= 0, x.slot, le, ln, GlobalNodes<NodeD>{a.nodes},
-                                                   a.tris, a.leaf_of, pol, ws.stage, lane, tc);
+      res = kMiss;
+      if (have && ln >= 0)
+        res = in_smem ? trace_list(le, ln, SwizNodes<NodeD>{reinterpret_cast<const int4*>(snodes)}, a.tris, a.leaf_of,
+                                   pol, tc)
+                      : trace_list(le, ln, GlobalNodes<NodeD>{a.nodes}, a.tris, a.leaf_of, pol, tc);
       if (__any_sync(kFull, walk)) {
         const int rw =
             in_smem ? trace_batch(walk, SwizNodes<NodeD>{reinterpret_cast<const int4*>(snodes)}, n_nodes, ws, pol, tc)
@@ -1412,15 +1345,11 @@ __global__ void __launch_bounds__(256, 4) k_trace32(const TraceBatch* __restrict
       le = Q.pool + pl.off;
     }
     const bool walk = have && ln < 0;
-    // the rays of one warp come from one or two pairs: their lists are staged
-    static_assert(sizeof(ws.stage) >= 32 * (sizeof(TriF) + sizeof(NodeF)), "list stage");
-    const int res_l =
-        in_smem ? trace_list_staged<32, NodeF>(have && ln >= 0, x.slot, le, ln,
-                                        SwizNodes<NodeF>{reinterpret_cast<const int4*>(snodes)}, a.trisf, a.leaf_of, pol,
-                                        ws.stage, lane, tc)
-                : trace_list_staged<32, NodeF>(have && ln >= 0, x.slot, le, ln, GlobalNodes<NodeF>{a.nodesf}, a.trisf,
-                                        a.leaf_of, pol, ws.stage, lane, tc);
-    int res = res_l;
+    int res = kMiss;
+    if (have && ln >= 0)
+      res = in_smem ? trace_list(le, ln, SwizNodes<NodeF>{reinterpret_cast<const int4*>(snodes)}, a.trisf, a.leaf_of,
+                                 pol, tc)
+                    : trace_list(le, ln, GlobalNodes<NodeF>{a.nodesf}, a.trisf, a.leaf_of, pol, tc);
     if (__any_sync(kFull, walk)) {
       const int rw =
           in_smem ? trace_batch(walk, SwizNodes<NodeF>{reinterpret_cast<const int4*>(snodes)}, n_nodes, ws, pol, tc)
@@ -1575,9 +1504,10 @@ __global__ void __launch_bounds__(256) k_resolve_mixed(const ResolveBatch* __res
 #endif
 
 // A task is one row group of a tile: groups = 1 (the whole tile: row
-// classes li0 = 0..7, each the rows li0, li0 + 8, ...), 2 or 4 (half or a
-// quarter of the row classes), so small meshes spread over more warps.  The
-// shape changes no sum: every pair is formed by the same loop.
+// classes li0 = 0..7, each the rows li0, li0 + 8, ...), 2, 4 or 8 (half, a
+// quarter or one of the row classes), or 32 (one row: li0 = 8 + row), so
+// small meshes spread over more warps.  The shape changes no sum: every pair
+// is formed by the same loop.
 __device__ __forceinline__ bool fast_task(unsigned long long* task_ctr, int64_t n_tiles, int groups,
                                           const uint8_t* tcls, uint8_t skip, int lane, int64_t& t, int& r0,
                                           int& r1) {
@@ -1588,10 +1518,15 @@ __device__ __forceinline__ bool fast_task(unsigned long long* task_ctr, int64_t 
     const unsigned long long tile = k / (unsigned)groups;
     if (tile >= (unsigned long long)n_tiles) return false;
     if (tcls[tile] & skip) continue;
-    const int g = (int)(k - tile * (unsigned)groups), per = 8 / groups;
+    const int g = (int)(k - tile * (unsigned)groups);
     t = (int64_t)tile;
-    r0 = g * per;
-    r1 = r0 + per;
+    if (groups <= 8) {
+      r0 = g * (8 / groups);
+      r1 = r0 + 8 / groups;
+    } else {
+      r0 = 8 + g;
+      r1 = r0 + 1;
+    }
     return true;
   }
 }

@@ -157,17 +157,21 @@ const int kCand[][2] = {{0, 0}, {2, 0}, {0, 2}, {2, 2}};
 constexpr int kNCand = 4;
 
 // Candidate shapes of the quadrature-only kernel: the default (points by the
-// rule, whole tiles), about half the points per lane block (fewer registers,
-// more resident warps), and 2 or 4 warp tasks per tile (more tasks than
-// warps for small meshes).
+// rule, tasks per tile by the tile count), about half the points per lane
+// block (fewer registers, more resident warps), and the next finer and the
+// next coarser split of a tile into warp tasks (1, 2, 4, 8, 32).
 constexpr int kNFastCand = 4;
-void fast_cand(bool mixed, int pmax, size_t c, int& qb, int& groups) {
+void fast_cand(bool mixed, int pmax, int64_t n_tiles, int sm_count, size_t c, int& qb, int& groups) {
+  static const int steps[5] = {1, 2, 4, 8, 32};
   const int d = fast_qb_default(mixed, pmax);
+  const int ga = fast_groups_auto(n_tiles, sm_count);
+  int k = 0;
+  while (steps[k] != ga) ++k;
   qb = d;
-  groups = 1;
+  groups = ga;
   if (c == 1) qb = std::max(2, (d + 1) / 2);
-  if (c == 2) groups = 2;
-  if (c == 3) groups = 4;
+  if (c == 2) groups = steps[k < 4 ? k + 1 : 2];
+  if (c == 3) groups = steps[k > 0 ? k - 1 : 2];
 }
 
 // launch class: precision, surface or curve mesh, occlusion
@@ -268,7 +272,7 @@ int admit_one(rvf_server* sv, Req* r) {
   FastTune t;
   const double gpp = (double)r->w.n_fast_tiles * kTile * kTile * r->w.pmax * r->w.pmax * 1e-9;
   for (int c = 0; c < kNFastCand; ++c) {
-    fast_cand(r->w.mixed, r->w.pmax, (size_t)c, r->w.fast_qb, r->w.fast_groups);
+    fast_cand(r->w.mixed, r->w.pmax, r->w.n_fast_tiles, s->sm_count, (size_t)c, r->w.fast_qb, r->w.fast_groups);
     cudaEventRecord(s->ev[0], s->stream);
     if ((rc = wave_fast(s, r->w, nullptr))) return rc;
     cudaEventRecord(s->ev[1], s->stream);
@@ -280,7 +284,7 @@ int admit_one(rvf_server* sv, Req* r) {
   size_t b = 0;
   for (size_t c = 1; c < (size_t)kNFastCand; ++c)
     if (t.score[c] < t.score[b]) b = c;
-  fast_cand(r->w.mixed, r->w.pmax, b, t.qb, t.groups);
+  fast_cand(r->w.mixed, r->w.pmax, r->w.n_fast_tiles, s->sm_count, b, t.qb, t.groups);
   t.done = true;
   std::lock_guard<std::mutex> lk2(s->tune_mu);
   if (!s->ftune[fkey].done) {

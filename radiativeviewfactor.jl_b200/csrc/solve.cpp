@@ -79,8 +79,9 @@ int validate_options(const rvf_mesh* m, const rvf_options* o) {
       !fast_qb_supported(o->precision == RVF_PREC_MIXED && m->dim == 2 && o->method == RVF_METHOD_QUADRATURE,
                          o->fast_points))
     return set_err(RVF_EINVAL, "fast_points %d is not a compiled block for this precision", o->fast_points);
-  if (o->fast_row_groups != 0 && o->fast_row_groups != 1 && o->fast_row_groups != 2 && o->fast_row_groups != 4)
-    return set_err(RVF_EINVAL, "fast_row_groups must be 0, 1, 2 or 4, got %d", o->fast_row_groups);
+  if (o->fast_row_groups != 0 && o->fast_row_groups != 1 && o->fast_row_groups != 2 && o->fast_row_groups != 4 &&
+      o->fast_row_groups != 8 && o->fast_row_groups != 32)
+    return set_err(RVF_EINVAL, "fast_row_groups must be 0, 1, 2, 4, 8 or 32, got %d", o->fast_row_groups);
   if (o->self_vf && o->method == RVF_METHOD_MONTE_CARLO)
     return set_err(RVF_EINVAL, "self_vf is supported with quadrature only");
   return RVF_OK;

@@ -88,7 +88,7 @@ int wave_prepare(Session* s, rvf_mesh* m, Tables* T, const rvf_options* o, uint8
   w.pmax = T->pmax;
   if (o->fault_inject & RVF_FAULT_CLAIM) w.claim_retries = 0;
   w.fast_qb = o->fast_points;
-  w.fast_groups = o->fast_row_groups > 0 ? o->fast_row_groups : 1;
+  w.fast_groups = o->fast_row_groups;  // 0: by the tile count (wave_fast)
   PairArgs& a = w.pa;
   a.N = N;
   a.nT = (N + kTile - 1) / kTile;
@@ -231,11 +231,20 @@ int wave_prepare(Session* s, rvf_mesh* m, Tables* T, const rvf_options* o, uint8
   return 0;
 }
 
+int fast_groups_auto(int64_t n_tiles, int sm_count) {
+  const int64_t want = (int64_t)4 * 16 * std::max(sm_count, 1);  // four tasks per resident warp (16 per SM)
+  int g = 1;
+  while (g < 32 && n_tiles * g < want) g = g == 8 ? 32 : 2 * g;
+  return g;
+}
+
 int wave_fast(Session* s, WaveReq& w, int64_t* n_kernels) {
   if (!w.pa.tcls || w.pa.ray_log || w.pa.n_tiles == 0) return 0;
   int rc = 0;
   if (!s->fast_ctr.ptr && (rc = s->fast_ctr.alloc(s, 256))) return rc;
-  w.pa.fast_groups = w.ma.fast_groups = w.fast_groups;
+  w.pa.fast_groups = w.ma.fast_groups =
+      w.fast_groups > 0 ? w.fast_groups : fast_groups_auto(w.n_fast_tiles > 0 ? w.n_fast_tiles : w.pa.n_tiles,
+                                                           s->sm_count);
   const int qb = w.fast_qb > 0 ? w.fast_qb : fast_qb_default(w.mixed, w.pmax);
   cudaError_t e = cudaMemsetAsync(s->fast_ctr.ptr, 0, sizeof(unsigned long long), s->stream);
   if (e == cudaSuccess)

@@ -23,7 +23,7 @@ struct WaveReq {
   int64_t claimed = 0;  // tiles integrated so far
   int claim_retries = 4096;  // compare-and-swap attempts of a tile claim (0: every claim gives up)
   int fast_qb = 0;           // quadrature-only kernel shape: points per lane block (0: by the rule)
-  int fast_groups = 1;       //   and warp tasks per tile
+  int fast_groups = 0;       //   and warp tasks per tile (0: fast_groups_auto)
   int64_t n_fast_tiles = 0;  // tiles of the quadrature-only kernel
   const NodeD* nodes_d = nullptr;
   const NodeF* nodes_f = nullptr;
@@ -46,6 +46,9 @@ int wave_prepare(Session* s, rvf_mesh* m, Tables* T, const rvf_options* o, uint8
 WaveShape wave_shape(Session* s, WaveReq* const* reqs, int n);
 // The request's tiles without shadow-ray work (by class), before its chunks;
 // the chunks then skip them.  No-op without tile classes or with a ray log.
+// Warp tasks per tile of the quadrature-only kernel when the caller names
+// none: the fewest of 1, 2, 4, 8, 32 that give four tasks per resident warp.
+int fast_groups_auto(int64_t n_tiles, int sm_count);
 int wave_fast(Session* s, WaveReq& w, int64_t* n_kernels);
 // One chunk over n requests of one shape (mixed, dim3, occ equal): claims
 // tiles in request order while the queues have room, traces and resolves

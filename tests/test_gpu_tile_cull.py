@@ -133,7 +133,7 @@ def test_fast_kernel_shapes_bit_identical(rvf, session, precision):
             N = md.n_elems
             ref = None
             for qb in (0,) + points:
-                for groups in (1, 2, 4):
+                for groups in (0, 1, 2, 4, 8, 32):
                     o = rvf.make_options(nquad, precision=precision, seed=0)
                     o.fast_points, o.fast_row_groups = qb, groups
                     F = np.empty((N, N), order="F")
