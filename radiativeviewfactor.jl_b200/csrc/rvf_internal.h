@@ -45,7 +45,7 @@ struct DevBuf {
 };
 
 int upload(Session* s, DevBuf& b, const void* src, size_t n);
-constexpr size_t kSpareMin = (size_t)64 << 20;
+constexpr size_t kSpareMin = (size_t)1 << 20;
 void release_spares(Session* s);
 
 struct Tables {
@@ -104,7 +104,7 @@ struct rvf_session {
   std::map<uint64_t, cudaGraphExec_t> graphs;
   std::set<rvf_mesh*> meshes;
   cudaEvent_t ev[8] = {};
-  // Freed device buffers of kSpareMin bytes or more, kept for reuse and still
+  // Freed device buffers of kSpareMin bytes (1 MiB) or more, kept for reuse and still
   // charged to the budget: solving one new mesh after another (an F of
   // 15 GB each) then skips cudaMalloc / cudaFree, whose mapping work costs
   // a few hundred milliseconds per mesh.  Dropped when an allocation would
@@ -164,6 +164,7 @@ int ensure_tables(Session* s, rvf_mesh* m, int nquad, Tables** out);
 int read_err(Session* s);
 int validate_options(const rvf_mesh* m, const rvf_options* o);
 int no_progress(Session* s);
+int reduce_alloc(Session* s, rvf_mesh* m);  // the reductions' buffers (before any kernel runs)
 int run_reduce(Session* s, rvf_mesh* m, const double* area);
 // The self pairs (i, i) of a quadrature solve with the pipeline's FP64
 // arguments, counted in the session's counters.

@@ -233,6 +233,7 @@ int admit_one(rvf_server* sv, Req* r) {
       if ((rc = m->mc_area.alloc(s, sizeof(double) * std::max<int64_t>(N, 1)))) return rc;
     if (m->F.bytes < sizeof(double) * N * N)
       if ((rc = m->F.alloc(s, sizeof(double) * std::max<int64_t>(N * N, 1)))) return rc;
+    if ((rc = reduce_alloc(s, m))) return rc;
     m->has_result = false;
     r->mc_tiles = nT * (nT + 1) / 2;
     return RVF_OK;
@@ -243,6 +244,7 @@ int admit_one(rvf_server* sv, Req* r) {
   const int64_t N = m->N;
   if (m->F.bytes < sizeof(double) * N * N)
     if ((rc = m->F.alloc(s, sizeof(double) * std::max<int64_t>(N * N, 1)))) return rc;
+  if ((rc = reduce_alloc(s, m))) return rc;
   m->has_result = false;
   if (N == 1) cudaMemsetAsync(m->F.ptr, 0, sizeof(double), s->stream);
   if ((rc = wave_prepare(s, m, r->T, &r->opts, nullptr, r->w, nullptr))) return rc;

@@ -133,10 +133,12 @@ cudaError_t launch_self_pairs(Session* s, const PairArgs& pa, cudaStream_t st) {
   return launch_self(a, st);
 }
 
-int run_reduce(Session* s, rvf_mesh* m, const double* area) {
+// The reductions' buffers, allocated before the pair pipeline starts: an
+// allocation while kernels and F copies are in flight can wait for them.
+int reduce_alloc(Session* s, rvf_mesh* m) {
   const int64_t N = m->N;
   if (N == 0 || m->G == 0) return RVF_OK;
-  int n_chunks = (int)std::min<int64_t>(256, std::max<int64_t>(1, (1 << 20) / std::max<int64_t>(N, 1)));
+  const int n_chunks = (int)std::min<int64_t>(256, std::max<int64_t>(1, (1 << 20) / std::max<int64_t>(N, 1)));
   int rc;
   if (m->part.bytes < sizeof(double) * n_chunks * m->G * N)
     if ((rc = m->part.alloc(s, sizeof(double) * n_chunks * m->G * N))) return rc;
@@ -148,6 +150,15 @@ int run_reduce(Session* s, rvf_mesh* m, const double* area) {
     if ((rc = m->Fgroup.alloc(s, sizeof(double) * m->G * m->G))) return rc;
   if (m->Agroup.bytes < sizeof(double) * m->G)
     if ((rc = m->Agroup.alloc(s, sizeof(double) * m->G))) return rc;
+  return RVF_OK;
+}
+
+int run_reduce(Session* s, rvf_mesh* m, const double* area) {
+  const int64_t N = m->N;
+  if (N == 0 || m->G == 0) return RVF_OK;
+  const int n_chunks = (int)std::min<int64_t>(256, std::max<int64_t>(1, (1 << 20) / std::max<int64_t>(N, 1)));
+  int rc = reduce_alloc(s, m);
+  if (rc) return rc;
   RedArgs r{};
   r.N = N;
   r.G = m->G;
@@ -476,12 +487,14 @@ int rvf_solve(rvf_session* s, rvf_mesh* m, const rvf_options* o, double* F_elem,
     EvTimer t(s->stream);
     const bool fresh = m->tables.find(o->nquad) == m->tables.end();
     if ((rc = ensure_tables(s, m, o->nquad, &T))) return rc;
+    if ((rc = reduce_alloc(s, m))) return rc;
     if (fresh && N > 0) n_kernels += 1;
     S.ms_prep = t.stop();
     area_res = T->area_orig.as<double>();
   } else {
     if (m->mc_area.bytes < sizeof(double) * std::max<int64_t>(N, 1))
       if ((rc = m->mc_area.alloc(s, sizeof(double) * std::max<int64_t>(N, 1)))) return rc;
+    if ((rc = reduce_alloc(s, m))) return rc;
     area_res = m->mc_area.as<double>();
   }
   if (m->F.bytes < sizeof(double) * N * N)
