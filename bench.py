@@ -446,6 +446,7 @@ def run_serve(rvf, sess, size: str, local: int):
     # the work the server does per request; each after one warm-up solve of
     # its own mesh (session buffers and launch graphs warm, as in a service)
     t_alone, t_solve_only = [], []
+    clk_alone = Clocks(local).__enter__()
     for k in burst:
         r = reqs[k]
         dm = _abi.DeviceMesh(sess, arrays[k])
@@ -459,12 +460,14 @@ def run_serve(rvf, sess, size: str, local: int):
         dm.solve(r["opts"])
         dm.release()
         t_alone.append(time.perf_counter() - t0)
+    clk_alone.__exit__(None, None, None)
     # the burst: the same requests submitted at once to a server of their own,
     # each released when done; timed on its second pass, when the session's
     # buffer cache holds F buffers for the burst's concurrent requests (as the
     # one-at-a-time solves above reuse theirs: a service in steady state)
     for rep in range(2):
         sv = _abi.Server(sess, admit_bytes=admit)
+        clk_burst = Clocks(local).__enter__()
         t0 = time.perf_counter()
         rids = {sv.submit(arrays[k], reqs[k]["opts"]) for k in burst}
         while rids:  # release in completion order
@@ -475,6 +478,7 @@ def run_serve(rvf, sess, size: str, local: int):
             if not done:
                 time.sleep(0.0005)
         t_burst = time.perf_counter() - t0
+        clk_burst.__exit__(None, None, None)
         st_burst = sv.stats()
         sv.close()
     # Offered load: each request's cost is its work (quadrature point pairs or
@@ -581,6 +585,7 @@ def run_serve(rvf, sess, size: str, local: int):
                          "release -- the work the server does per request",
         "one_at_a_time_solve_only_pairs_per_s": burst_pairs / sum(t_solve_only),
         "burst_over_one_at_a_time": sum(t_alone) / t_burst,
+        "clocks_one_at_a_time": clk_alone.summary(), "clocks_burst": clk_burst.summary(),
         "lambda_per_s": lam, "offered_load": 0.8, "estimated_service_s": est_service,
         "max_abs_dF_vs_fp64_solo": dF, "checked_requests": n_checked,
         "check": "64 rows and columns of each checked served F against a plain FP64 one-at-a-time solve",

@@ -313,7 +313,9 @@ int rvf_request_result(rvf_server* sv, int64_t id, double* F_elem, double* A_ele
 /* Device addresses of a done request's F (n_elems^2, column-major) and A,
  * valid until rvf_release: for callers that read the result on the GPU. */
 int rvf_request_result_device(rvf_server* sv, int64_t id, const double** F_dev, const double** A_dev);
-/* Frees a finished request's device memory and its admission charge. */
+/* Drops a finished request: its admission charge at once, its device memory
+ * when the server's worker next looks for work (the caller does not wait
+ * for a running chunk). */
 int rvf_release(rvf_server* sv, int64_t id);
 int rvf_server_stats_get(rvf_server* sv, rvf_server_stats* st);
 

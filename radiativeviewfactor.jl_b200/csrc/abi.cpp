@@ -94,7 +94,7 @@ int DevBuf::alloc(Session* s, size_t n) {
     }
     if (s->used + c <= s->budget || s->used + n > s->budget) n = c;  // the class when it fits the budget
   }
-  if (s->used + n > s->budget) release_spares(s);
+  if (s->used + n > s->budget) release_spares(s, n);
   if (s->used + n > s->budget)
     return set_err(RVF_EBUDGET, "HBM budget exceeded: need %zu more bytes, %zu of %zu in use", n, s->used,
                    s->budget);
@@ -131,13 +131,15 @@ void DevBuf::free_() {
   owner = nullptr;
 }
 
-void release_spares(Session* s) {
+void release_spares(Session* s, size_t need) {
   std::lock_guard<std::mutex> lk(s->spare_mu);
-  for (auto& sp : s->spares) {
-    cudaFree(sp.first);
-    s->used -= sp.second;
+  // the oldest first (the front of the list), until `need` more bytes fit
+  size_t k = 0;
+  for (; k < s->spares.size() && (need == 0 || s->used + need > s->budget); ++k) {
+    cudaFree(s->spares[k].first);
+    s->used -= s->spares[k].second;
   }
-  s->spares.clear();
+  s->spares.erase(s->spares.begin(), s->spares.begin() + (std::ptrdiff_t)k);
 }
 
 int upload(Session* s, DevBuf& b, const void* src, size_t n) {

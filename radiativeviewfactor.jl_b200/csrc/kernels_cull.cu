@@ -163,7 +163,11 @@ __device__ __forceinline__ bool hull_misses_tri(const HullF& H, const float4& p0
 }  // namespace
 
 // One warp per tile, grid-stride over the tiles of one request.
-__global__ void __launch_bounds__(kCullWarps * 32) k_tile_class(const TileClassArgs a) {
+// resident blocks per SM the classification is compiled for
+#ifndef RVF_CULL_MIN_BLOCKS
+#define RVF_CULL_MIN_BLOCKS 1
+#endif
+__global__ void __launch_bounds__(kCullWarps * 32, RVF_CULL_MIN_BLOCKS) k_tile_class(const TileClassArgs a) {
   __shared__ int s_front[kCullWarps][2 * kTileFront];
   __shared__ int s_leaf[kCullWarps][kTileLeaves];
   __shared__ int s_list[kCullWarps][kTileTris];

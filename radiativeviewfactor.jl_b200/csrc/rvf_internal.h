@@ -46,7 +46,9 @@ struct DevBuf {
 
 int upload(Session* s, DevBuf& b, const void* src, size_t n);
 constexpr size_t kSpareMin = (size_t)1 << 20;
-void release_spares(Session* s);
+// Frees cached buffers, the oldest first, until `need` more bytes fit the
+// budget (need = 0: all of them).
+void release_spares(Session* s, size_t need = 0);
 
 struct Tables {
   int nquad = 0, pmax = 0;

@@ -130,6 +130,7 @@ struct rvf_server {
   std::deque<Req*> queue;
   std::vector<Req*> active;
   std::map<int64_t, std::unique_ptr<Req>> reqs;
+  std::vector<rvf_mesh*> to_free;  // meshes of released requests, freed by the worker
   int64_t next_id = 1;
   bool closing = false;
   std::thread worker;
@@ -203,10 +204,13 @@ void finish(rvf_server* sv, Req* r, int state, int status) {  // sv->mu held
   sv->cv_done.notify_all();
 }
 
-// Frees a request's device memory and its admission charge (sv->mu held).
+// Hands a request's device memory to the worker, which frees it before its
+// next admission, and drops the request's admission charge (sv->mu held).
+// The caller -- rvf_release on a client thread -- thus never waits for the
+// session lock, which the worker holds while a chunk runs.
 void drop_device(rvf_server* sv, Req* r) {
   if (r->m) {
-    rvf_mesh_release(sv->s, r->m);
+    sv->to_free.push_back(r->m);
     r->m = nullptr;
     r->T = nullptr;
   }
@@ -511,8 +515,19 @@ void worker_main(rvf_server* sv) {
   }
 }
 
+// Frees the meshes of released and failed requests (no lock held).
+void free_released(rvf_server* sv) {
+  std::vector<rvf_mesh*> fr;
+  {
+    std::lock_guard<std::mutex> lk(sv->mu);
+    fr.swap(sv->to_free);
+  }
+  for (rvf_mesh* m : fr) rvf_mesh_release(sv->s, m);
+}
+
 void worker_loop(rvf_server* sv) {
   for (;;) {
+    free_released(sv);
     std::vector<Req*> admit;
     {
       std::unique_lock<std::mutex> lk(sv->mu);
@@ -674,6 +689,7 @@ int rvf_server_destroy(rvf_server* sv) try {
     for (auto& kv : sv->reqs) drop_device(sv, kv.second.get());
     sv->reqs.clear();
   }
+  free_released(sv);
   delete sv;
   return RVF_OK;
 } catch (...) {
