@@ -56,6 +56,22 @@ constexpr int kCullWarps = 4;
 #define RVF_MASK_FULL_AXES 0
 #endif
 
+// Position of the n-th (from 0) set bit of m (n < popc(m)): binary search
+// over halves by population count.
+__device__ __forceinline__ int nth_set_bit(uint32_t m, int n) {
+  int pos = 0;
+#pragma unroll
+  for (int s = 16; s >= 1; s >>= 1) {
+    const int c = __popc(m & ((1u << s) - 1u));
+    if (n >= c) {
+      n -= c;
+      m >>= s;
+      pos += s;
+    }
+  }
+  return pos;
+}
+
 // H = conv(B_1 u B_2) of two boxes (FP32 centres c and half extents h).
 struct HullF {
   float c[2][3], h[2][3];
@@ -174,6 +190,7 @@ __global__ void __launch_bounds__(kCullWarps * 32, RVF_CULL_MIN_BLOCKS) k_tile_c
   __shared__ int s_rleaf[kCullWarps][kTileLeaves];  // runs of the list: leaf node
   __shared__ int s_rspan[kCullWarps][kTileLeaves];  //   first list entry * 16 + count
   __shared__ int s_row[kCullWarps][kTileLeaves];    // a row's runs
+  __shared__ float s_cap[kCullWarps][32][12];        // a row's pairs: capsule start, end, direction, R, group
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   int* front = s_front[warp];
   int* leaves = s_leaf[warp];
@@ -416,23 +433,53 @@ __global__ void __launch_bounds__(kCullWarps * 32, RVF_CULL_MIN_BLOCKS) k_tile_c
           for (int c = 0; c < 3; ++c) df[c] = bf[c] - cap.A[c];
           Rf = (float)R;
         }
-        bool bit = false, done = !valid;
+        // Each pair's capsule against each run's leaf (lanes are pairs), then
+        // the (pair, triangle) tests of each run dealt out to the lanes --
+        // lane w of a round takes test w: pair w / count, triangle w % count
+        // -- so the lanes stay busy however few pairs reach a leaf.  A pair
+        // leaves once one of its triangles survives.
+        float* cd = s_cap[warp][lane];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          cd[c] = cap.A[c];
+          cd[3 + c] = bf[c];
+          cd[6 + c] = df[c];
+        }
+        cd[9] = Rf;
+        cd[10] = __int_as_float(gj);
+        const uint32_t none = __ballot_sync(kFull, !valid);
+        // the pairs reaching each run's leaf, in the walk's leaf array (not
+        // needed once the runs are recorded)
+        uint32_t* pms = reinterpret_cast<uint32_t*>(leaves);
         for (int e = 0; e < nr; ++e) {
-          if (__all_sync(kFull, done)) break;
-          const int r = rowl[e];
-          const int span = rspan[r];
-          if (done || capsule_misses_box(cap, a.nodesf[rleaf[r]])) continue;
-          for (int k = span >> 4; k < (span >> 4) + (span & 15) && !bit; ++k) {
-            const int u = list[k];
+          const bool pass = valid && !capsule_misses_box(cap, a.nodesf[rleaf[rowl[e]]]);
+          const uint32_t pm = __ballot_sync(kFull, pass);
+          if (lane == 0) pms[e] = pm;
+        }
+        __syncwarp();
+        uint32_t hit = 0;
+        for (int e = 0; e < nr; ++e) {
+          const uint32_t pm = pms[e] & ~hit & ~none;
+          if (pm == 0) continue;  // warp-uniform
+          const int span = rspan[rowl[e]], k0 = span >> 4, cnt = span & 15;
+          const int total = __popc(pm) * cnt;
+          uint32_t h = 0;
+          for (int w = lane; w < total; w += 32) {
+            const int pi = w / cnt, ti = w - pi * cnt;
+            const int p = nth_set_bit(pm, pi);
+            const float* q = s_cap[warp][p];
+            const int u = list[k0 + ti];
             const float4 p0 = a.sat[3 * u], p1 = a.sat[3 * u + 1], p2 = a.sat[3 * u + 2];
             const int32_t g = __float_as_int(p1.w);
-            if (g == g_i || g == gj) continue;
-            const bool miss = RVF_MASK_FULL_AXES ? pair_misses_tri_full(cap.A, bf, df, Rf, a.sat_em, p0, p1, p2)
-                                                 : pair_misses_tri(cap.A, bf, df, Rf, a.sat_em, p0, p1, p2);
-            bit = !miss;
+            if (g == g_i || g == __float_as_int(q[10])) continue;
+            const float qa[3] = {q[0], q[1], q[2]}, qb[3] = {q[3], q[4], q[5]}, qd[3] = {q[6], q[7], q[8]};
+            const bool miss = RVF_MASK_FULL_AXES ? pair_misses_tri_full(qa, qb, qd, q[9], a.sat_em, p0, p1, p2)
+                                                 : pair_misses_tri(qa, qb, qd, q[9], a.sat_em, p0, p1, p2);
+            if (!miss) h |= 1u << p;
           }
-          done = done || bit;
+          hit |= __reduce_or_sync(kFull, h);
         }
+        const bool bit = (hit >> lane) & 1u;
         __syncwarp();
         const uint32_t m = __ballot_sync(kFull, bit);
         if (lane == 0) {
