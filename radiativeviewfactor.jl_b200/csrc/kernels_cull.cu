@@ -50,7 +50,6 @@ namespace rvf {
 namespace {
 
 constexpr int kCullWarps = 4;
-constexpr int kMaskBlock = 8;  // runs per block of the mask stage
 
 // Pair masks: the capsule test over all 16 axes (1) or the pair lists' 4 (0).
 #ifndef RVF_MASK_FULL_AXES
@@ -182,7 +181,7 @@ __device__ __forceinline__ bool hull_misses_tri(const HullF& H, const float4& p0
 // One warp per tile, grid-stride over the tiles of one request.
 // resident blocks per SM the classification is compiled for
 #ifndef RVF_CULL_MIN_BLOCKS
-#define RVF_CULL_MIN_BLOCKS 4
+#define RVF_CULL_MIN_BLOCKS 1
 #endif
 __global__ void __launch_bounds__(kCullWarps * 32, RVF_CULL_MIN_BLOCKS) k_tile_class(const TileClassArgs a) {
   __shared__ int s_front[kCullWarps][2 * kTileFront];
@@ -449,41 +448,36 @@ __global__ void __launch_bounds__(kCullWarps * 32, RVF_CULL_MIN_BLOCKS) k_tile_c
         cd[9] = Rf;
         cd[10] = __int_as_float(gj);
         const uint32_t none = __ballot_sync(kFull, !valid);
-        // the pairs reaching each leaf of a block of runs, in the walk's leaf
-        // array (not needed once the runs are recorded); blocks of runs so
-        // that pairs already known to be blockable skip the later leaves
+        // the pairs reaching each run's leaf, in the walk's leaf array (not
+        // needed once the runs are recorded)
         uint32_t* pms = reinterpret_cast<uint32_t*>(leaves);
+        for (int e = 0; e < nr; ++e) {
+          const bool pass = valid && !capsule_misses_box(cap, a.nodesf[rleaf[rowl[e]]]);
+          const uint32_t pm = __ballot_sync(kFull, pass);
+          if (lane == 0) pms[e] = pm;
+        }
+        __syncwarp();
         uint32_t hit = 0;
-        for (int e0 = 0; e0 < nr && (hit | none) != kFull; e0 += kMaskBlock) {
-          const int e1 = min(nr, e0 + kMaskBlock);
-          for (int e = e0; e < e1; ++e) {
-            const bool pass = valid && !((hit >> lane) & 1u) && !capsule_misses_box(cap, a.nodesf[rleaf[rowl[e]]]);
-            const uint32_t pm = __ballot_sync(kFull, pass);
-            if (lane == 0) pms[e - e0] = pm;
+        for (int e = 0; e < nr; ++e) {
+          const uint32_t pm = pms[e] & ~hit & ~none;
+          if (pm == 0) continue;  // warp-uniform
+          const int span = rspan[rowl[e]], k0 = span >> 4, cnt = span & 15;
+          const int total = __popc(pm) * cnt;
+          uint32_t h = 0;
+          for (int w = lane; w < total; w += 32) {
+            const int pi = w / cnt, ti = w - pi * cnt;
+            const int p = nth_set_bit(pm, pi);
+            const float* q = s_cap[warp][p];
+            const int u = list[k0 + ti];
+            const float4 p0 = a.sat[3 * u], p1 = a.sat[3 * u + 1], p2 = a.sat[3 * u + 2];
+            const int32_t g = __float_as_int(p1.w);
+            if (g == g_i || g == __float_as_int(q[10])) continue;
+            const float qa[3] = {q[0], q[1], q[2]}, qb[3] = {q[3], q[4], q[5]}, qd[3] = {q[6], q[7], q[8]};
+            const bool miss = RVF_MASK_FULL_AXES ? pair_misses_tri_full(qa, qb, qd, q[9], a.sat_em, p0, p1, p2)
+                                                 : pair_misses_tri(qa, qb, qd, q[9], a.sat_em, p0, p1, p2);
+            if (!miss) h |= 1u << p;
           }
-          __syncwarp();
-          for (int e = e0; e < e1; ++e) {
-            const uint32_t pm = pms[e - e0] & ~hit;
-            if (pm == 0) continue;  // warp-uniform
-            const int span = rspan[rowl[e]], k0 = span >> 4, cnt = span & 15;
-            const int total = __popc(pm) * cnt;
-            uint32_t h = 0;
-            for (int w = lane; w < total; w += 32) {
-              const int pi = w / cnt, ti = w - pi * cnt;
-              const int p = nth_set_bit(pm, pi);
-              const float* q = s_cap[warp][p];
-              const int u = list[k0 + ti];
-              const float4 p0 = a.sat[3 * u], p1 = a.sat[3 * u + 1], p2 = a.sat[3 * u + 2];
-              const int32_t g = __float_as_int(p1.w);
-              if (g == g_i || g == __float_as_int(q[10])) continue;
-              const float qa[3] = {q[0], q[1], q[2]}, qb[3] = {q[3], q[4], q[5]}, qd[3] = {q[6], q[7], q[8]};
-              const bool miss = RVF_MASK_FULL_AXES ? pair_misses_tri_full(qa, qb, qd, q[9], a.sat_em, p0, p1, p2)
-                                                   : pair_misses_tri(qa, qb, qd, q[9], a.sat_em, p0, p1, p2);
-              if (!miss) h |= 1u << p;
-            }
-            hit |= __reduce_or_sync(kFull, h);
-          }
-          __syncwarp();
+          hit |= __reduce_or_sync(kFull, h);
         }
         const bool bit = (hit >> lane) & 1u;
         __syncwarp();
