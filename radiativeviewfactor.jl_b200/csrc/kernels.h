@@ -66,6 +66,7 @@ struct TileClassArgs {
   double tiny_gap;     // pairs closer than rad_i + rad_j + tiny_gap are kClsTiny
   double cull_margin;
   bool occ, dim3;
+  bool skip_groups;  // rays skip the triangles of their elements' groups (false: a ray may hit any triangle)
   const NodeF* nodesf;
   int n_nodes;
   const int32_t* frontier;
@@ -389,11 +390,24 @@ struct McArgs {
   const TriD* tris;
   const SegD* segs;
   double cand_margin;  // curves: distance beyond which rounding cannot let a segment block a ray
+  const uint8_t* tcls;    // surfaces with occlusion: tile classes and masks (kernels_cull.cu) for the
+  const uint32_t* tmask;  //   elements' whole extent, or null (every sample ray walks the tree)
   unsigned long long* tile_counter;
   unsigned long long* counters;
   uint8_t* ray_log;  // [(i*N + j) * n_samples + k] for caller indices i < j
 };
 
+// Centres (of the nodes) and radii bounding every point of each surface
+// element, for the tile classification of Monte Carlo solves.
+struct McBoundsArgs {
+  int64_t N;
+  const double* coords;
+  const int32_t* enodes;
+  const int8_t* fam;
+  double* cen;  // 3 x N
+  double* rad;  // N
+};
+cudaError_t launch_mc_bounds(const McBoundsArgs& a, cudaStream_t st);
 // Blocks of the Monte Carlo kernel resident at once (its persistent grid).
 int mc_resident_blocks(const McArgs& a, int sm_count);
 cudaError_t launch_mc(const McArgs& a, int sm_count, cudaStream_t st);

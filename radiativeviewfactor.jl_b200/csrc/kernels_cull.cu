@@ -277,7 +277,7 @@ __global__ void __launch_bounds__(kCullWarps * 32, RVF_CULL_MIN_BLOCKS) k_tile_c
       }
       // one group per block: its triangles are skipped by every ray of the tile
       const int32_t gi0 = __shfl_sync(kFull, gi, 0), gj0 = __shfl_sync(kFull, gj, 0);
-      const bool g_same = __all_sync(kFull, (!oki || gi == gi0) && (!okj || gj == gj0));
+      const bool g_same = a.skip_groups && __all_sync(kFull, (!oki || gi == gi0) && (!okj || gj == gj0));
       double rj_max = rj;
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) rj_max = fmax(rj_max, __shfl_xor_sync(kFull, rj_max, o));
@@ -471,7 +471,7 @@ __global__ void __launch_bounds__(kCullWarps * 32, RVF_CULL_MIN_BLOCKS) k_tile_c
             const int u = list[k0 + ti];
             const float4 p0 = a.sat[3 * u], p1 = a.sat[3 * u + 1], p2 = a.sat[3 * u + 2];
             const int32_t g = __float_as_int(p1.w);
-            if (g == g_i || g == __float_as_int(q[10])) continue;
+            if (a.skip_groups && (g == g_i || g == __float_as_int(q[10]))) continue;
             const float qa[3] = {q[0], q[1], q[2]}, qb[3] = {q[3], q[4], q[5]}, qd[3] = {q[6], q[7], q[8]};
             const bool miss = RVF_MASK_FULL_AXES ? pair_misses_tri_full(qa, qb, qd, q[9], a.sat_em, p0, p1, p2)
                                                  : pair_misses_tri(qa, qb, qd, q[9], a.sat_em, p0, p1, p2);

@@ -216,6 +216,34 @@ __device__ int mc_candidates(const McArgs& a, const double* ca, const double* cb
 }  // namespace
 
 // Area rule: one thread per caller-order element.
+// Every point of a surface element is sum_k N_k(xi) x_k with sum_k N_k = 1,
+// so |x - c| <= (max_xi sum_k |N_k(xi)|) max_k |x_k - c| for any centre c.
+// That maximum (the node set's Lebesgue constant) is 1 for the linear
+// families (non-negative N), 5/3 for Tri6 (at the centroid: 3 x 1/9 + 3 x
+// 4/9) and 3 for Quad8 (at the centre: 4 x 1/4 + 4 x 1/2).  The radius is
+// rounded up by a relative 1e-9: a Monte Carlo sample point, evaluated in
+// FP64 from the same nodes, lies inside it.
+__global__ void k_mc_bounds(McBoundsArgs a) {
+  const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= a.N) return;
+  const int f = a.fam[e];
+  const int nn = f == 0 ? 8 : f == 1 ? 6 : f == 2 ? 4 : 3;
+  const double lam = f == 0 ? 3.0 : f == 1 ? 5.0 / 3.0 : 1.0;
+  const int32_t* en = a.enodes + 8 * e;
+  double c[3] = {0.0, 0.0, 0.0};
+  for (int k = 0; k < nn; ++k)
+    for (int d = 0; d < 3; ++d) c[d] += a.coords[3 * (int64_t)en[k] + d];
+  for (int d = 0; d < 3; ++d) c[d] /= nn;
+  double r2 = 0.0;
+  for (int k = 0; k < nn; ++k) {
+    const double* x = a.coords + 3 * (int64_t)en[k];
+    const double dx = x[0] - c[0], dy = x[1] - c[1], dz = x[2] - c[2];
+    r2 = fmax(r2, dx * dx + dy * dy + dz * dz);
+  }
+  for (int d = 0; d < 3; ++d) a.cen[3 * e + d] = c[d];
+  a.rad[e] = lam * sqrt(r2) * (1.0 + 1e-9);
+}
+
 __global__ void k_mc_area(McArgs a) {
   const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int64_t N = a.N;
@@ -266,9 +294,14 @@ __global__ void __launch_bounds__(256, DIM3 ? 2 : RVF_MC2D_MIN_BLOCKS) k_pairs_m
     tile_coords(t, a.nT, bi, bj);
     const int64_t j = bj * kTile + lane;
     const int64_t oj = (j < N) ? (int64_t)a.orig[j] : 0;
+    // surfaces: the tile's class; a pair outside its row's mask has no
+    // sample ray that can be blocked (its rays skip the traversal)
+    const uint8_t tcl = (DIM3 && OCC && a.tcls) ? a.tcls[t] : (uint8_t)kClsSlow;
     for (int rr = 0; rr < kTile / 8; ++rr) {
       const int64_t i = bi * kTile + warp + 8 * rr;
       if (i >= N) continue;  // warp-uniform
+      const bool may_block = !(DIM3 && OCC && a.tcls) ||
+                             ((tcl & kClsSlow) && ((a.tmask[t * kTile + warp + 8 * rr] >> lane) & 1u));
       const bool valid = (j < N) && (i < j);
       const int64_t oi = a.orig[i];
       const bool sw = valid && oi > oj;
@@ -310,7 +343,7 @@ __global__ void __launch_bounds__(256, DIM3 ? 2 : RVF_MC2D_MIN_BLOCKS) k_pairs_m
             const bool cast = (K > 0.0) && make_ray(xi, rx, ry, rz, r2, R);
             n_rays += cast ? 1 : 0;
             const bool blocked = packet_any_hit(
-                cast, a.nodes, a.n_nodes, [&](const NodeD& nd) { return slab_d(nd, R); },
+                cast && may_block, a.nodes, a.n_nodes, [&](const NodeD& nd) { return slab_d(nd, R); },
                 [&](int kk, bool test) {
                   const TriD tr = a.tris[kk];
                   if (!test || tr.group == gx || tr.group == gy) return false;
@@ -397,6 +430,12 @@ int mc_resident_blocks(const McArgs& a, int sm_count) {
                           : (occ ? (const void*)k_pairs_mc<false, true> : (const void*)k_pairs_mc<false, false>);
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 256, 0) != cudaSuccess || per_sm < 1) per_sm = 1;
   return sm_count * per_sm;
+}
+
+cudaError_t launch_mc_bounds(const McBoundsArgs& a, cudaStream_t st) {
+  if (a.N <= 0) return cudaSuccess;
+  k_mc_bounds<<<(unsigned)((a.N + 127) / 128), 128, 0, st>>>(a);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_mc(const McArgs& a, int sm_count, cudaStream_t st) {

@@ -136,6 +136,8 @@ struct rvf_mesh {
   rvf::DevBuf orig;                                             // int32 internal -> caller's index
   rvf::DevBuf inv;                                              // int32 caller's index -> internal
   rvf::DevBuf mc_area;                                          // Monte Carlo areas (caller's order)
+  rvf::DevBuf mc_cen, mc_rad, mc_tcls, mc_tmask;                // Monte Carlo tile classes (surfaces)
+  bool mc_cls_ready = false;                                    //   valid for the current options
   rvf::DevBuf nodes, tris_ref, tris_geo, segs;
   rvf::DevBuf nodesf, trisf_ref, trisf_geo;  // FP32 copies (mixed precision)
   rvf::DevBuf leaf_of;                        // int32 leaf node of each primitive (leaf order)
@@ -167,6 +169,7 @@ int read_err(Session* s);
 int validate_options(const rvf_mesh* m, const rvf_options* o);
 int no_progress(Session* s);
 int reduce_alloc(Session* s, rvf_mesh* m);  // the reductions' buffers (before any kernel runs)
+int mc_classify(Session* s, rvf_mesh* m, const rvf_options* o);  // Monte Carlo tile classes (surfaces)
 int run_reduce(Session* s, rvf_mesh* m, const double* area);
 // The self pairs (i, i) of a quadrature solve with the pipeline's FP64
 // arguments, counted in the session's counters.

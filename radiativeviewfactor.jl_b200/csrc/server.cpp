@@ -238,9 +238,11 @@ int admit_one(rvf_server* sv, Req* r) {
     if (m->F.bytes < sizeof(double) * N * N)
       if ((rc = m->F.alloc(s, sizeof(double) * std::max<int64_t>(N * N, 1)))) return rc;
     if ((rc = reduce_alloc(s, m))) return rc;
+    if ((rc = mc_classify(s, m, &r->opts))) return rc;
     m->has_result = false;
     r->mc_tiles = nT * (nT + 1) / 2;
-    return RVF_OK;
+    const cudaError_t e = cudaStreamSynchronize(s->stream);
+    return e == cudaSuccess ? RVF_OK : cuda_err(e, "request set-up");
   }
   if (r->opts.precision == RVF_PREC_MIXED && !(r->opts.near_field_factor >= 0.0))
     return set_err(RVF_EINVAL, "near_field_factor must be >= 0");

@@ -122,9 +122,65 @@ void fill_mc_args(Session* s, rvf_mesh* m, const rvf_options* o, uint8_t* ray_lo
     const double S = 2.0 * m->extent;
     c.cand_margin = 1e-5 * S * S * S + std::ldexp(S, -16);
   }
+  c.tcls = (occ && c.dim3 && m->mc_cls_ready) ? m->mc_tcls.as<uint8_t>() : nullptr;
+  c.tmask = c.tcls ? m->mc_tmask.as<uint32_t>() : nullptr;
   c.tile_counter = s->tile_counter.as<unsigned long long>();
   c.counters = s->counters.as<unsigned long long>();
   c.ray_log = ray_log;
+}
+
+// Tile classes for a Monte Carlo solve of a surface mesh with occlusion:
+// the quadrature pipeline's classification (kernels_cull.cu) with element
+// centres and radii that bound every point of each element (a sample can lie
+// anywhere on it), and, unless the solve skips the elements' own groups,
+// every triangle a candidate.  A pair outside its row's mask has no sample
+// ray that can be blocked.
+int mc_classify(Session* s, rvf_mesh* m, const rvf_options* o) {
+  m->mc_cls_ready = false;
+  const int64_t N = m->N;
+  const bool occ = o->occlusion && m->n_nodes > 0;
+  if (o->disable_tile_cull || !occ || m->dim != 2 || N == 0 || !m->frontier.ptr) return RVF_OK;
+  const int64_t nT = (N + kTile - 1) / kTile, nt = nT * (nT + 1) / 2;
+  int rc = 0;
+  if (m->mc_cen.bytes < sizeof(double) * 3 * N && (rc = m->mc_cen.alloc(s, sizeof(double) * 3 * N))) return rc;
+  if (m->mc_rad.bytes < sizeof(double) * N && (rc = m->mc_rad.alloc(s, sizeof(double) * N))) return rc;
+  if (m->mc_tcls.bytes < (size_t)nt && (rc = m->mc_tcls.alloc(s, (size_t)nt))) return rc;
+  if (m->mc_tmask.bytes < sizeof(uint32_t) * kTile * nt && (rc = m->mc_tmask.alloc(s, sizeof(uint32_t) * kTile * nt)))
+    return rc;
+  if (!s->fast_ctr.ptr && (rc = s->fast_ctr.alloc(s, 256))) return rc;
+  McBoundsArgs b{N, m->coords.as<double>(), m->enodes.as<int32_t>(), m->fam.as<int8_t>(), m->mc_cen.as<double>(),
+                 m->mc_rad.as<double>()};
+  cudaError_t e = launch_mc_bounds(b, s->stream);
+  if (e != cudaSuccess) return cuda_err(e, "Monte Carlo bounds launch");
+  TileClassArgs c{};
+  c.N = N;
+  c.nT = nT;
+  c.n_tiles = nt;
+  c.cen = m->mc_cen.as<double>();
+  c.rad = m->mc_rad.as<double>();
+  c.diam = c.rad;  // read only by the near-field pass, which is off
+  c.group = m->group.as<int32_t>();
+  c.near_factor = -1.0;
+  c.tiny_gap = -1.0;
+  c.cull_margin = std::ldexp(m->extent, -30);
+  c.occ = true;
+  c.dim3 = true;
+  c.skip_groups = o->mc_exclude_groups != 0;  // otherwise the rays skip group 0 only: test every triangle
+  c.nodesf = m->nodesf.as<NodeF>();
+  c.n_nodes = m->n_nodes;
+  c.frontier = m->frontier.as<int32_t>();
+  c.n_frontier = m->n_frontier;
+  c.leaf_of = m->leaf_of.as<int32_t>();
+  c.sat = o->geometric_soup ? m->sat_geo.as<float4>() : m->sat_ref.as<float4>();
+  c.sat_em = m->sat_em;
+  c.cls = m->mc_tcls.as<uint8_t>();
+  c.mask = m->mc_tmask.as<uint32_t>();
+  c.claim = s->fast_ctr.as<unsigned long long>() + 1;
+  c.counters = s->counters.as<unsigned long long>() + 13;
+  if ((e = launch_tile_class(c, s->sm_count, s->stream)) != cudaSuccess)
+    return cuda_err(e, "Monte Carlo tile classification launch");
+  m->mc_cls_ready = true;
+  return RVF_OK;
 }
 
 cudaError_t launch_self_pairs(Session* s, const PairArgs& pa, cudaStream_t st) {
@@ -517,6 +573,11 @@ int rvf_solve(rvf_session* s, rvf_mesh* m, const rvf_options* o, double* F_elem,
     log_bytes = lb;
   }
   if (mc) {  // src/GPUMCKernels.jl:295-328
+    {
+      EvTimer tc(s->stream);
+      if ((rc = mc_classify(s, m, o))) return rc;
+      S.ms_cull = tc.stop();
+    }
     McArgs c{};
     fill_mc_args(s, m, o, o->ray_log ? log.as<uint8_t>() : nullptr, c);
     if (N > 0) {

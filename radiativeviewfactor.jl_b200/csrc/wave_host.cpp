@@ -156,6 +156,7 @@ int wave_prepare(Session* s, rvf_mesh* m, Tables* T, const rvf_options* o, uint8
     c.tiny_gap = w.mixed ? std::ldexp(m->extent, -16) : -1.0;
     c.cull_margin = a.cull_margin;
     c.occ = occ;
+    c.skip_groups = true;
     c.dim3 = w.dim3;
     if (occ && w.dim3) {
       c.nodesf = m->nodesf.as<NodeF>();

@@ -133,3 +133,57 @@ def test_mc_public_api(rvf, orc):
     Fo, Ao, _, _ = oracle_mc(orc, md, 16, 99, [7])
     assert_same(res.F_elem, Fo)
     assert np.array_equal(res.A_elem, Ao)
+
+
+def _mc_solve(rvf, session, md, obs, n_samples, seed, exclude, cull):
+    from rvf_b200 import _abi
+    dm = _abi.DeviceMesh(session, rvf.mesh_desc_arrays(md, obs))
+    try:
+        N = md.n_elems
+        o = rvf.make_options(4, monte_carlo=True, n_samples=n_samples, seed=seed, mc_exclude_groups=exclude)
+        o.disable_tile_cull = 0 if cull else 1
+        lg = np.zeros(N * N * n_samples, dtype=np.uint8)
+        o.ray_log = lg.ctypes.data_as(_abi._pu8)
+        o.ray_log_pm = 1
+        F = np.empty((N, N), order="F")
+        A = np.empty(N)
+        st = dm.solve(o, F, A).as_dict()
+        return F, A, lg, st
+    finally:
+        dm.release()
+
+
+def _box_cylinder(rvf):
+    """Curved Quad8 walls and caps around a box: sample points bulge past the
+    elements' node hulls, which the classification's radii must cover."""
+    M = rvf.meshes
+    md = M.cylinder(nc=16, na=8, cap_rings=2, seed=3)
+    md.group_tri_soup[99] = M.obstruction_box(center=(0.0, 0.0, 0.5), edge=0.3, m=4)
+    return md, [99]
+
+
+@pytest.mark.parametrize("case", ["quad8_cube", "tri6_cube", "quad8_cylinder"])
+@pytest.mark.parametrize("exclude", [False, True])
+def test_mc_tile_masks_exact(rvf, orc, session, case, exclude):
+    """Surface Monte Carlo with occlusion skips the traversal of pairs outside
+    the tile classification's masks; every sample ray's decision, and so F,
+    stays the oracle's bit for bit, and equal to the unclassified solve."""
+    M = rvf.meshes
+    if case == "quad8_cube":
+        md, obs = M.cube_enclosure(8, family="quad", box_m=4), [7]
+    elif case == "tri6_cube":
+        md, obs = M.cube_enclosure(6, family="tri", box_m=4), [7]
+    else:
+        md, obs = _box_cylinder(rvf)
+    F, A, lg, st = _mc_solve(rvf, session, md, obs, 8, 4321, exclude, True)
+    F0, A0, lg0, st0 = _mc_solve(rvf, session, md, obs, 8, 4321, exclude, False)
+    assert st["n_tiles_culled"] > 0 and st0["n_tiles_culled"] == 0
+    assert st["n_rays"] == st0["n_rays"]
+    assert st["n_node_visits"] < st0["n_node_visits"]
+    assert np.array_equal(lg, lg0), f"{int((lg != lg0).sum())} ray decisions differ"
+    assert_same(F, F0)
+    Fo, Ao, lgo, _ = oracle_mc(orc, md, 8, 4321, obs, exclude, log=True)
+    assert (lgo == 2).sum() > 0, "the box must block some rays"
+    assert np.array_equal(lg, lgo), f"{int((lg != lgo).sum())} ray decisions differ from the oracle"
+    assert np.array_equal(A, Ao)
+    assert_same(F, Fo)
