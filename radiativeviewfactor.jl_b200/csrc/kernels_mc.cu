@@ -216,32 +216,54 @@ __device__ int mc_candidates(const McArgs& a, const double* ca, const double* cb
 }  // namespace
 
 // Area rule: one thread per caller-order element.
-// Every point of a surface element is sum_k N_k(xi) x_k with sum_k N_k = 1,
-// so |x - c| <= (max_xi sum_k |N_k(xi)|) max_k |x_k - c| for any centre c.
-// That maximum (the node set's Lebesgue constant) is 1 for the linear
-// families (non-negative N), 5/3 for Tri6 (at the centroid: 3 x 1/9 + 3 x
-// 4/9) and 3 for Quad8 (at the centre: 4 x 1/4 + 4 x 1/2).  The radius is
-// rounded up by a relative 1e-9: a Monte Carlo sample point, evaluated in
-// FP64 from the same nodes, lies inside it.
+// A point of a surface element: with each mid-side node written as its
+// edge's midpoint plus a deviation, x_m = (x_a + x_b) / 2 + delta_m, the
+// quadratic families reproduce their linear / bilinear interpolant, so
+//   x(xi) = sum_c L_c(xi) x_c + sum_m N_m(xi) delta_m
+// with L_c >= 0 summing to 1 (the corners' linear or bilinear functions) and
+// N_m >= 0 the mid-side functions, whose sum peaks at 2 (Quad8, at the
+// centre) and 4/3 (Tri6, at the centroid).  Hence |x - c| <= max_c |x_c - c|
+// + (2 or 4/3) max_m |delta_m| for the corners' centroid c.  Node order as
+// shape_surface: Quad8 mid-sides 4..7 on edges 0-1, 1-2, 2-3, 3-0; Tri6 3..5
+// on edges 0-1, 1-2, 0-2.  The radius is rounded up by a relative 1e-9: a
+// Monte Carlo sample point, evaluated in FP64 from the same nodes, lies
+// inside it.
 __global__ void k_mc_bounds(McBoundsArgs a) {
   const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= a.N) return;
   const int f = a.fam[e];
-  const int nn = f == 0 ? 8 : f == 1 ? 6 : f == 2 ? 4 : 3;
-  const double lam = f == 0 ? 3.0 : f == 1 ? 5.0 / 3.0 : 1.0;
+  const int nc = (f == 0 || f == 2) ? 4 : 3;
   const int32_t* en = a.enodes + 8 * e;
+  auto X = [&](int k) { return a.coords + 3 * (int64_t)en[k]; };
   double c[3] = {0.0, 0.0, 0.0};
-  for (int k = 0; k < nn; ++k)
-    for (int d = 0; d < 3; ++d) c[d] += a.coords[3 * (int64_t)en[k] + d];
-  for (int d = 0; d < 3; ++d) c[d] /= nn;
+  for (int k = 0; k < nc; ++k)
+    for (int d = 0; d < 3; ++d) c[d] += X(k)[d];
+  for (int d = 0; d < 3; ++d) c[d] /= nc;
   double r2 = 0.0;
-  for (int k = 0; k < nn; ++k) {
-    const double* x = a.coords + 3 * (int64_t)en[k];
+  for (int k = 0; k < nc; ++k) {
+    const double* x = X(k);
     const double dx = x[0] - c[0], dy = x[1] - c[1], dz = x[2] - c[2];
     r2 = fmax(r2, dx * dx + dy * dy + dz * dz);
   }
+  double dev2 = 0.0, lam = 0.0;
+  if (f == 0 || f == 1) {
+    static constexpr int q8[4][3] = {{4, 0, 1}, {5, 1, 2}, {6, 2, 3}, {7, 3, 0}};
+    static constexpr int t6[3][3] = {{3, 0, 1}, {4, 1, 2}, {5, 0, 2}};
+    const int nm = f == 0 ? 4 : 3;
+    lam = f == 0 ? 2.0 : 4.0 / 3.0;
+    for (int m = 0; m < nm; ++m) {
+      const int* mb = f == 0 ? q8[m] : t6[m];
+      const double *xm = X(mb[0]), *xa = X(mb[1]), *xb = X(mb[2]);
+      double q = 0.0;
+      for (int d = 0; d < 3; ++d) {
+        const double dd = xm[d] - 0.5 * (xa[d] + xb[d]);
+        q += dd * dd;
+      }
+      dev2 = fmax(dev2, q);
+    }
+  }
   for (int d = 0; d < 3; ++d) a.cen[3 * e + d] = c[d];
-  a.rad[e] = lam * sqrt(r2) * (1.0 + 1e-9);
+  a.rad[e] = (sqrt(r2) + lam * sqrt(dev2)) * (1.0 + 1e-9);
 }
 
 __global__ void k_mc_area(McArgs a) {

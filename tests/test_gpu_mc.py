@@ -170,7 +170,7 @@ def test_mc_tile_masks_exact(rvf, orc, session, case, exclude):
     stays the oracle's bit for bit, and equal to the unclassified solve."""
     M = rvf.meshes
     if case == "quad8_cube":
-        md, obs = M.cube_enclosure(8, family="quad", box_m=4), [7]
+        md, obs = M.cube_enclosure(16, family="quad", box_m=4), [7]
     elif case == "tri6_cube":
         md, obs = M.cube_enclosure(6, family="tri", box_m=4), [7]
     else:
