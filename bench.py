@@ -592,7 +592,8 @@ def run_serve(rvf, sess, size: str, local: int):
         "chunks": st["chunks"], "batched_requests": st["batched_requests"], "graph_replays": st["graph_replays"],
         "admit_bytes": admit, "admitted_bytes_peak": st["admitted_bytes_peak"],
         "burst_worker_ms": {"admit": st_burst["ms_admit"], "quad_chunks": st_burst["ms_quad_chunks"],
-                            "mc_chunks": st_burst["ms_mc_chunks"]},
+                            "mc_chunks": st_burst["ms_mc_chunks"], "free": st_burst["ms_free"],
+                            "idle": st_burst["ms_idle"]},
         "one_at_a_time_ms": {"quad": 1e3 * sum(t for n, t in enumerate(t_alone) if not reqs[burst[n]]["mc"]),
                              "mc": 1e3 * sum(t for n, t in enumerate(t_alone) if reqs[burst[n]]["mc"]),
                              "solve_only": 1e3 * sum(t_solve_only)},

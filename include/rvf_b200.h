@@ -291,6 +291,8 @@ typedef struct {
   double ms_admit;                 /* worker time: admissions (upload, tables, classes, quadrature-only tiles) */
   double ms_quad_chunks;           /*   batched quadrature chunks (with the tail of the requests they finish) */
   double ms_mc_chunks;             /*   Monte Carlo chunks */
+  double ms_free;                  /*   freeing released requests' device memory */
+  double ms_idle;                  /*   waiting for work (nothing admissible, nothing running) */
   rvf_tuned_shape tuned[8];        /* the autotuner's choices, kept by the session for all its servers (the
                                       last 8 classes it finished) */
 } rvf_server_stats;

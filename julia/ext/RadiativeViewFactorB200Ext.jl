@@ -166,6 +166,8 @@ struct RvfServerStats
     ms_admit::Float64
     ms_quad_chunks::Float64
     ms_mc_chunks::Float64
+    ms_free::Float64
+    ms_idle::Float64
     tuned::NTuple{8,RvfTunedShape}
 end
 

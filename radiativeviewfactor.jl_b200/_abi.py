@@ -111,7 +111,8 @@ class ServerStats(C.Structure):
                 ("pairs_done", C.c_int64), ("chunks", C.c_int64), ("graph_replays", C.c_int64),
                 ("batched_requests", C.c_int64), ("admitted_bytes_peak", C.c_uint64), ("n_tuned", C.c_int32),
                 ("reserved", C.c_int32), ("ms_admit", C.c_double), ("ms_quad_chunks", C.c_double),
-                ("ms_mc_chunks", C.c_double), ("tuned", TunedShape * 8)]
+                ("ms_mc_chunks", C.c_double), ("ms_free", C.c_double), ("ms_idle", C.c_double),
+                ("tuned", TunedShape * 8)]
 
     def as_dict(self):
         d = {k: getattr(self, k) for k, _ in self._fields_ if k not in ("reserved", "tuned")}

@@ -138,7 +138,7 @@ struct rvf_server {
   // statistics
   int64_t submitted = 0, completed = 0, failed = 0, canceled = 0;
   int64_t chunks = 0, graph_replays = 0, batched = 0, pairs_done = 0;
-  double ms_admit = 0, ms_quad = 0, ms_mc = 0;  // worker time by activity
+  double ms_admit = 0, ms_quad = 0, ms_mc = 0, ms_free = 0, ms_idle = 0;  // worker time by activity
   double share_mc = 0, share_quad = 0;           // the same while both kinds wait (time sharing)
   std::vector<double> latencies;
   double first_submit = -1, last_done = 0;
@@ -524,7 +524,11 @@ void free_released(rvf_server* sv) {
     std::lock_guard<std::mutex> lk(sv->mu);
     fr.swap(sv->to_free);
   }
+  if (fr.empty()) return;
+  const auto f0 = Clock::now();
   for (rvf_mesh* m : fr) rvf_mesh_release(sv->s, m);
+  std::lock_guard<std::mutex> lk(sv->mu);
+  sv->ms_free += std::chrono::duration<double, std::milli>(Clock::now() - f0).count();
 }
 
 void worker_loop(rvf_server* sv) {
@@ -566,7 +570,9 @@ void worker_loop(rvf_server* sv) {
       }
       if (admit.empty() && sv->active.empty()) {
         if (sv->closing && sv->queue.empty()) return;
+        const auto w0 = Clock::now();
         sv->cv_work.wait_for(lk, std::chrono::milliseconds(50));
+        sv->ms_idle += std::chrono::duration<double, std::milli>(Clock::now() - w0).count();
         continue;
       }
     }
@@ -854,6 +860,8 @@ int rvf_server_stats_get(rvf_server* sv, rvf_server_stats* st) try {
   st->ms_admit = sv->ms_admit;
   st->ms_quad_chunks = sv->ms_quad;
   st->ms_mc_chunks = sv->ms_mc;
+  st->ms_free = sv->ms_free;
+  st->ms_idle = sv->ms_idle;
   Session* s = sv->s;
   std::lock_guard<std::mutex> lk2(s->tune_mu);
   const size_t first = s->ftune_done.size() > 8 ? s->ftune_done.size() - 8 : 0;
