@@ -471,12 +471,10 @@ def run_serve(rvf, sess, size: str, local: int):
         t0 = time.perf_counter()
         rids = {sv.submit(arrays[k], reqs[k]["opts"]) for k in burst}
         while rids:  # release in completion order
-            done = [rid for rid in rids if sv.poll(rid)[0] not in ("queued", "running")]
-            for rid in done:
+            rid = sv.wait_any(3_600_000)
+            if rid in rids:
                 sv.release(rid)
                 rids.discard(rid)
-            if not done:
-                time.sleep(0.0005)
         t_burst = time.perf_counter() - t0
         clk_burst.__exit__(None, None, None)
         st_burst = sv.stats()
@@ -529,44 +527,33 @@ def run_serve(rvf, sess, size: str, local: int):
     th = threading.Thread(target=submitter)
     t_start = time.perf_counter()
     th.start()
-    # The client reads each checked result on the device and releases every
-    # request as soon as it is done, in the order they complete: a finished
-    # request keeps its device memory and its admission charge until
-    # rvf_release, so releasing in submission order would hold finished
+    # The client takes each request as it finishes (rvf_wait_any), reads the
+    # checked results on the device and releases every request at once: a
+    # finished request keeps its device memory and its admission charge
+    # until rvf_release, so releasing in submission order would hold finished
     # results behind a long request and stall admission.
-    pending = {}
-    finished = 0
-    while finished < n_req:
-        while True:
-            try:
-                k, rid = submitted.get_nowait()
-                pending[rid] = k
-            except queue.Empty:
-                break
-        progressed = False
-        for rid in list(pending):
+    id2k = {}
+    for _ in range(n_req):
+        rid = sv.wait_any(3_600_000)
+        while rid not in id2k:  # the submitter thread hands over (k, id) after rvf_submit returns
+            k, r = submitted.get()
+            id2k[r] = k
+        k = id2k.pop(rid)
+        try:
             state, status, _ = sv.poll(rid)
-            if state in ("queued", "running"):
-                continue
-            k = pending.pop(rid)
-            finished += 1
-            progressed = True
-            try:
-                if status != 0:
-                    raise _abi.RVFError(status, f"request {k}: {state}")
-                if k in ref_rows:
-                    idx, rr, cc = ref_rows.pop(k)
-                    rows, cols = device_rows_cols(sv.result_device(rid), reqs[k]["N"], idx, local)
-                    dF = max(dF, float(np.nanmax(np.abs(rows - rr))), float(np.nanmax(np.abs(cols - cc))))
-                    n_checked += 1
-            except _abi.RVFError as e:
-                err.append(str(e))
-            try:
-                sv.release(rid)
-            except _abi.RVFError:
-                pass
-        if not progressed:
-            time.sleep(0.0005)
+            if status != 0:
+                raise _abi.RVFError(status, f"request {k}: {state}")
+            if k in ref_rows:
+                idx, rr, cc = ref_rows.pop(k)
+                rows, cols = device_rows_cols(sv.result_device(rid), reqs[k]["N"], idx, local)
+                dF = max(dF, float(np.nanmax(np.abs(rows - rr))), float(np.nanmax(np.abs(cols - cc))))
+                n_checked += 1
+        except _abi.RVFError as e:
+            err.append(str(e))
+        try:
+            sv.release(rid)
+        except _abi.RVFError:
+            pass
     wall = time.perf_counter() - t_start
     th.join()
     st = sv.stats()

@@ -308,6 +308,11 @@ int rvf_poll(rvf_server* sv, int64_t id, rvf_request_info* info);
 /* As rvf_poll, waiting up to timeout_ms (< 0: no limit); RVF_ETIMEDOUT when
  * the request is still queued or running at the limit. */
 int rvf_wait(rvf_server* sv, int64_t id, int64_t timeout_ms, rvf_request_info* info);
+/* Waits up to timeout_ms (< 0: no limit) for any request to finish (done,
+ * failed or cancelled) that no earlier rvf_wait_any returned, in the order
+ * they finished, and stores its id; RVF_ETIMEDOUT when none did.  A client
+ * collecting results as they complete needs no polling loop. */
+int rvf_wait_any(rvf_server* sv, int64_t timeout_ms, int64_t* id);
 int rvf_cancel(rvf_server* sv, int64_t id);
 /* Host copies of a done request's result (any pointer may be NULL). */
 int rvf_request_result(rvf_server* sv, int64_t id, double* F_elem, double* A_elem, double* F_group,

@@ -300,6 +300,15 @@ function collect!(sv, id, N, G)
     F, A, Fg, Ag
 end
 
+# the id of the next request to finish (in finishing order), or nothing at the time limit
+function wait_any(sv; timeout_ms=-1)
+    id = Ref{Int64}(0)
+    rc = ccall((:rvf_wait_any, LIB), Cint, (Ptr{Cvoid}, Int64, Ref{Int64}), sv, timeout_ms, id)
+    rc == -5 && return nothing  # RVF_ETIMEDOUT
+    check(rc)
+    id[]
+end
+
 # counts, latency percentiles and the autotuner's chosen launch shapes
 function stats(sv)
     st = Ref{RvfServerStats}()

@@ -153,6 +153,7 @@ SIGNATURES = {
     "rvf_cancel": (C.c_int, [_p, C.c_int64]),
     "rvf_request_result": (C.c_int, [_p, C.c_int64, _pd, _pd, _pd, _pd, _pd]),
     "rvf_request_result_device": (C.c_int, [_p, C.c_int64, C.POINTER(_pd), C.POINTER(_pd)]),
+    "rvf_wait_any": (C.c_int, [_p, C.c_int64, C.POINTER(C.c_int64)]),
     "rvf_release": (C.c_int, [_p, C.c_int64]),
     "rvf_server_stats_get": (C.c_int, [_p, C.POINTER(ServerStats)]),
 }
@@ -410,6 +411,15 @@ class Server:
         info = RequestInfo()
         check(self.lib.rvf_wait(self.handle, rid, timeout_ms, C.byref(info)), self.lib)
         return info
+
+    def wait_any(self, timeout_ms: int = -1):
+        """The id of the next request to finish (in finishing order), or None at the time limit."""
+        rid = C.c_int64(0)
+        st = self.lib.rvf_wait_any(self.handle, timeout_ms, C.byref(rid))
+        if st == RVF_ETIMEDOUT:
+            return None
+        check(st, self.lib)
+        return int(rid.value)
 
     def cancel(self, rid: int):
         check(self.lib.rvf_cancel(self.handle, rid), self.lib)

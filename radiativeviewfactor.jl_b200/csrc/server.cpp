@@ -127,6 +127,7 @@ struct rvf_server {
   uint64_t admit_budget = 0, admitted = 0, admitted_peak = 0;
   std::mutex mu;
   std::condition_variable cv_work, cv_done;
+  std::deque<int64_t> finished_ids;  // finished requests not yet returned by rvf_wait_any
   std::deque<Req*> queue;
   std::vector<Req*> active;
   std::map<int64_t, std::unique_ptr<Req>> reqs;
@@ -201,6 +202,7 @@ void finish(rvf_server* sv, Req* r, int state, int status) {  // sv->mu held
   } else if (state == RVF_REQ_CANCELED) {
     ++sv->canceled;
   }
+  sv->finished_ids.push_back(r->id);
   sv->cv_done.notify_all();
 }
 
@@ -753,6 +755,20 @@ int rvf_wait(rvf_server* sv, int64_t id, int64_t timeout_ms, rvf_request_info* i
   const int rc = report(r, info);
   if (rc == RVF_ECANCELED) return set_err(rc, "request %lld was cancelled", (long long)id);
   if (rc != RVF_OK) return set_err(rc, "request %lld failed (status %d)", (long long)id, rc);
+  return RVF_OK;
+} catch (...) {
+  return exception_status();
+}
+
+int rvf_wait_any(rvf_server* sv, int64_t timeout_ms, int64_t* id) try {
+  if (!sv || !id) return set_err(RVF_EINVAL, "null argument");
+  std::unique_lock<std::mutex> lk(sv->mu);
+  auto ready = [&] { return !sv->finished_ids.empty(); };
+  if (timeout_ms < 0) sv->cv_done.wait(lk, ready);
+  else if (!sv->cv_done.wait_for(lk, std::chrono::milliseconds(timeout_ms), ready))
+    return set_err(RVF_ETIMEDOUT, "no request finished within %lld ms", (long long)timeout_ms);
+  *id = sv->finished_ids.front();
+  sv->finished_ids.pop_front();
   return RVF_OK;
 } catch (...) {
   return exception_status();

@@ -169,3 +169,27 @@ def test_autotuned_shapes_reported_and_identical(rvf, session):
     finally:
         sv.close()
         own.close()
+
+
+def test_wait_any_returns_each_finished_request_once(rvf, session):
+    """rvf_wait_any hands out every finished request once, in the order they
+    finished, and times out when no unreported request is finished."""
+    from rvf_b200 import _abi
+    m = rvf.meshes
+    mix = [(m.cube_enclosure(8, family="tri3", box_m=3), [7], rvf.make_options(3, seed=0)),
+           (m.parallel_plates(4, "quad4"), [], rvf.make_options(2, seed=0)),
+           (m.cube_enclosure(3, family="quad4", box_m=2), [7], rvf.make_options(2, monte_carlo=True, n_samples=4, seed=1))]
+    sv = _abi.Server(session)
+    try:
+        ids = [sv.submit(rvf.mesh_desc_arrays(md, obs), o) for md, obs, o in mix]
+        got = []
+        for _ in ids:
+            rid = sv.wait_any(120000)
+            assert rid is not None
+            assert sv.poll(rid)[0] == "done"
+            got.append(rid)
+            sv.release(rid)
+        assert sorted(got) == sorted(ids)
+        assert sv.wait_any(50) is None
+    finally:
+        sv.close()
