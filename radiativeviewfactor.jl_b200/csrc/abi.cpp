@@ -66,6 +66,10 @@ int exception_status() noexcept {
 int DevBuf::alloc(Session* s, size_t n) {
   free_();
   if (n == 0) return RVF_OK;
+  // test hook: this allocation fails (before the cache could serve it)
+  if (s->fail_alloc_in > 0 && --s->fail_alloc_in == 0)
+    return set_err(RVF_ENOMEM, "cudaMalloc(%zu) failed: injected allocation failure (fault_inject)", n);
+  if (n < kSpareMin) n = kSpareMin;  // the smallest size class
   if (n >= kSpareMin) {
     // the smallest cached buffer that holds n with at most a quarter to spare
     std::lock_guard<std::mutex> lk(s->spare_mu);
@@ -82,10 +86,12 @@ int DevBuf::alloc(Session* s, size_t n) {
       return RVF_OK;  // already charged to the budget
     }
   }
-  // Large buffers come in size classes 2^(1/4) apart (at most 19% spare), so
-  // that a freed one serves the next request of about the same size -- mesh
-  // after mesh of different element counts, as a serving stream sends them --
-  // instead of a cudaMalloc / cudaFree of gigabytes each time.
+  // Buffers come in size classes 2^(1/4) apart from 4 KiB (at most 19%
+  // spare), so that a freed one serves the next request of about the same
+  // size -- mesh after mesh of different element counts, as a serving stream
+  // sends them -- instead of a cudaMalloc / cudaFree each time (gigabytes of
+  // mapping work for an F; about a millisecond and a device synchronisation
+  // for any buffer).
   if (n >= kSpareMin) {
     size_t c = kSpareMin;
     while (c < n) {
@@ -98,8 +104,6 @@ int DevBuf::alloc(Session* s, size_t n) {
   if (s->used + n > s->budget)
     return set_err(RVF_EBUDGET, "HBM budget exceeded: need %zu more bytes, %zu of %zu in use", n, s->used,
                    s->budget);
-  if (s->fail_alloc_in > 0 && --s->fail_alloc_in == 0)
-    return set_err(RVF_ENOMEM, "cudaMalloc(%zu) failed: injected allocation failure (fault_inject)", n);
   cudaError_t e = cudaMalloc(&ptr, n);
   if (e != cudaSuccess) {
     cudaGetLastError();

@@ -45,7 +45,7 @@ struct DevBuf {
 };
 
 int upload(Session* s, DevBuf& b, const void* src, size_t n);
-constexpr size_t kSpareMin = (size_t)1 << 20;
+constexpr size_t kSpareMin = (size_t)4096;  // every buffer: cudaFree costs ~1 ms and synchronises the device
 // Frees cached buffers, the oldest first, until `need` more bytes fit the
 // budget (need = 0: all of them).
 void release_spares(Session* s, size_t need = 0);
@@ -106,7 +106,7 @@ struct rvf_session {
   std::map<uint64_t, cudaGraphExec_t> graphs;
   std::set<rvf_mesh*> meshes;
   cudaEvent_t ev[8] = {};
-  // Freed device buffers of kSpareMin bytes (1 MiB) or more, kept for reuse and still
+  // Freed device buffers (all of them, in size classes from 4 KiB), kept for reuse and still
   // charged to the budget: solving one new mesh after another (an F of
   // 15 GB each) then skips cudaMalloc / cudaFree, whose mapping work costs
   // a few hundred milliseconds per mesh.  Dropped when an allocation would
