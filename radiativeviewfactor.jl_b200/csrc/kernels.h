@@ -67,9 +67,6 @@ struct TileClassArgs {
   double cull_margin;
   bool occ, dim3;
   bool skip_groups;  // rays skip the triangles of their elements' groups (false: a ray may hit any triangle)
-  const NodeD* nodes;  // FP64 boxes of the same tree (for ubox)
-  NodeD* ubox;         // per tile with ray work: the union of its candidate leaves' boxes, or null
-  NodeF* uboxf;        //   and its FP32 copy (each bound rounded to nearest, as the tree's FP32 boxes)
   const NodeF* nodesf;
   int n_nodes;
   const int32_t* frontier;
@@ -152,7 +149,6 @@ struct PairArgs {
   int64_t tile0;                 // batched generation: first tile of this request in the launch
   const uint8_t* tcls;           // tile classes and masks (kernels_cull.cu), or null
   const uint32_t* tmask;
-  const NodeD* ubox;             // per tile: the box a ray must reach to be blockable (kernels_cull.cu), or null
   bool fast_done;                // tiles without ray work were integrated by k_fast_fp64: skip them
   int fast_groups;               // k_fast_fp64 tasks per tile (1, 2 or 4 row groups)
   const int32_t* work;           // the tiles of the chunked pipeline in order (null: every tile)
@@ -216,7 +212,6 @@ struct MixedArgs {
   int64_t tile0;
   const uint8_t* tcls;  // tile classes and masks (kernels_cull.cu), or null
   const uint32_t* tmask;
-  const NodeF* uboxf;   // per tile: the box a ray must reach to be blockable (FP32), or null
   bool fast_done;       // tiles without ray work were integrated by k_fast_mixed: skip them
   int fast_groups;      // k_fast_mixed tasks per tile (1, 2 or 4 row groups)
   const int32_t* work;  // the tiles of the chunked pipeline in order (null: every tile)

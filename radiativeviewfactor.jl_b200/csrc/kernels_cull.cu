@@ -370,44 +370,6 @@ __global__ void __launch_bounds__(kCullWarps * 32, RVF_CULL_MIN_BLOCKS) k_tile_c
       }
       __syncwarp();
       all_ones = over;
-      // A blocked ray passes the box test of its triangle's leaf, so of every
-      // box holding that leaf's: the union of the candidate leaves' boxes is
-      // the box the generation tests instead of the root's (exact min / max
-      // of the FP64 boxes; the FP32 copy rounds each bound as the tree's FP32
-      // boxes do, and rounding is monotone).  Overflow: the root's.
-      if (a.ubox && nl > 0) {
-        double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
-        for (int r = lane; r < (over ? 0 : nrun); r += 32) {
-          const NodeD nd = a.nodes[rleaf[r]];
-#pragma unroll
-          for (int c = 0; c < 3; ++c) {
-            lo[c] = fmin(lo[c], nd.lo[c]);
-            hi[c] = fmax(hi[c], nd.hi[c]);
-          }
-        }
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1)
-#pragma unroll
-          for (int c = 0; c < 3; ++c) {
-            lo[c] = fmin(lo[c], __shfl_xor_sync(kFull, lo[c], o));
-            hi[c] = fmax(hi[c], __shfl_xor_sync(kFull, hi[c], o));
-          }
-        if (lane == 0) {
-          NodeD u = a.nodes[0];
-          NodeF uf = a.nodesf[0];
-          if (!over) {
-#pragma unroll
-            for (int c = 0; c < 3; ++c) {
-              u.lo[c] = lo[c];
-              u.hi[c] = hi[c];
-              uf.lo[c] = (float)lo[c];
-              uf.hi[c] = (float)hi[c];
-            }
-          }
-          a.ubox[t] = u;
-          a.uboxf[t] = uf;
-        }
-      }
     }
     if (all_ones) {
       cls |= kClsSlow;

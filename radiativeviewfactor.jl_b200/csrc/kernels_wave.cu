@@ -508,7 +508,6 @@ __global__ void __launch_bounds__(256, 2) k_gen_fp64(const GenBatch* __restrict_
   __shared__ int s_req;
   __shared__ unsigned long long s_used, s_slots;
   __shared__ NodeD s_root;  // the request's root box: the only node the generation tests
-  __shared__ NodeD s_ubox;  // the tile's candidate leaves' union box (the root's without classes)
   __shared__ uint32_t s_mask[kTile];  // pairs of the tile whose rays may be blocked (row -> lanes)
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -531,10 +530,7 @@ __global__ void __launch_bounds__(256, 2) k_gen_fp64(const GenBatch* __restrict_
         s_req = r;
         s_tile = g - L.tile_base[r] + a.tile0;
         if (a.work) s_tile = a.work[s_tile];
-        if (OCC) {
-          s_root = a.nodes[0];
-          s_ubox = (a.ubox && a.tcls && (a.tcls[s_tile] & kClsSlow)) ? a.ubox[s_tile] : s_root;
-        }
+        if (OCC) s_root = a.nodes[0];
         int64_t bi, bj;
         tile_coords(s_tile, a.nT, bi, bj);
         const uint32_t blk_bytes = (uint32_t)(kComp * a.pmax * kTile * sizeof(double));
@@ -640,10 +636,7 @@ __global__ void __launch_bounds__(256, 2) k_gen_fp64(const GenBatch* __restrict_
             } else if (DIM3) {
               RayD R;
               cast = (K > 0.0) && (sw ? make_ray(xj, -rx, -ry, -rz, r2, R) : make_ray(xi, rx, ry, rz, r2, R));
-              // a ray with a finite 1/d is blockable only through the tile's
-              // candidate leaves (box monotonicity); others test the root
-              const bool fin = !R.zdir && isfinite(R.inv[0]) && isfinite(R.inv[1]) && isfinite(R.inv[2]);
-              if (cast) defer = slab_d(fin ? s_ubox : root, R);
+              if (cast) defer = slab_d(root, R);
             } else {
               cast = K > 0.0;
               if (cast) {
@@ -757,7 +750,6 @@ __global__ void __launch_bounds__(256, 2) k_gen_mixed(const GenBatch* __restrict
   __shared__ unsigned long long s_used, s_slots;
   __shared__ NodeF s_rootf;  // the request's root box, FP32 and FP64
   __shared__ NodeD s_root;
-  __shared__ NodeF s_uboxf;  // the tile's candidate leaves' union box (FP32; the root's without classes)
   __shared__ uint32_t s_mask[kTile];  // pairs of the tile whose rays may be blocked (row -> lanes)
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -784,7 +776,6 @@ __global__ void __launch_bounds__(256, 2) k_gen_mixed(const GenBatch* __restrict
         if (OCC) {
           s_rootf = a.nodesf[0];
           s_root = a.nodes[0];
-          s_uboxf = (a.uboxf && a.tcls && (a.tcls[s_tile] & kClsSlow)) ? a.uboxf[s_tile] : s_rootf;
         }
         int64_t bi, bj;
         tile_coords(s_tile, a.nT, bi, bj);
@@ -911,7 +902,7 @@ __global__ void __launch_bounds__(256, 2) k_gen_mixed(const GenBatch* __restrict
                 sw ? make_ray_f(xo, -rx, -ry, -rz, r2, a.delta, R) : make_ray_f(xo, rx, ry, rz, r2, a.delta, R);
             badray = !rok;
             if (rok) {
-              defer32 = slab_f(s_uboxf, R) != kMiss;  // FP32 rays have a finite 1/d
+              defer32 = slab_f(s_rootf, R) != kMiss;
               if (!defer32 && logp) logp[sw ? q * a.log_pm + p : p * a.log_pm + q] = 1;
             }
           }

@@ -57,7 +57,6 @@ struct Tables {
   DevBuf tabf;  // FP32 table, built on the first mixed-precision solve
   DevBuf tcls, tmask;  // tile classes and masks of the last solve (kernels_cull.cu)
   DevBuf twork;        // the tiles the chunked pipeline integrates (tile indices, row-major)
-  DevBuf tubox, tuboxf;  // per tile: union of its candidate leaves' boxes (FP64, FP32)
 };
 
 // Autotuner choices of the request server (server.cpp), kept by the session

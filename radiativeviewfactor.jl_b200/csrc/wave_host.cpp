@@ -166,11 +166,6 @@ int wave_prepare(Session* s, rvf_mesh* m, Tables* T, const rvf_options* o, uint8
       c.leaf_of = m->leaf_of.as<int32_t>();
       c.sat = o->geometric_soup ? m->sat_geo.as<float4>() : m->sat_ref.as<float4>();
       c.sat_em = m->sat_em;
-      c.nodes = m->nodes.as<NodeD>();
-      if (T->tubox.bytes < sizeof(NodeD) * nt && (rc = T->tubox.alloc(s, sizeof(NodeD) * nt))) return rc;
-      if (T->tuboxf.bytes < sizeof(NodeF) * nt && (rc = T->tuboxf.alloc(s, sizeof(NodeF) * nt))) return rc;
-      c.ubox = T->tubox.as<NodeD>();
-      c.uboxf = T->tuboxf.as<NodeF>();
     }
     c.cls = T->tcls.as<uint8_t>();
     c.mask = T->tmask.as<uint32_t>();
@@ -182,10 +177,8 @@ int wave_prepare(Session* s, rvf_mesh* m, Tables* T, const rvf_options* o, uint8
     if (n_kernels) *n_kernels += 1;
     a.tcls = c.cls;
     a.tmask = c.mask;
-    a.ubox = c.ubox;
     w.ma.tcls = c.cls;
     w.ma.tmask = c.mask;
-    w.ma.uboxf = c.uboxf;
     if (!ray_log) {
       // The chunked pipeline's tiles: those with ray work (or near-field /
       // nearly coincident pairs in mixed precision), in row-major order; the
