@@ -238,3 +238,43 @@ def test_curve_mesh_guard_for_backends_without_support(rvf):
     assert not assembly._gpu_supports(Other(), "curves")
     with pytest.raises(ValueError, match="curve meshes"):
         rvf.compute_view_factors(md, backend=Other())
+
+
+def test_mc_element_bound_covers_quadratic_elements():
+    """The Monte Carlo classification's element radius (k_mc_bounds): corner
+    radius about the corners' centroid plus the mid-side nodes' largest
+    deviation from their edges' midpoints times 2 (Quad8) or 4/3 (Tri6).
+    Every point of random curved elements, evaluated with the shape
+    functions of shape_surface (same node order), lies inside it."""
+    import numpy as np
+    rng = np.random.default_rng(11)
+
+    def quad8(x, e):
+        return np.array([0.25 * (1 - x) * (1 - e) * (-x - e - 1), 0.25 * (1 + x) * (1 - e) * (x - e - 1),
+                         0.25 * (1 + x) * (1 + e) * (x + e - 1), 0.25 * (1 - x) * (1 + e) * (-x + e - 1),
+                         0.5 * (1 - x * x) * (1 - e), 0.5 * (1 + x) * (1 - e * e), 0.5 * (1 - x * x) * (1 + e),
+                         0.5 * (1 - x) * (1 - e * e)])
+
+    def tri6(x, e):
+        l1, l2, l3 = 1 - x - e, x, e
+        return np.array([l1 * (2 * l1 - 1), l2 * (2 * l2 - 1), l3 * (2 * l3 - 1), 4 * l1 * l2, 4 * l2 * l3,
+                         4 * l1 * l3])
+
+    fams = {"quad8": (quad8, 4, [(4, 0, 1), (5, 1, 2), (6, 2, 3), (7, 3, 0)], 2.0, np.linspace(-1, 1, 121)),
+            "tri6": (tri6, 3, [(3, 0, 1), (4, 1, 2), (5, 0, 2)], 4.0 / 3.0, np.linspace(0, 1, 121))}
+    for name, (shape, nc, mids, lam, g) in fams.items():
+        X, E = np.meshgrid(g, g)
+        if name == "tri6":
+            keep = X + E <= 1
+            X, E = X[keep], E[keep]
+        N = shape(X.ravel(), E.ravel())
+        for _ in range(200):
+            nodes = np.zeros((nc + len(mids), 3))
+            nodes[:nc] = rng.normal(size=(nc, 3))
+            for m, a, b in mids:
+                nodes[m] = 0.5 * (nodes[a] + nodes[b]) + rng.normal(size=3) * rng.uniform(0, 0.6)
+            c = nodes[:nc].mean(axis=0)
+            dev = max(np.linalg.norm(nodes[m] - 0.5 * (nodes[a] + nodes[b])) for m, a, b in mids)
+            r = np.linalg.norm(nodes[:nc] - c, axis=1).max() + lam * dev
+            pts = N.T @ nodes
+            assert np.linalg.norm(pts - c, axis=1).max() <= r * (1 + 1e-12), name
