@@ -158,7 +158,10 @@ int upload(Session* s, DevBuf& b, const void* src, size_t n) {
 // mesh upload
 // ---------------------------------------------------------------------------
 static const int kFamNodes[6] = {8, 6, 4, 3, 3, 2};
-static const int64_t kOrderRun = 8;  // caller-consecutive elements kept together in the internal order
+#ifndef RVF_ORDER_RUN
+#define RVF_ORDER_RUN 8
+#endif
+static const int64_t kOrderRun = RVF_ORDER_RUN;  // caller-consecutive elements kept together in the internal order
 
 int mesh_upload(Session* s, const rvf_mesh_desc* d, rvf_mesh** out) {
   if (!d || !out) return set_err(RVF_EINVAL, "null argument");

@@ -467,6 +467,9 @@ namespace {
 #ifndef RVF_DL_CHUNKS
 #define RVF_DL_CHUNKS 8
 #endif
+#ifndef RVF_DL_MIN_PP
+#define RVF_DL_MIN_PP 1e9  // point pairs of a download chunk at least
+#endif
 constexpr int kDownloadChunks = RVF_DL_CHUNKS;
 
 struct ColumnDownload {
@@ -634,7 +637,7 @@ int rvf_solve(rvf_session* s, rvf_mesh* m, const rvf_options* o, double* F_elem,
     // columns); without, one chunk as far as the ray queues allow.
     double pp_budget = 0.0;
     if (dl.host && w.n_tiles > 0)
-      pp_budget = std::max(1e9, (double)w.n_tiles * kTile * kTile * w.pmax * w.pmax / kDownloadChunks);
+      pp_budget = std::max((double)RVF_DL_MIN_PP, (double)w.n_tiles * kTile * kTile * w.pmax * w.pmax / kDownloadChunks);
     while (!w.done()) {  // chunks: each claims tiles while the ray queues have room
       ChunkInfo ci;
       const int64_t before = w.claimed;
