@@ -465,10 +465,10 @@ namespace {
 // one copy).  A pageable destination makes the copies synchronous: still
 // correct, without the overlap.
 #ifndef RVF_DL_CHUNKS
-#define RVF_DL_CHUNKS 8
+#define RVF_DL_CHUNKS 16
 #endif
 #ifndef RVF_DL_MIN_PP
-#define RVF_DL_MIN_PP 1e9  // point pairs of a download chunk at least
+#define RVF_DL_MIN_PP 2.5e8  // point pairs of a download chunk at least
 #endif
 constexpr int kDownloadChunks = RVF_DL_CHUNKS;
 
@@ -631,10 +631,11 @@ int rvf_solve(rvf_session* s, rvf_mesh* m, const rvf_options* o, double* F_elem,
     const std::function<void()> queue_columns = [&]() {
       if (dl.host && dl_err == cudaSuccess) dl_err = dl.advance(dl_upto);
     };
-    // With a host F the pipeline runs in at least kDownloadChunks chunks, so
-    // that the columns of finished tile rows go down while later chunks
-    // compute (the last chunk's rows hold about 1/sqrt(chunks) of the
-    // columns); without, one chunk as far as the ray queues allow.
+    // With a host F the pipeline runs in up to kDownloadChunks chunks (none
+    // below RVF_DL_MIN_PP point pairs), so that the columns of finished tile
+    // rows go down while later chunks compute (the last chunk's rows hold
+    // about 1/sqrt(chunks) of the columns); without, one chunk as far as the
+    // ray queues allow.
     double pp_budget = 0.0;
     if (dl.host && w.n_tiles > 0)
       pp_budget = std::max((double)RVF_DL_MIN_PP, (double)w.n_tiles * kTile * kTile * w.pmax * w.pmax / kDownloadChunks);
